@@ -1,0 +1,292 @@
+#!/usr/bin/env python
+"""Benchmark of the CLUE make_clusters path on B200 (one JSON line on rank 0).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload NAME]
+
+A step is one pass of the five CLUE stages over one synthetic workload already resident in
+HBM (`value`, device time from CUDA events on the launching stream, L2 flushed between steps
+by writing a 256 MiB buffer).  `e2e` repeats the step through the C ABI with pinned host
+buffers: host->device copy of coordinates and weights, the stages, and device->host copy of
+the labels, seed flags, densities, nearest highers and deltas, all inside the timed region.
+Under torchrun every rank clusters its own replica of the workload (seeded by rank, no
+collective on the data path, scaling "weak"); the step time is the max over ranks.
+
+--impl reference times the CPU restatement of the reference's serial path (OpenMP over points,
+all host cores) on the same workload, on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "points/sec batched vs plain launch on 1 B200; p50/p99 event latency"
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def make_workload(name: str, rank: int):
+    from cluestering_alpaka3_b200 import synthetic
+    if name == "blobs2d_1m":
+        return synthetic.blobs_2d_1m(seed=2000 + rank)
+    if name == "blobs2d_16k":
+        return synthetic.blobs_2d_16k(seed=1000 + rank)
+    if name == "blobs3d_4m":
+        return synthetic.blobs_3d_4m(seed=3000 + rank)
+    raise SystemExit(f"unknown workload {name}")
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons while the timed region runs."""
+
+    def __init__(self, device: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(device), f"--query-gpu={q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.p.terminate()
+        self.p.wait()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[0]))
+                mx.append(float(r[1]))
+                for k, nm in enumerate(names):
+                    if r[4 + k].strip().lower() == "active":
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline_run(wl, nthreads: int):
+    from oracle import oracle as O
+    kname, kpar = wl.kernel
+    cfg = O.Config(dc=wl.dc, rhoc=wl.rhoc, dm=wl.dm, kernel=kname, kernel_par=kpar, nthreads=nthreads)
+    t0 = time.perf_counter()
+    r = O.run(wl.coords, wl.weight, cfg)
+    return time.perf_counter() - t0, r
+
+
+def reference_arm(args, rank: int):
+    """The reference's path restated in C (the reference itself cannot be built: its alpaka3
+    dependency is fetched over the network), timed on the host cores."""
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    O.build()
+    wl = make_workload(args.workload, 0)
+    n = wl.coords.shape[1]
+    cores = os.cpu_count() or 1
+    for _ in range(max(1, min(args.warmup, 1))):
+        cpu_baseline_run(wl, cores)
+    times = []
+    for _ in range(args.steps):
+        dt, _ = cpu_baseline_run(wl, cores)
+        times.append(dt)
+    tot = sum(times)
+    v = n * len(times) / tot
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "points/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": wl.name, "n_points": n, "ndim": wl.coords.shape[0], "dc": wl.dc,
+                       "rhoc": wl.rhoc, "dm": wl.dm, "kernel": list(wl.kernel)},
+            "cpu_baseline": {"value": v, "unit": "points/s", "cores": cores, "kind": "port",
+                             "sample": f"full {wl.name} workload ({n} points) per step"},
+            "e2e": {"value": v, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="blobs2d_1m")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+
+    from cluestering_alpaka3_b200 import bytes_model, capi
+
+    wl = make_workload(args.workload, rank)
+    ndim, n = wl.coords.shape
+    kname, kpar = wl.kernel
+    kernel = {"flat": capi.FlatKernel, "exp": capi.ExponentialKernel, "gaus": capi.GaussianKernel}[kname](*kpar)
+    params = capi.Params(dc=wl.dc, rhoc=wl.rhoc, dm=wl.dm)
+    metric = capi.Metric()
+
+    ctx = capi.Context(local)
+    ctx.reserve(ndim, n)
+    stream = torch.cuda.Stream(device=local)
+    sp = stream.cuda_stream
+    dcoords = torch.from_numpy(wl.coords).cuda(local)
+    dweight = torch.from_numpy(wl.weight).cuda(local)
+    outs = {k: torch.empty(n, dtype=dt, device=f"cuda:{local}") for k, dt in
+            (("cluster_index", torch.int32), ("is_seed", torch.int32), ("rho", torch.float32),
+             ("nearest_higher", torch.int32), ("delta", torch.float32))}
+    optr = {k: v.data_ptr() for k, v in outs.items()}
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+    def step_device():
+        ctx.make_clusters_device(dcoords.data_ptr(), dweight.data_ptr(), ndim, n, optr, params, kernel,
+                                 metric, stream=sp, blocking=False)
+
+    torch.cuda.synchronize()
+    for _ in range(args.warmup):
+        step_device()
+    info = ctx.read_info(sp)
+    torch.cuda.synchronize()
+
+    # ---- timed device-resident steps --------------------------------------
+    ctx.set_timing(True)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    stage_ms = np.zeros(4)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = ctx.kernel_launches
+    clocks = Clocks(local)
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            starts[k].record(stream)
+        step_device()
+        with torch.cuda.stream(stream):
+            ends[k].record(stream)
+        stage_ms += np.array(ctx.stage_times())
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    launches = ctx.kernel_launches - launches0
+    ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = float(sum(ms))
+    if world > 1:
+        t = torch.tensor([total_ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        dist.barrier()
+    ctx.set_timing(False)
+    value = world * n * args.steps / (total_ms / 1e3)
+
+    # ---- end to end through the C ABI with pinned host buffers ----------------
+    hc = torch.from_numpy(wl.coords).pin_memory().numpy()
+    hw = torch.from_numpy(wl.weight).pin_memory().numpy()
+    for _ in range(2):
+        res = ctx.make_clusters_host(hc, hw, params, kernel, metric, stream=sp)
+    e2e_ms = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = ctx.make_clusters_host(hc, hw, params, kernel, metric, stream=sp)
+        e2e_ms.append(1e3 * (time.perf_counter() - t0))
+    e2e_total = float(sum(e2e_ms))
+    if world > 1:
+        t = torch.tensor([e2e_total], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+
+    # ---- roofline of the dominant kernel (local density) ------------------------
+    peak, peak_kind = load_peaks()
+    B = bytes_model.algorithmic_bytes(wl.coords, wl.dc, wl.dm)
+    stage_avg = stage_ms / args.steps
+    dens_ms = float(stage_avg[1])
+    achieved = B["density_kernel"] / (dens_ms / 1e3) / 1e9
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", f"traffic_{wl.name}.json")
+    if os.path.exists(tfile):
+        with open(tfile) as f:
+            traffic = json.load(f).get("density_bytes_per_launch")
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cores = os.cpu_count() or 1
+        dt, ref = cpu_baseline_run(wl, cores)
+        same = bool(np.array_equal(ref.cluster_index, res.cluster_index))
+        cpu = {"value": n / dt, "unit": "points/s", "cores": cores, "kind": "port",
+               "sample": f"full {wl.name} workload ({n} points), OpenMP over points",
+               "labels_equal_to_gpu": same}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": wl.name, "n_points": n, "ndim": ndim, "dc": wl.dc, "rhoc": wl.rhoc,
+                       "dm": wl.dm, "kernel": [kname, list(kpar)], "metric": "euclidean",
+                       "l2": "flushed between steps (256 MiB write)",
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "n_clusters": int(info.n_clusters), "n_tiles": int(info.n_tiles)},
+            "e2e": {"value": world * n * args.steps / (e2e_total / 1e3), "unit": "points/s",
+                    "h2d_bytes_per_step": int(n * (ndim + 1) * 4),
+                    "d2h_bytes_per_step": int(n * 5 * 4)},
+            "roofline": {"bound": "hbm", "kernel": "k_density", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": traffic, "algorithmic_bytes": B["density_kernel"],
+                         "launch_ms": dens_ms},
+            "stage_ms": {"tiles": stage_avg[0], "density": stage_avg[1], "nearest_higher": stage_avg[2],
+                         "seeds_labels": stage_avg[3]},
+            "b_alg_total": B["total"],
+            "pipeline_hbm_frac": B["total"] / (total_ms / args.steps / 1e3) / 1e9 / peak,
+            "cpu_baseline": cpu, "clocks": clk, "gpu_launches": int(launches),
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,364 @@
+"""ctypes binding of the C ABI in include/clue_b200.h (libclue_b200.so, built in-tree).
+
+The library is the product: there is no Python or CPU fallback.  Importing this module
+raises if the shared library is missing; calls raise ``ClueError`` subclasses that mirror
+the reference's host exceptions (std::invalid_argument -> ValueError,
+std::out_of_range -> IndexError, std::runtime_error -> RuntimeError).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "libclue_b200.so")
+MAX_DIM = 10
+
+OK, ERR_INVALID_ARG, ERR_OOM, ERR_CAPACITY, ERR_TIMEOUT, ERR_CUDA, ERR_NOT_SUPPORTED, \
+    ERR_NONFINITE, ERR_OUT_OF_RANGE = range(9)
+
+KERNEL_FLAT, KERNEL_EXPONENTIAL, KERNEL_GAUSSIAN = 0, 1, 2
+METRIC_EUCLIDEAN, METRIC_WEIGHTED_EUCLIDEAN, METRIC_PERIODIC_EUCLIDEAN, METRIC_MANHATTAN, \
+    METRIC_CHEBYSHEV, METRIC_WEIGHTED_CHEBYSHEV = range(6)
+TIE_REFERENCE, TIE_RHO_INDEX = 0, 1
+MEM_DEVICE, MEM_HOST = 0, 1
+
+# Every symbol declared in include/clue_b200.h.
+EXPORTED = [
+    "clue_abi_version", "clue_last_error", "clue_status_string", "clue_check_params",
+    "clue_check_kernel", "clue_check_metric", "clue_grid_shape", "clue_metric_eval",
+    "clue_kernel_eval", "clue_device_count", "clue_device_alloc", "clue_device_free",
+    "clue_host_alloc_pinned", "clue_host_free_pinned", "clue_memcpy_htod", "clue_memcpy_dtoh",
+    "clue_memcpy_dtod", "clue_stream_create", "clue_stream_destroy", "clue_stream_synchronize",
+    "clue_context_create", "clue_context_destroy", "clue_context_reserve",
+    "clue_context_workspace_bytes", "clue_make_clusters", "clue_make_clusters_async",
+    "clue_context_read_info", "clue_get_clusters", "clue_context_set_timing",
+    "clue_context_stage_times", "clue_context_kernel_launches",
+]
+
+
+class ClueError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"[{status}] {msg}")
+        self.status = status
+
+
+class ClueInvalidArgument(ClueError, ValueError):
+    pass
+
+
+class ClueOutOfRange(ClueError, IndexError):
+    pass
+
+
+class _Kernel(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int32), ("par", ctypes.c_float * 3)]
+
+
+class _Metric(ctypes.Structure):
+    _fields_ = [("type", ctypes.c_int32), ("par", ctypes.c_float * MAX_DIM)]
+
+
+class _Params(ctypes.Structure):
+    _fields_ = [("dc", ctypes.c_float), ("rhoc", ctypes.c_float), ("dm", ctypes.c_float),
+                ("seed_dc", ctypes.c_float), ("points_per_tile", ctypes.c_int32),
+                ("wrapped", ctypes.c_uint8 * MAX_DIM), ("seed_capacity", ctypes.c_int64),
+                ("tiebreak", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+class _Outputs(ctypes.Structure):
+    _fields_ = [("cluster_index", ctypes.c_void_p), ("is_seed", ctypes.c_void_p),
+                ("rho", ctypes.c_void_p), ("nearest_higher", ctypes.c_void_p),
+                ("delta", ctypes.c_void_p)]
+
+
+class _RunInfo(ctypes.Structure):
+    _fields_ = [("n_seeds", ctypes.c_int64), ("n_clusters", ctypes.c_int64),
+                ("dropped_seeds", ctypes.c_int64), ("seed_capacity_used", ctypes.c_int64),
+                ("n_tiles", ctypes.c_int64), ("n_per_dim", ctypes.c_int64),
+                ("label_rounds", ctypes.c_int64)]
+
+
+def _load() -> ctypes.CDLL:
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"libclue_b200.so is not built ({LIB_PATH}); run `make -C {_PKG}`")
+    lib = ctypes.CDLL(LIB_PATH)
+    vp, i32, i64, f32, sz = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_float, ctypes.c_size_t
+    sig = {
+        "clue_abi_version": ([], i32),
+        "clue_last_error": ([], ctypes.c_char_p),
+        "clue_status_string": ([ctypes.c_int], ctypes.c_char_p),
+        "clue_check_params": ([ctypes.POINTER(_Params)], ctypes.c_int),
+        "clue_check_kernel": ([ctypes.POINTER(_Kernel)], ctypes.c_int),
+        "clue_check_metric": ([ctypes.POINTER(_Metric), i32], ctypes.c_int),
+        "clue_grid_shape": ([i32, i32, i32, ctypes.POINTER(i32), ctypes.POINTER(i32)], ctypes.c_int),
+        "clue_metric_eval": ([ctypes.POINTER(_Metric), i32, vp, vp], f32),
+        "clue_kernel_eval": ([ctypes.POINTER(_Kernel), f32, i32, i32], f32),
+        "clue_device_count": ([ctypes.POINTER(i32)], ctypes.c_int),
+        "clue_device_alloc": ([i32, sz, ctypes.POINTER(vp)], ctypes.c_int),
+        "clue_device_free": ([vp], ctypes.c_int),
+        "clue_host_alloc_pinned": ([sz, ctypes.POINTER(vp)], ctypes.c_int),
+        "clue_host_free_pinned": ([vp], ctypes.c_int),
+        "clue_memcpy_htod": ([vp, vp, sz, vp], ctypes.c_int),
+        "clue_memcpy_dtoh": ([vp, vp, sz, vp], ctypes.c_int),
+        "clue_memcpy_dtod": ([vp, vp, sz, vp], ctypes.c_int),
+        "clue_stream_create": ([i32, ctypes.POINTER(vp)], ctypes.c_int),
+        "clue_stream_destroy": ([vp], ctypes.c_int),
+        "clue_stream_synchronize": ([vp], ctypes.c_int),
+        "clue_context_create": ([i32, ctypes.POINTER(vp)], ctypes.c_int),
+        "clue_context_destroy": ([vp], ctypes.c_int),
+        "clue_context_reserve": ([vp, i32, i32, i32], ctypes.c_int),
+        "clue_context_workspace_bytes": ([vp], sz),
+        "clue_make_clusters": ([vp, ctypes.POINTER(_Params), ctypes.POINTER(_Kernel),
+                                ctypes.POINTER(_Metric), i32, i32, vp, vp, ctypes.POINTER(_Outputs),
+                                i32, vp, ctypes.POINTER(_RunInfo)], ctypes.c_int),
+        "clue_make_clusters_async": ([vp, ctypes.POINTER(_Params), ctypes.POINTER(_Kernel),
+                                      ctypes.POINTER(_Metric), i32, i32, vp, vp,
+                                      ctypes.POINTER(_Outputs), vp], ctypes.c_int),
+        "clue_context_read_info": ([vp, vp, ctypes.POINTER(_RunInfo)], ctypes.c_int),
+        "clue_context_set_timing": ([vp, i32], ctypes.c_int),
+        "clue_context_stage_times": ([vp, ctypes.POINTER(f32), i32], ctypes.c_int),
+        "clue_context_kernel_launches": ([vp], ctypes.c_uint64),
+        "clue_get_clusters": ([vp, i32, vp, vp, vp, ctypes.POINTER(i32), ctypes.POINTER(i32), vp],
+                              ctypes.c_int),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    _ = i64
+    return lib
+
+
+lib = _load()
+
+
+def last_error() -> str:
+    msg = lib.clue_last_error()
+    return msg.decode() if msg else ""
+
+
+def check(status: int) -> None:
+    if status == OK:
+        return
+    msg = last_error()
+    if status == ERR_INVALID_ARG or status == ERR_NONFINITE:
+        raise ClueInvalidArgument(status, msg)
+    if status == ERR_OUT_OF_RANGE:
+        raise ClueOutOfRange(status, msg)
+    raise ClueError(status, msg)
+
+
+@dataclass
+class Kernel:
+    """A convolutional kernel plugin: FlatKernel / ExponentialKernel / GaussianKernel."""
+    type: int
+    par: tuple
+
+    def struct(self) -> _Kernel:
+        k = _Kernel()
+        k.type = self.type
+        for i, v in enumerate(self.par):
+            k.par[i] = v
+        check(lib.clue_check_kernel(ctypes.byref(k)))
+        return k
+
+
+def FlatKernel(flat: float) -> Kernel:
+    return Kernel(KERNEL_FLAT, (flat,))
+
+
+def ExponentialKernel(avg: float, amplitude: float) -> Kernel:
+    return Kernel(KERNEL_EXPONENTIAL, (avg, amplitude))
+
+
+def GaussianKernel(avg: float, std: float, amplitude: float) -> Kernel:
+    return Kernel(KERNEL_GAUSSIAN, (avg, std, amplitude))
+
+
+@dataclass
+class Metric:
+    type: int = METRIC_EUCLIDEAN
+    par: tuple = ()
+
+    def struct(self, ndim: int) -> _Metric:
+        m = _Metric()
+        m.type = self.type
+        for i, v in enumerate(self.par):
+            m.par[i] = v
+        check(lib.clue_check_metric(ctypes.byref(m), ndim))
+        return m
+
+
+@dataclass
+class Params:
+    dc: float
+    rhoc: float
+    dm: float | None = None
+    seed_dc: float | None = None
+    points_per_tile: int = 128
+    wrapped: tuple = ()
+    seed_capacity: int = 0       # reference SeedArray policy; < 0 keeps every seed
+    tiebreak: int = TIE_REFERENCE
+
+    def struct(self) -> _Params:
+        p = _Params()
+        p.dc = self.dc
+        p.rhoc = self.rhoc
+        p.dm = self.dc if self.dm is None else self.dm
+        p.seed_dc = self.dc if self.seed_dc is None else self.seed_dc
+        p.points_per_tile = self.points_per_tile
+        for d, w in enumerate(self.wrapped):
+            p.wrapped[d] = 1 if w else 0
+        p.seed_capacity = self.seed_capacity
+        p.tiebreak = self.tiebreak
+        check(lib.clue_check_params(ctypes.byref(p)))
+        return p
+
+
+@dataclass
+class RunInfo:
+    n_seeds: int = 0
+    n_clusters: int = 0
+    dropped_seeds: int = 0
+    seed_capacity_used: int = 0
+    n_tiles: int = 0
+    n_per_dim: int = 0
+    label_rounds: int = 0
+
+
+@dataclass
+class Result:
+    cluster_index: object
+    is_seed: object = None
+    rho: object = None
+    nearest_higher: object = None
+    delta: object = None
+    info: RunInfo = field(default_factory=RunInfo)
+
+
+def grid_shape(n: int, points_per_tile: int, ndim: int) -> tuple[int, int]:
+    npd, nt = ctypes.c_int32(), ctypes.c_int32()
+    check(lib.clue_grid_shape(n, points_per_tile, ndim, ctypes.byref(npd), ctypes.byref(nt)))
+    return npd.value, nt.value
+
+
+def metric_eval(metric: Metric, a, b) -> float:
+    a = np.ascontiguousarray(a, np.float32)
+    b = np.ascontiguousarray(b, np.float32)
+    m = metric.struct(a.shape[0])
+    return lib.clue_metric_eval(ctypes.byref(m), a.shape[0], a.ctypes.data, b.ctypes.data)
+
+
+def kernel_eval(kernel: Kernel, dist: float, i: int, j: int) -> float:
+    return lib.clue_kernel_eval(ctypes.byref(kernel.struct()), dist, i, j)
+
+
+def device_count() -> int:
+    c = ctypes.c_int32()
+    st = lib.clue_device_count(ctypes.byref(c))
+    return c.value if st == OK else 0
+
+
+class Context:
+    """Reusable device workspace on one GPU (the Clusterer's tiles/seeds/followers)."""
+
+    def __init__(self, device: int = 0):
+        h = ctypes.c_void_p()
+        check(lib.clue_context_create(device, ctypes.byref(h)))
+        self.handle = h
+        self.device = device
+
+    def close(self):
+        if self.handle:
+            lib.clue_context_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def reserve(self, ndim: int, n: int, points_per_tile: int = 128):
+        check(lib.clue_context_reserve(self.handle, ndim, n, points_per_tile))
+
+    @property
+    def workspace_bytes(self) -> int:
+        return lib.clue_context_workspace_bytes(self.handle)
+
+    def make_clusters_host(self, coords: np.ndarray, weight: np.ndarray, params: Params,
+                           kernel: Kernel | None = None, metric: Metric | None = None,
+                           outputs: tuple = ("cluster_index", "is_seed", "rho", "nearest_higher",
+                                             "delta"), stream: int = 0) -> Result:
+        """Host (numpy) inputs and outputs; the library stages them through the device."""
+        c = np.ascontiguousarray(coords, dtype=np.float32)
+        if c.ndim == 1:
+            c = c[None, :]
+        ndim, n = c.shape
+        w = np.ascontiguousarray(weight, dtype=np.float32)
+        if w.shape != (n,):
+            raise ValueError("weight must have one entry per point")
+        res = Result(np.empty(n, np.int32))
+        out = _Outputs()
+        out.cluster_index = res.cluster_index.ctypes.data
+        for name, dt in (("is_seed", np.int32), ("rho", np.float32), ("nearest_higher", np.int32),
+                         ("delta", np.float32)):
+            if name in outputs:
+                arr = np.empty(n, dt)
+                setattr(res, name, arr)
+                setattr(out, name, arr.ctypes.data)
+        info = _RunInfo()
+        k = (kernel or FlatKernel(0.5)).struct()
+        m = (metric or Metric()).struct(ndim)
+        p = params.struct()
+        check(lib.clue_make_clusters(self.handle, ctypes.byref(p), ctypes.byref(k), ctypes.byref(m),
+                                     ndim, n, c.ctypes.data, w.ctypes.data, ctypes.byref(out),
+                                     MEM_HOST, ctypes.c_void_p(stream), ctypes.byref(info)))
+        res.info = RunInfo(**{f: getattr(info, f) for f, _ in _RunInfo._fields_})
+        return res
+
+    def make_clusters_device(self, coords_ptr: int, weight_ptr: int, ndim: int, n: int,
+                             out_ptrs: dict, params: Params, kernel: Kernel | None = None,
+                             metric: Metric | None = None, stream: int = 0,
+                             blocking: bool = True) -> RunInfo | None:
+        """Device pointers in and out (e.g. torch CUDA tensors' data_ptr())."""
+        out = _Outputs()
+        for name in ("cluster_index", "is_seed", "rho", "nearest_higher", "delta"):
+            setattr(out, name, out_ptrs.get(name) or None)
+        k = (kernel or FlatKernel(0.5)).struct()
+        m = (metric or Metric()).struct(ndim)
+        p = params.struct()
+        if blocking:
+            info = _RunInfo()
+            check(lib.clue_make_clusters(self.handle, ctypes.byref(p), ctypes.byref(k),
+                                         ctypes.byref(m), ndim, n, ctypes.c_void_p(coords_ptr),
+                                         ctypes.c_void_p(weight_ptr), ctypes.byref(out), MEM_DEVICE,
+                                         ctypes.c_void_p(stream), ctypes.byref(info)))
+            return RunInfo(**{f: getattr(info, f) for f, _ in _RunInfo._fields_})
+        check(lib.clue_make_clusters_async(self.handle, ctypes.byref(p), ctypes.byref(k),
+                                           ctypes.byref(m), ndim, n, ctypes.c_void_p(coords_ptr),
+                                           ctypes.c_void_p(weight_ptr), ctypes.byref(out),
+                                           ctypes.c_void_p(stream)))
+        return None
+
+    def set_timing(self, enable: bool = True):
+        check(lib.clue_context_set_timing(self.handle, 1 if enable else 0))
+
+    def stage_times(self) -> list[float]:
+        """Milliseconds of (tile build, density, nearest higher, seeds+labels) of the last run."""
+        arr = (ctypes.c_float * 4)()
+        check(lib.clue_context_stage_times(self.handle, arr, 4))
+        return list(arr)
+
+    @property
+    def kernel_launches(self) -> int:
+        return lib.clue_context_kernel_launches(self.handle)
+
+    def read_info(self, stream: int = 0) -> RunInfo:
+        info = _RunInfo()
+        check(lib.clue_context_read_info(self.handle, ctypes.c_void_p(stream), ctypes.byref(info)))
+        return RunInfo(**{f: getattr(info, f) for f, _ in _RunInfo._fields_})

@@ -1,0 +1,700 @@
+// clue_capi.cu -- the extern "C" entry points of libclue_b200.so (include/clue_b200.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "clue_internal.h"
+
+namespace clue_b200 {
+
+namespace {
+thread_local std::string g_last_error;
+}
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+template <int N>
+clue_status finish_labels(Workspace& ws, const RunArgs& a, cudaStream_t s, int first_round);
+
+#define CLUE_DECLARE_DIM(N)                                                      \
+  extern template clue_status run_pipeline<N>(Workspace&, const RunArgs&, cudaStream_t); \
+  extern template clue_status finish_labels<N>(Workspace&, const RunArgs&, cudaStream_t, int);
+CLUE_DECLARE_DIM(1)
+CLUE_DECLARE_DIM(2)
+CLUE_DECLARE_DIM(3)
+CLUE_DECLARE_DIM(4)
+CLUE_DECLARE_DIM(5)
+CLUE_DECLARE_DIM(6)
+CLUE_DECLARE_DIM(7)
+CLUE_DECLARE_DIM(8)
+CLUE_DECLARE_DIM(9)
+CLUE_DECLARE_DIM(10)
+
+clue_status run_pipeline_dispatch(Workspace& ws, const RunArgs& a, cudaStream_t s) {
+  switch (a.ndim) {
+    case 1: return run_pipeline<1>(ws, a, s);
+    case 2: return run_pipeline<2>(ws, a, s);
+    case 3: return run_pipeline<3>(ws, a, s);
+    case 4: return run_pipeline<4>(ws, a, s);
+    case 5: return run_pipeline<5>(ws, a, s);
+    case 6: return run_pipeline<6>(ws, a, s);
+    case 7: return run_pipeline<7>(ws, a, s);
+    case 8: return run_pipeline<8>(ws, a, s);
+    case 9: return run_pipeline<9>(ws, a, s);
+    case 10: return run_pipeline<10>(ws, a, s);
+  }
+  set_error("ndim must be in [1, 10]");
+  return CLUE_ERR_INVALID_ARG;
+}
+
+static clue_status finish_labels_dispatch(Workspace& ws, const RunArgs& a, cudaStream_t s, int first) {
+  switch (a.ndim) {
+    case 1: return finish_labels<1>(ws, a, s, first);
+    case 2: return finish_labels<2>(ws, a, s, first);
+    case 3: return finish_labels<3>(ws, a, s, first);
+    case 4: return finish_labels<4>(ws, a, s, first);
+    case 5: return finish_labels<5>(ws, a, s, first);
+    case 6: return finish_labels<6>(ws, a, s, first);
+    case 7: return finish_labels<7>(ws, a, s, first);
+    case 8: return finish_labels<8>(ws, a, s, first);
+    case 9: return finish_labels<9>(ws, a, s, first);
+    case 10: return finish_labels<10>(ws, a, s, first);
+  }
+  return CLUE_ERR_INVALID_ARG;
+}
+
+// core/detail/SetupTiles.hpp:23-26.
+void grid_shape(int32_t n, int32_t ppbin, int32_t ndim, int32_t* nperdim, int32_t* ntiles) {
+  const int32_t t0 = (int32_t)std::ceil((float)n / (float)ppbin);
+  const int32_t npd = (int32_t)std::ceil(std::pow((double)t0, 1.0 / (double)ndim));
+  *nperdim = npd;
+  *ntiles = (int32_t)std::pow((double)npd, (double)ndim);
+}
+
+// Largest s with sqrtf(s) <= r (sqrtf is correctly rounded on host and device, so
+// `s <= threshold_for(r)` decides exactly what `sqrtf(s) <= r` decides); r itself for
+// metrics without a square root.
+float threshold_for(float r, bool root) {
+  if (!root) return r;
+  float s = (float)((double)r * (double)r);
+  if (!std::isfinite(s)) s = FLT_MAX;
+  while (s > 0.0f && std::sqrt(s) > r) s = std::nextafter(s, 0.0f);
+  while (true) {
+    const float nx = std::nextafter(s, INFINITY);
+    if (std::isfinite(nx) && std::sqrt(nx) <= r)
+      s = nx;
+    else
+      break;
+  }
+  return s;
+}
+
+static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+clue_status workspace_reserve(Workspace& ws, int ndim, size_t n, size_t ntiles) {
+  const size_t words = (size_t)((ndim + 1 + 3) / 4);
+  if (n <= ws.cap_n && ntiles <= ws.cap_tiles && words <= ws.cap_words && ws.arena) return CLUE_OK;
+  n = std::max(n, ws.cap_n);
+  ntiles = std::max(ntiles, ws.cap_tiles);
+  const size_t w = std::max(words, ws.cap_words);
+  const size_t nb = (size_t)sort_blocks((int)n);
+  const size_t hist_len = (size_t)kRadix * nb;
+  const size_t scan_words = scan_scratch_words(std::max(hist_len, n)) + 1;
+  struct Item {
+    void** ptr;
+    size_t bytes;
+  };
+  Workspace nw = ws;
+  Item items[] = {
+      {(void**)&nw.grid, sizeof(DevGrid)},
+      {(void**)&nw.status, sizeof(DevStatus)},
+      {(void**)&nw.keys[0], n * 4},
+      {(void**)&nw.keys[1], n * 4},
+      {(void**)&nw.vals[0], n * 4},
+      {(void**)&nw.vals[1], n * 4},
+      {(void**)&nw.hist, hist_len * 4},
+      {(void**)&nw.scan_scratch, scan_words * 4},
+      {(void**)&nw.offsets, (ntiles + 1) * 4},
+      {(void**)&nw.rec_w, n * w * 16},
+      {(void**)&nw.rec_r, n * w * 16},
+      {(void**)&nw.delta_s, n * 4},
+      {(void**)&nw.nh_s, n * 4},
+      {(void**)&nw.par, n * 4},
+      {(void**)&nw.is_seed_s, n * 4},
+      {(void**)&nw.seed_flag, n * 4},
+      {(void**)&nw.seed_total, 16},
+  };
+  size_t total = 0;
+  for (auto& it : items) total = align_up(total, 256) + align_up(it.bytes, 256);
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(ws.device);
+  if (ws.arena) {
+    cudaDeviceSynchronize();
+    cudaFree(ws.arena);
+    ws.arena = nullptr;
+  }
+  void* arena = nullptr;
+  cudaError_t e = cudaMalloc(&arena, total);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    cudaSetDevice(prev);
+    ws.cap_n = ws.cap_tiles = ws.cap_words = 0;
+    set_error(std::string("workspace allocation of ") + std::to_string(total) + " bytes failed: " +
+              cudaGetErrorString(e));
+    return CLUE_ERR_OUT_OF_MEMORY;
+  }
+  size_t offset = 0;
+  for (auto& it : items) {
+    offset = align_up(offset, 256);
+    *it.ptr = static_cast<char*>(arena) + offset;
+    offset += align_up(it.bytes, 256);
+  }
+  nw.arena = arena;
+  nw.arena_bytes = total;
+  nw.cap_n = n;
+  nw.cap_tiles = ntiles;
+  nw.cap_words = w;
+  if (!nw.status_host) {
+    e = cudaMallocHost((void**)&nw.status_host, sizeof(DevStatus) + 64);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      cudaSetDevice(prev);
+      set_error("pinned status allocation failed");
+      return CLUE_ERR_OUT_OF_MEMORY;
+    }
+  }
+  ws = nw;
+  cudaSetDevice(prev);
+  return CLUE_OK;
+}
+
+static clue_status reserve_stage(Workspace& ws, size_t bytes) {
+  if (bytes <= ws.dstage_bytes) return CLUE_OK;
+  if (ws.dstage) {
+    cudaDeviceSynchronize();
+    cudaFree(ws.dstage);
+    ws.dstage = nullptr;
+    ws.dstage_bytes = 0;
+  }
+  CLUE_CUDA_TRY(cudaMalloc(&ws.dstage, bytes));
+  ws.dstage_bytes = bytes;
+  return CLUE_OK;
+}
+
+void workspace_release(Workspace& ws) {
+  for (auto& e : ws.ev)
+    if (e) cudaEventDestroy(e);
+  if (ws.arena) cudaFree(ws.arena);
+  if (ws.dstage) cudaFree(ws.dstage);
+  if (ws.status_host) cudaFreeHost(ws.status_host);
+  ws = Workspace{};
+}
+
+static clue_status check_finite(float v, const char* what) {
+  if (!std::isfinite(v)) {
+    set_error(std::string(what) + " must be finite");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  return CLUE_OK;
+}
+
+template <int N>
+float metric_eval_n(int32_t type, const float* a, const float* b, const float* par) {
+  switch (type) {
+    case CLUE_METRIC_EUCLIDEAN: {
+      using M = Metric<N, CLUE_METRIC_EUCLIDEAN>;
+      return M::finish(M::partial(a, b, par));
+    }
+    case CLUE_METRIC_WEIGHTED_EUCLIDEAN: {
+      using M = Metric<N, CLUE_METRIC_WEIGHTED_EUCLIDEAN>;
+      return M::finish(M::partial(a, b, par));
+    }
+    case CLUE_METRIC_PERIODIC_EUCLIDEAN: {
+      using M = Metric<N, CLUE_METRIC_PERIODIC_EUCLIDEAN>;
+      return M::finish(M::partial(a, b, par));
+    }
+    case CLUE_METRIC_MANHATTAN: {
+      using M = Metric<N, CLUE_METRIC_MANHATTAN>;
+      return M::finish(M::partial(a, b, par));
+    }
+    case CLUE_METRIC_CHEBYSHEV: {
+      using M = Metric<N, CLUE_METRIC_CHEBYSHEV>;
+      return M::finish(M::partial(a, b, par));
+    }
+    default: {
+      using M = Metric<N, CLUE_METRIC_WEIGHTED_CHEBYSHEV>;
+      return M::finish(M::partial(a, b, par));
+    }
+  }
+}
+
+}  // namespace clue_b200
+
+using namespace clue_b200;
+
+struct clue_context_s {
+  Workspace ws;
+};
+
+extern "C" {
+
+int32_t clue_abi_version(void) { return CLUE_ABI_VERSION; }
+
+const char* clue_last_error(void) { return g_last_error.c_str(); }
+
+const char* clue_status_string(clue_status s) {
+  switch (s) {
+    case CLUE_OK: return "ok";
+    case CLUE_ERR_INVALID_ARG: return "invalid argument";
+    case CLUE_ERR_OUT_OF_MEMORY: return "out of memory";
+    case CLUE_ERR_CAPACITY: return "capacity exceeded";
+    case CLUE_ERR_TIMEOUT: return "timeout";
+    case CLUE_ERR_CUDA: return "cuda error";
+    case CLUE_ERR_NOT_SUPPORTED: return "not supported";
+    case CLUE_ERR_NONFINITE: return "non-finite input";
+    case CLUE_ERR_OUT_OF_RANGE: return "out of range";
+  }
+  return "unknown";
+}
+
+clue_status clue_check_params(const clue_params* p) {
+  if (!p) {
+    set_error("params is null");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  for (float v : {p->dc, p->rhoc, p->dm, p->seed_dc})
+    if (check_finite(v, "clustering parameters") != CLUE_OK) return CLUE_ERR_INVALID_ARG;
+  if (p->dc <= 0.f || p->rhoc < 0.f || p->dm <= 0.f || p->seed_dc <= 0.f || p->points_per_tile <= 0) {
+    set_error("Invalid clustering parameters. The parameters must be positive.");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  if (p->tiebreak != CLUE_TIE_REFERENCE && p->tiebreak != CLUE_TIE_RHO_INDEX) {
+    set_error("unknown tiebreak");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  return CLUE_OK;
+}
+
+clue_status clue_check_kernel(const clue_kernel* k) {
+  if (!k) {
+    set_error("kernel is null");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  switch (k->type) {
+    case CLUE_KERNEL_FLAT:
+      if (!(k->par[0] > 0.f) || !std::isfinite(k->par[0])) {
+        set_error("Flat kernel parameter must be positive.");
+        return CLUE_ERR_INVALID_ARG;
+      }
+      return CLUE_OK;
+    case CLUE_KERNEL_EXPONENTIAL:
+      if (!(k->par[0] > 0.f) || !(k->par[1] > 0.f) || !std::isfinite(k->par[0]) || !std::isfinite(k->par[1])) {
+        set_error("Exponential kernel parameters must be positive.");
+        return CLUE_ERR_INVALID_ARG;
+      }
+      return CLUE_OK;
+    case CLUE_KERNEL_GAUSSIAN:
+      if (!(k->par[0] >= 0.f) || !(k->par[1] > 0.f) || !(k->par[2] > 0.f) || !std::isfinite(k->par[0]) ||
+          !std::isfinite(k->par[1]) || !std::isfinite(k->par[2])) {
+        set_error("Gaussian kernel parameters must be positive (mean may be 0).");
+        return CLUE_ERR_INVALID_ARG;
+      }
+      return CLUE_OK;
+  }
+  set_error("unknown kernel type");
+  return CLUE_ERR_INVALID_ARG;
+}
+
+clue_status clue_check_metric(const clue_metric* m, int32_t ndim) {
+  if (!m) {
+    set_error("metric is null");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  if (m->type < CLUE_METRIC_EUCLIDEAN || m->type > CLUE_METRIC_WEIGHTED_CHEBYSHEV) {
+    set_error("unknown metric type");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  if (ndim < 1 || ndim > CLUE_MAX_DIM) {
+    set_error("ndim must be in [1, 10]");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  for (int d = 0; d < ndim; ++d)
+    if (!std::isfinite(m->par[d])) {
+      set_error("metric parameters must be finite");
+      return CLUE_ERR_INVALID_ARG;
+    }
+  return CLUE_OK;
+}
+
+clue_status clue_grid_shape(int32_t n, int32_t ppbin, int32_t ndim, int32_t* n_per_dim, int32_t* n_tiles) {
+  if (n <= 0 || ppbin <= 0 || ndim < 1 || ndim > CLUE_MAX_DIM || !n_per_dim || !n_tiles) {
+    set_error("invalid grid request");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  grid_shape(n, ppbin, ndim, n_per_dim, n_tiles);
+  return CLUE_OK;
+}
+
+float clue_metric_eval(const clue_metric* m, int32_t ndim, const float* a, const float* b) {
+  if (!m || !a || !b) return NAN;
+  switch (ndim) {
+    case 1: return metric_eval_n<1>(m->type, a, b, m->par);
+    case 2: return metric_eval_n<2>(m->type, a, b, m->par);
+    case 3: return metric_eval_n<3>(m->type, a, b, m->par);
+    case 4: return metric_eval_n<4>(m->type, a, b, m->par);
+    case 5: return metric_eval_n<5>(m->type, a, b, m->par);
+    case 6: return metric_eval_n<6>(m->type, a, b, m->par);
+    case 7: return metric_eval_n<7>(m->type, a, b, m->par);
+    case 8: return metric_eval_n<8>(m->type, a, b, m->par);
+    case 9: return metric_eval_n<9>(m->type, a, b, m->par);
+    case 10: return metric_eval_n<10>(m->type, a, b, m->par);
+  }
+  return NAN;
+}
+
+float clue_kernel_eval(const clue_kernel* k, float dist, int32_t i, int32_t j) {
+  if (!k) return NAN;
+  if (i == j) return 1.0f;
+  return kernel_value(k->type, k->par, dist);
+}
+
+clue_status clue_device_count(int32_t* count) {
+  int c = 0;
+  cudaError_t e = cudaGetDeviceCount(&c);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    *count = 0;
+    set_error(std::string("cudaGetDeviceCount: ") + cudaGetErrorString(e));
+    return CLUE_ERR_CUDA;
+  }
+  *count = c;
+  return CLUE_OK;
+}
+
+clue_status clue_device_alloc(int32_t device, size_t bytes, void** ptr) {
+  if (!ptr) return CLUE_ERR_INVALID_ARG;
+  int prev = 0;
+  CLUE_CUDA_TRY(cudaGetDevice(&prev));
+  CLUE_CUDA_TRY(cudaSetDevice(device));
+  cudaError_t e = cudaMalloc(ptr, bytes ? bytes : 1);
+  cudaSetDevice(prev);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    set_error(std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? CLUE_ERR_OUT_OF_MEMORY : CLUE_ERR_CUDA;
+  }
+  return CLUE_OK;
+}
+
+clue_status clue_device_free(void* ptr) {
+  CLUE_CUDA_TRY(cudaFree(ptr));
+  return CLUE_OK;
+}
+
+clue_status clue_host_alloc_pinned(size_t bytes, void** ptr) {
+  if (!ptr) return CLUE_ERR_INVALID_ARG;
+  CLUE_CUDA_TRY(cudaMallocHost(ptr, bytes ? bytes : 1));
+  return CLUE_OK;
+}
+
+clue_status clue_host_free_pinned(void* ptr) {
+  CLUE_CUDA_TRY(cudaFreeHost(ptr));
+  return CLUE_OK;
+}
+
+clue_status clue_memcpy_htod(void* dst, const void* src, size_t bytes, void* stream) {
+  CLUE_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, (cudaStream_t)stream));
+  return CLUE_OK;
+}
+clue_status clue_memcpy_dtoh(void* dst, const void* src, size_t bytes, void* stream) {
+  CLUE_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+  return CLUE_OK;
+}
+clue_status clue_memcpy_dtod(void* dst, const void* src, size_t bytes, void* stream) {
+  CLUE_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, (cudaStream_t)stream));
+  return CLUE_OK;
+}
+clue_status clue_stream_create(int32_t device, void** stream) {
+  int prev = 0;
+  CLUE_CUDA_TRY(cudaGetDevice(&prev));
+  CLUE_CUDA_TRY(cudaSetDevice(device));
+  cudaStream_t s;
+  cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  cudaSetDevice(prev);
+  if (e != cudaSuccess) {
+    set_error(cudaGetErrorString(e));
+    return CLUE_ERR_CUDA;
+  }
+  *stream = (void*)s;
+  return CLUE_OK;
+}
+clue_status clue_stream_destroy(void* stream) {
+  CLUE_CUDA_TRY(cudaStreamDestroy((cudaStream_t)stream));
+  return CLUE_OK;
+}
+clue_status clue_stream_synchronize(void* stream) {
+  CLUE_CUDA_TRY(cudaStreamSynchronize((cudaStream_t)stream));
+  return CLUE_OK;
+}
+
+clue_status clue_context_create(int32_t device, clue_context* ctx) {
+  if (!ctx) return CLUE_ERR_INVALID_ARG;
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || device < 0 || device >= count) {
+    cudaGetLastError();
+    set_error("no CUDA device with id " + std::to_string(device));
+    return CLUE_ERR_CUDA;
+  }
+  auto* c = new (std::nothrow) clue_context_s;
+  if (!c) return CLUE_ERR_OUT_OF_MEMORY;
+  c->ws.device = device;
+  *ctx = c;
+  return CLUE_OK;
+}
+
+clue_status clue_context_destroy(clue_context ctx) {
+  if (!ctx) return CLUE_OK;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(ctx->ws.device);
+  workspace_release(ctx->ws);
+  cudaSetDevice(prev);
+  delete ctx;
+  return CLUE_OK;
+}
+
+clue_status clue_context_reserve(clue_context ctx, int32_t ndim, int32_t n, int32_t ppbin) {
+  if (!ctx || n <= 0 || ppbin <= 0 || ndim < 1 || ndim > CLUE_MAX_DIM) {
+    set_error("invalid reserve request");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  int32_t npd, nt;
+  grid_shape(n, ppbin, ndim, &npd, &nt);
+  return workspace_reserve(ctx->ws, ndim, (size_t)n, (size_t)nt);
+}
+
+size_t clue_context_workspace_bytes(clue_context ctx) { return ctx ? ctx->ws.arena_bytes + ctx->ws.dstage_bytes : 0; }
+
+}  // extern "C"
+
+namespace clue_b200 {
+
+static clue_status prepare(clue_context ctx, const clue_params* params, const clue_kernel* kernel,
+                           const clue_metric* metric, int32_t ndim, int32_t n, const float* coords,
+                           const float* weight, const clue_outputs* out, RunArgs& a) {
+  if (!ctx) {
+    set_error("context is null");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  clue_status st;
+  if ((st = clue_check_params(params)) != CLUE_OK) return st;
+  if ((st = clue_check_kernel(kernel)) != CLUE_OK) return st;
+  if ((st = clue_check_metric(metric, ndim)) != CLUE_OK) return st;
+  if (n <= 0) {
+    set_error("Number of points must be positive.");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  if (!coords || !weight || !out || !out->cluster_index) {
+    set_error("coords, weight and out->cluster_index must be non-null");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  int32_t npd, nt;
+  grid_shape(n, params->points_per_tile, ndim, &npd, &nt);
+  if (npd <= 0 || nt <= 0 || (double)nt > 2147483000.0) {
+    set_error("tile grid too large");
+    return CLUE_ERR_CAPACITY;
+  }
+  KParams& kp = a.kp;
+  std::memset(&kp, 0, sizeof(kp));
+  const bool root = metric->type == CLUE_METRIC_EUCLIDEAN || metric->type == CLUE_METRIC_WEIGHTED_EUCLIDEAN ||
+                    metric->type == CLUE_METRIC_PERIODIC_EUCLIDEAN;
+  kp.dc = params->dc;
+  kp.dm = params->dm;
+  kp.seed_dc = params->seed_dc;
+  kp.rhoc = params->rhoc;
+  kp.t_dc = threshold_for(params->dc, root);
+  kp.t_dm = threshold_for(params->dm, root);
+  kp.kernel_type = kernel->type;
+  for (int k = 0; k < 3; ++k) kp.kpar[k] = kernel->par[k];
+  for (int d = 0; d < ndim; ++d) kp.mpar[d] = metric->par[d];
+  kp.nperdim = npd;
+  kp.ntiles = nt;
+  int64_t s = 1;
+  for (int d = ndim - 1; d >= 0; --d) {
+    kp.stride[d] = (int32_t)s;
+    s *= npd;
+  }
+  for (int d = 0; d < ndim; ++d) kp.wrapped[d] = params->wrapped[d] ? 1 : 0;
+  kp.tiebreak = params->tiebreak;
+  kp.seed_capacity = params->seed_capacity;
+  kp.n = n;
+  a.ndim = ndim;
+  a.n = n;
+  a.metric = metric->type;
+  for (int d = 0; d < ndim; ++d) a.coords[d] = coords + (size_t)d * n;
+  a.weight = weight;
+  a.out = *out;
+  ctx->ws.last_kp = kp;
+  return workspace_reserve(ctx->ws, ndim, (size_t)n, (size_t)nt);
+}
+
+static clue_status read_info(Workspace& ws, const KParams& kp, cudaStream_t s, clue_run_info* info,
+                             bool& unresolved) {
+  DevStatus* h = ws.status_host;
+  uint32_t* total = reinterpret_cast<uint32_t*>(h + 1);
+  CLUE_CUDA_TRY(cudaMemcpyAsync(h, ws.status, sizeof(DevStatus), cudaMemcpyDeviceToHost, s));
+  CLUE_CUDA_TRY(cudaMemcpyAsync(total, ws.seed_total, 4, cudaMemcpyDeviceToHost, s));
+  CLUE_CUDA_TRY(cudaStreamSynchronize(s));
+  unresolved = h->unresolved[3] != 0;
+  if (h->nonfinite) {
+    set_error("coordinates or weights contain NaN or Inf");
+    return CLUE_ERR_NONFINITE;
+  }
+  if (info) {
+    const int64_t nseeds = *total;
+    const int64_t cap = kp.seed_capacity < 0 ? -1
+                                             : std::max<int64_t>(kp.seed_capacity, (int64_t)h->seed_candidates);
+    info->n_seeds = nseeds;
+    info->n_clusters = cap < 0 ? nseeds : std::min(nseeds, cap);
+    info->dropped_seeds = nseeds - info->n_clusters;
+    info->seed_capacity_used = cap;
+    info->n_tiles = kp.ntiles;
+    info->n_per_dim = kp.nperdim;
+    info->label_rounds = h->label_rounds;
+  }
+  return CLUE_OK;
+}
+
+}  // namespace clue_b200
+
+extern "C" {
+
+clue_status clue_make_clusters(clue_context ctx, const clue_params* params, const clue_kernel* kernel,
+                               const clue_metric* metric, int32_t ndim, int32_t n, const float* coords,
+                               const float* weight, const clue_outputs* out, int32_t memory, void* stream,
+                               clue_run_info* info) {
+  RunArgs a;
+  clue_status st = prepare(ctx, params, kernel, metric, ndim, n, coords, weight, out, a);
+  if (st != CLUE_OK) return st;
+  Workspace& ws = ctx->ws;
+  int prev = 0;
+  CLUE_CUDA_TRY(cudaGetDevice(&prev));
+  CLUE_CUDA_TRY(cudaSetDevice(ws.device));
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t nn = (size_t)n;
+  clue_outputs dev_out = *out;
+  if (memory == CLUE_MEM_HOST) {
+    // device staging: coords, weight, then the five outputs
+    st = reserve_stage(ws, (nn * (size_t)(ndim + 1) + 5 * nn) * 4);
+    if (st != CLUE_OK) {
+      cudaSetDevice(prev);
+      return st;
+    }
+    float* dcoords = static_cast<float*>(ws.dstage);
+    float* dweight = dcoords + nn * ndim;
+    int32_t* o = reinterpret_cast<int32_t*>(dweight + nn);
+    CLUE_CUDA_TRY(cudaMemcpyAsync(dcoords, coords, nn * ndim * 4, cudaMemcpyHostToDevice, s));
+    CLUE_CUDA_TRY(cudaMemcpyAsync(dweight, weight, nn * 4, cudaMemcpyHostToDevice, s));
+    for (int d = 0; d < ndim; ++d) a.coords[d] = dcoords + (size_t)d * nn;
+    a.weight = dweight;
+    dev_out.cluster_index = o;
+    dev_out.is_seed = out->is_seed ? o + nn : nullptr;
+    dev_out.rho = out->rho ? reinterpret_cast<float*>(o + 2 * nn) : nullptr;
+    dev_out.nearest_higher = out->nearest_higher ? o + 3 * nn : nullptr;
+    dev_out.delta = out->delta ? reinterpret_cast<float*>(o + 4 * nn) : nullptr;
+    a.out = dev_out;
+  }
+  st = run_pipeline_dispatch(ws, a, s);
+  bool unresolved = false;
+  if (st == CLUE_OK) st = read_info(ws, a.kp, s, info, unresolved);
+  if (st == CLUE_OK && unresolved) {
+    st = finish_labels_dispatch(ws, a, s, 4);
+    if (st == CLUE_OK) st = read_info(ws, a.kp, s, info, unresolved);
+  }
+  if (st == CLUE_OK && memory == CLUE_MEM_HOST) {
+    auto back = [&](void* dst, const void* src) -> cudaError_t {
+      return dst ? cudaMemcpyAsync(dst, src, nn * 4, cudaMemcpyDeviceToHost, s) : cudaSuccess;
+    };
+    cudaError_t e = back(out->cluster_index, dev_out.cluster_index);
+    if (e == cudaSuccess) e = back(out->is_seed, dev_out.is_seed);
+    if (e == cudaSuccess) e = back(out->rho, dev_out.rho);
+    if (e == cudaSuccess) e = back(out->nearest_higher, dev_out.nearest_higher);
+    if (e == cudaSuccess) e = back(out->delta, dev_out.delta);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+      set_error(std::string("copy back: ") + cudaGetErrorString(e));
+      st = CLUE_ERR_CUDA;
+    }
+  }
+  cudaSetDevice(prev);
+  return st;
+}
+
+clue_status clue_make_clusters_async(clue_context ctx, const clue_params* params, const clue_kernel* kernel,
+                                     const clue_metric* metric, int32_t ndim, int32_t n, const float* coords,
+                                     const float* weight, const clue_outputs* out, void* stream) {
+  RunArgs a;
+  clue_status st = prepare(ctx, params, kernel, metric, ndim, n, coords, weight, out, a);
+  if (st != CLUE_OK) return st;
+  return run_pipeline_dispatch(ctx->ws, a, (cudaStream_t)stream);
+}
+
+clue_status clue_context_read_info(clue_context ctx, void* stream, clue_run_info* info) {
+  if (!ctx || !ctx->ws.arena) {
+    set_error("context has no completed run");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  bool unresolved = false;
+  clue_status st = read_info(ctx->ws, ctx->ws.last_kp, (cudaStream_t)stream, info, unresolved);
+  if (st == CLUE_OK && unresolved) {
+    set_error("nearest-higher chains deeper than the enqueued label rounds; use clue_make_clusters");
+    return CLUE_ERR_TIMEOUT;
+  }
+  return st;
+}
+
+clue_status clue_context_set_timing(clue_context ctx, int32_t enable) {
+  if (!ctx) return CLUE_ERR_INVALID_ARG;
+  int prev = 0;
+  CLUE_CUDA_TRY(cudaGetDevice(&prev));
+  CLUE_CUDA_TRY(cudaSetDevice(ctx->ws.device));
+  for (auto& e : ctx->ws.ev)
+    if (!e) {
+      cudaError_t err = cudaEventCreate(&e);
+      if (err != cudaSuccess) {
+        cudaSetDevice(prev);
+        set_error(cudaGetErrorString(err));
+        return CLUE_ERR_CUDA;
+      }
+    }
+  ctx->ws.timing = enable != 0;
+  cudaSetDevice(prev);
+  return CLUE_OK;
+}
+
+clue_status clue_context_stage_times(clue_context ctx, float* ms, int32_t n_stages) {
+  if (!ctx || !ms || !ctx->ws.ev[CLUE_N_STAGES]) {
+    set_error("timing not enabled");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  CLUE_CUDA_TRY(cudaEventSynchronize(ctx->ws.ev[CLUE_N_STAGES]));
+  for (int k = 0; k < n_stages && k < CLUE_N_STAGES; ++k)
+    CLUE_CUDA_TRY(cudaEventElapsedTime(&ms[k], ctx->ws.ev[k], ctx->ws.ev[k + 1]));
+  return CLUE_OK;
+}
+
+uint64_t clue_context_kernel_launches(clue_context ctx) { return ctx ? ctx->ws.launches : 0; }
+
+clue_status clue_get_clusters(clue_context, int32_t, const int32_t*, int32_t*, int32_t*, int32_t*, int32_t*,
+                              void*) {
+  set_error("clue_get_clusters: not built yet");
+  return CLUE_ERR_NOT_SUPPORTED;
+}
+
+}  // extern "C"

@@ -1,0 +1,248 @@
+// clue_common.cuh -- definitions shared by host and device code of libclue_b200.
+//
+// The binning, metric and kernel arithmetic restates the reference bit for bit:
+// every float operation is a separately rounded IEEE op (explicit __f*_rn
+// intrinsics on the device, -ffp-contract=off on the host), in the order the
+// reference's headers write it.  References are to the reference project's
+// include/CLUEstering/ tree.
+#pragma once
+
+#include <cstdint>
+#include <cfloat>
+#include <cmath>
+
+#include "../../include/clue_b200.h"
+
+#if defined(__CUDACC__)
+#define CLUE_HD __host__ __device__ __forceinline__
+#else
+#define CLUE_HD inline
+#endif
+
+namespace clue_b200 {
+
+constexpr int kMaxDim = CLUE_MAX_DIM;
+
+// Number of float4 words of one tile-sorted point record: N coordinates followed by
+// one payload float (the weight in the density record, rho in the nearest-higher
+// record), payload in the last float of the last word.
+template <int N>
+struct Rec {
+  static constexpr int kWords = (N + 1 + 3) / 4;
+  static constexpr int kPayload = 4 * kWords - 1;
+};
+
+// Host-computed launch parameters, passed by value to every kernel.
+struct KParams {
+  float dc, dm, seed_dc, rhoc;
+  float t_dc, t_dm;  // thresholds on the metric's pre-root value (see threshold_for)
+  int32_t kernel_type;
+  float kpar[3];
+  float mpar[kMaxDim];
+  int32_t nperdim;
+  int32_t ntiles;
+  int32_t stride[kMaxDim];
+  uint8_t wrapped[kMaxDim];
+  int32_t tiebreak;
+  int64_t seed_capacity;
+  int32_t n;
+};
+
+// Tile grid geometry produced on the device from the bounding box.
+struct DevGrid {
+  uint32_t enc_min[kMaxDim];
+  uint32_t enc_max[kMaxDim];
+  float mn[kMaxDim];
+  float mx[kMaxDim];
+  float size[kMaxDim];
+};
+
+// Device-side status block (counters and flags), read back once per call.
+struct DevStatus {
+  uint32_t nonfinite;
+  uint32_t seed_candidates;  // points with no nearest higher (before the seed reset)
+  uint32_t n_seeds;
+  uint32_t unresolved[64];   // label rounds that left an unresolved parent chain
+  uint32_t label_rounds;
+  uint32_t pad[3];
+};
+
+// float -> int32 truncation with x86 cvttss2si semantics (NaN and out-of-range give
+// INT32_MIN), which is what the reference's static_cast<int>(float) does on its
+// serial CPU backend (data_structures/internal/TilesView.hpp:41-43,95).
+CLUE_HD int32_t cvt_i32(float f) {
+  if (!(f > -2147483904.0f && f < 2147483648.0f)) return INT32_MIN;
+  return (int32_t)f;
+}
+
+// Monotone float <-> uint32 encoding for atomic min/max.
+CLUE_HD uint32_t enc_float(float f) {
+#if defined(__CUDA_ARCH__)
+  uint32_t u = __float_as_uint(f);
+#else
+  uint32_t u;
+  __builtin_memcpy(&u, &f, 4);
+#endif
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+CLUE_HD float dec_float(uint32_t e) {
+  uint32_t u = (e & 0x80000000u) ? (e & 0x7fffffffu) : ~e;
+#if defined(__CUDA_ARCH__)
+  return __uint_as_float(u);
+#else
+  float f;
+  __builtin_memcpy(&f, &u, 4);
+  return f;
+#endif
+}
+
+// Separately rounded float ops (never contracted into FMA).
+#if defined(__CUDA_ARCH__)
+CLUE_HD float fadd(float a, float b) { return __fadd_rn(a, b); }
+CLUE_HD float fsub(float a, float b) { return __fsub_rn(a, b); }
+CLUE_HD float fmul(float a, float b) { return __fmul_rn(a, b); }
+CLUE_HD float fdiv(float a, float b) { return __fdiv_rn(a, b); }
+CLUE_HD float fsqrt(float a) { return __fsqrt_rn(a); }
+#else
+CLUE_HD float fadd(float a, float b) { return a + b; }
+CLUE_HD float fsub(float a, float b) { return a - b; }
+CLUE_HD float fmul(float a, float b) { return a * b; }
+CLUE_HD float fdiv(float a, float b) { return a / b; }
+CLUE_HD float fsqrt(float a) { return sqrtf(a); }
+#endif
+
+// ---- tile grid (data_structures/internal/TilesView.hpp) ---------------------
+
+// normalizeCoordinate, TilesView.hpp:93-101.
+CLUE_HD float normalize_coord(float coord, float mn, float mx) {
+  const float range = fsub(mx, mn);
+  float rem = fsub(coord, fmul((float)cvt_i32(fdiv(coord, range)), range));
+  if (rem >= mx)
+    rem = fsub(rem, range);
+  else if (rem < mn)
+    rem = fadd(rem, range);
+  return rem;
+}
+
+// getBin, TilesView.hpp:37-51.
+CLUE_HD int32_t get_bin(float coord, float mn, float mx, float size, bool wrapped, int32_t nperdim) {
+  int32_t b;
+  if (wrapped)
+    b = cvt_i32(fdiv(fsub(normalize_coord(coord, mn, mx), mn), size));
+  else
+    b = cvt_i32(fdiv(fsub(coord, mn), size));
+  b = b < nperdim - 1 ? b : nperdim - 1;
+  b = b > 0 ? b : 0;
+  return b;
+}
+
+// ---- distance metrics (core/DistanceMetrics.hpp:33-230) ---------------------
+// partial() returns the value before the final square root, summed as
+// meta::accumulate's right fold t0 + (t1 + (... + (t_{N-1} + 0))) or, for the
+// Chebyshev family, meta::maximum's left-to-right std::max starting from 0.
+// finish() applies the square root where the reference takes one.
+
+template <int N, int MT>
+struct Metric;
+
+template <int N>
+struct Metric<N, CLUE_METRIC_EUCLIDEAN> {
+  static constexpr bool kRoot = true;
+  CLUE_HD static float partial(const float* a, const float* b, const float*) {
+    float acc = 0.0f;
+#pragma unroll
+    for (int d = N - 1; d >= 0; --d) {
+      const float t = fmul(fsub(a[d], b[d]), fsub(a[d], b[d]));
+      acc = fadd(t, acc);
+    }
+    return acc;
+  }
+  CLUE_HD static float finish(float s) { return fsqrt(s); }
+};
+
+template <int N>
+struct Metric<N, CLUE_METRIC_WEIGHTED_EUCLIDEAN> {
+  static constexpr bool kRoot = true;
+  CLUE_HD static float partial(const float* a, const float* b, const float* w) {
+    float acc = 0.0f;
+#pragma unroll
+    for (int d = N - 1; d >= 0; --d) {
+      const float t = fmul(fmul(w[d], fsub(a[d], b[d])), fsub(a[d], b[d]));
+      acc = fadd(t, acc);
+    }
+    return acc;
+  }
+  CLUE_HD static float finish(float s) { return fsqrt(s); }
+};
+
+template <int N>
+struct Metric<N, CLUE_METRIC_PERIODIC_EUCLIDEAN> {
+  static constexpr bool kRoot = true;
+  CLUE_HD static float partial(const float* a, const float* b, const float* period) {
+    float acc = 0.0f;
+#pragma unroll
+    for (int d = N - 1; d >= 0; --d) {
+      const float diff = fabsf(fsub(a[d], b[d]));
+      const float alt = fsub(period[d], diff);
+      const float pd = alt < diff ? alt : diff;
+      acc = fadd(fmul(pd, pd), acc);
+    }
+    return acc;
+  }
+  CLUE_HD static float finish(float s) { return fsqrt(s); }
+};
+
+template <int N>
+struct Metric<N, CLUE_METRIC_MANHATTAN> {
+  static constexpr bool kRoot = false;
+  CLUE_HD static float partial(const float* a, const float* b, const float*) {
+    float acc = 0.0f;
+#pragma unroll
+    for (int d = N - 1; d >= 0; --d) acc = fadd(fabsf(fsub(a[d], b[d])), acc);
+    return acc;
+  }
+  CLUE_HD static float finish(float s) { return s; }
+};
+
+template <int N>
+struct Metric<N, CLUE_METRIC_CHEBYSHEV> {
+  static constexpr bool kRoot = false;
+  CLUE_HD static float partial(const float* a, const float* b, const float*) {
+    float m = 0.0f;
+#pragma unroll
+    for (int d = 0; d < N; ++d) {
+      const float t = fabsf(fsub(a[d], b[d]));
+      m = (m < t) ? t : m;
+    }
+    return m;
+  }
+  CLUE_HD static float finish(float s) { return s; }
+};
+
+template <int N>
+struct Metric<N, CLUE_METRIC_WEIGHTED_CHEBYSHEV> {
+  static constexpr bool kRoot = false;
+  CLUE_HD static float partial(const float* a, const float* b, const float* w) {
+    float m = 0.0f;
+#pragma unroll
+    for (int d = 0; d < N; ++d) {
+      const float t = fmul(w[d], fabsf(fsub(a[d], b[d])));
+      m = (m < t) ? t : m;
+    }
+    return m;
+  }
+  CLUE_HD static float finish(float s) { return s; }
+};
+
+// ---- convolutional kernels (core/detail/ConvolutionalKernel.hpp:16-65) -------
+// Value for a pair of distinct points; the self pair (i == j) is 1.
+CLUE_HD float kernel_value(int32_t type, const float* k, float dist) {
+  if (type == CLUE_KERNEL_FLAT) return k[0];
+  if (type == CLUE_KERNEL_EXPONENTIAL) return fmul(k[1], expf(fmul(-k[0], dist)));
+  // Gaussian: amp * exp(-(d - avg) * (d - avg) / (2 * std * std))
+  const float u = fsub(dist, k[0]);
+  const float e = fdiv(fmul(-u, u), fmul(fmul(2.0f, k[1]), k[1]));
+  return fmul(k[2], expf(e));
+}
+
+}  // namespace clue_b200

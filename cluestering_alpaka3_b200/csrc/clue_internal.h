@@ -1,0 +1,138 @@
+// clue_internal.h -- host-side internals shared by the translation units of libclue_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+
+#include "clue_common.cuh"
+
+namespace clue_b200 {
+
+// Thread-local error message behind clue_last_error().
+void set_error(const std::string& msg);
+
+#define CLUE_CUDA_TRY(expr)                                                            \
+  do {                                                                                 \
+    cudaError_t err_ = (expr);                                                         \
+    if (err_ != cudaSuccess) {                                                         \
+      ::clue_b200::set_error(std::string(#expr) + ": " + cudaGetErrorString(err_));     \
+      return err_ == cudaErrorMemoryAllocation ? CLUE_ERR_OUT_OF_MEMORY : CLUE_ERR_CUDA; \
+    }                                                                                  \
+  } while (0)
+
+// ---- radix sort / scan (clue_sort.cu) -----------------------------------------
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;  // keys per radix block
+constexpr int kRadixBits = 8;
+constexpr int kRadix = 1 << kRadixBits;
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+inline int sort_blocks(int n) { return (n + kSortTile - 1) / kSortTile; }
+inline int bits_for(uint32_t maxkey) {
+  int b = 0;
+  while (b < 32 && (maxkey >> b) != 0) ++b;
+  return b;
+}
+// Scratch words needed by exclusive_scan for a length-len array.
+inline size_t scan_scratch_words(size_t len) { return (len + kScanTile - 1) / kScanTile + 1; }
+
+// Stable LSD radix sort of (key, value) pairs by the low `bits` bits of key.  Values
+// start as the identity (0..n-1) when vals_in is null.  Ping-pongs between buffer 0
+// and 1 of keys/vals; returns the index (0 or 1) holding the result.
+int radix_sort_pairs(uint32_t* keys[2], int32_t* vals[2], bool vals_identity, int n, int bits,
+                     uint32_t* hist, uint32_t* scan_scratch, cudaStream_t s);
+// Kernel launches made by radix_sort_pairs / exclusive_scan for the given sizes.
+inline int radix_sort_launches(int bits) { return (bits <= 0 ? 1 : (bits + kRadixBits - 1) / kRadixBits) * 5; }
+constexpr int kScanLaunches = 3;
+
+// Exclusive scan of len uint32 values (in may alias out).  Writes the total to *total
+// (device pointer) when non-null.
+void exclusive_scan(const uint32_t* in, uint32_t* out, size_t len, uint32_t* scratch,
+                    uint32_t* total, cudaStream_t s);
+
+// offsets[b] = first position of key b in sorted keys (b = 0..nkeys), n at the end.
+void offsets_from_sorted(const uint32_t* sorted_keys, int n, int nkeys, int32_t* offsets,
+                         cudaStream_t s);
+
+// ---- per-dimension pipeline (clue_dim.cu, one instantiation per N) ----------
+struct Workspace;
+
+struct RunArgs {
+  KParams kp;
+  int32_t ndim;
+  int32_t n;
+  const float* coords[kMaxDim];  // device, per dimension
+  const float* weight;           // device
+  clue_outputs out;              // device pointers (may be null except cluster_index)
+  int32_t metric;
+};
+
+template <int N>
+clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s);
+
+// Dispatch on ndim (clue_dim.cu).
+clue_status run_pipeline_dispatch(Workspace& ws, const RunArgs& a, cudaStream_t s);
+
+// ---- workspace ----------------------------------------------------------------
+struct Workspace {
+  int device = 0;
+  // current capacities
+  size_t cap_n = 0, cap_tiles = 0, cap_words = 0;
+  void* arena = nullptr;
+  size_t arena_bytes = 0;
+
+  DevGrid* grid = nullptr;
+  DevStatus* status = nullptr;
+  uint32_t* keys[2] = {nullptr, nullptr};
+  int32_t* vals[2] = {nullptr, nullptr};
+  uint32_t* hist = nullptr;
+  uint32_t* scan_scratch = nullptr;
+  int32_t* offsets = nullptr;
+  float4* rec_w = nullptr;  // coords + weight, tile-sorted
+  float4* rec_r = nullptr;  // coords + rho, tile-sorted
+  float* delta_s = nullptr;
+  int32_t* nh_s = nullptr;
+  int32_t* par = nullptr;
+  int32_t* is_seed_s = nullptr;
+  uint32_t* seed_flag = nullptr;  // original order, then exclusive-scanned to ranks
+  uint32_t* seed_total = nullptr;
+
+  // host staging for CLUE_MEM_HOST calls
+  void* pinned = nullptr;
+  size_t pinned_bytes = 0;
+  DevStatus* status_host = nullptr;  // pinned mirror of *status
+
+  // device staging for host-memory inputs/outputs
+  void* dstage = nullptr;
+  size_t dstage_bytes = 0;
+
+  int32_t* perm = nullptr;  // alias of the sorted values buffer after the tile sort
+  uint32_t* sorted_keys = nullptr;
+
+  KParams last_kp{};  // parameters of the last enqueued run (for clue_context_read_info)
+
+  // optional per-stage timing (clue_context_set_timing)
+  bool timing = false;
+  uint64_t launches = 0;  // kernels launched by this workspace (clue_context_kernel_launches)
+  cudaEvent_t ev[CLUE_N_STAGES + 1] = {};
+};
+
+// Records stage boundary k on s when timing is enabled.
+inline void stage_mark(Workspace& ws, int k, cudaStream_t s) {
+  if (ws.timing && ws.ev[k]) cudaEventRecord(ws.ev[k], s);
+}
+
+clue_status workspace_reserve(Workspace& ws, int ndim, size_t n, size_t ntiles);
+void workspace_release(Workspace& ws);
+
+// Host helpers (clue_capi.cu)
+float threshold_for(float r, bool root);
+void grid_shape(int32_t n, int32_t ppbin, int32_t ndim, int32_t* nperdim, int32_t* ntiles);
+
+}  // namespace clue_b200

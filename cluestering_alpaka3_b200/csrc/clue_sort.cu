@@ -1,0 +1,208 @@
+// clue_sort.cu -- stable LSD radix sort, exclusive scan and CSR offsets.
+//
+// These replace the reference's atomic association-map fill
+// (data_structures/AssociationMap.hpp:122-191 with the kernels of
+// data_structures/detail/AssociationMap.hpp:13-67) and alpaka's inclusiveScan: the
+// tile CSR is produced by a stable sort of (tile, point index) pairs, so the order
+// inside every tile is ascending point index -- the order the reference's serial
+// backend produces -- instead of the GPU atomic order.
+#include "clue_internal.h"
+
+namespace clue_b200 {
+
+namespace {
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  uint32_t m;
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// Per-block digit histogram; hist is digit-major: hist[d * nblocks + block].
+__global__ void __launch_bounds__(kSortThreads) k_radix_hist(const uint32_t* __restrict__ keys, int n,
+                                                             int shift, uint32_t* __restrict__ hist,
+                                                             int nblocks) {
+  __shared__ uint32_t h[kRadix];
+  for (int d = threadIdx.x; d < kRadix; d += blockDim.x) h[d] = 0;
+  __syncthreads();
+  const int base = blockIdx.x * kSortTile;
+#pragma unroll 4
+  for (int r = 0; r < kSortItems; ++r) {
+    const int i = base + r * kSortThreads + threadIdx.x;
+    const bool valid = i < n;
+    const uint32_t d = valid ? (keys[i] >> shift) & (kRadix - 1) : (uint32_t)kRadix;
+    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    if (valid && (peers & lanemask_lt()) == 0) atomicAdd(&h[d], __popc(peers));
+  }
+  __syncthreads();
+  for (int d = threadIdx.x; d < kRadix; d += blockDim.x) hist[(size_t)d * nblocks + blockIdx.x] = h[d];
+}
+
+// Stable scatter: items are visited in index order (round-major, then warp, then lane),
+// each gets its global slot = scanned[d][block] + items of digit d before it in the block.
+__global__ void __launch_bounds__(kSortThreads) k_radix_scatter(
+    const uint32_t* __restrict__ kin, const int32_t* __restrict__ vin, uint32_t* __restrict__ kout,
+    int32_t* __restrict__ vout, int n, int shift, const uint32_t* __restrict__ scanned, int nblocks) {
+  constexpr int kWarps = kSortThreads / 32;
+  __shared__ uint32_t run[kRadix];
+  __shared__ uint32_t wcnt[kWarps][kRadix];
+  const int warp = threadIdx.x >> 5;
+  for (int d = threadIdx.x; d < kRadix; d += blockDim.x) run[d] = scanned[(size_t)d * nblocks + blockIdx.x];
+  const int base = blockIdx.x * kSortTile;
+  for (int r = 0; r < kSortItems; ++r) {
+    if (base + r * kSortThreads >= n) break;  // uniform across the block
+    for (int e = threadIdx.x; e < kWarps * kRadix; e += blockDim.x) (&wcnt[0][0])[e] = 0;
+    __syncthreads();
+    const int i = base + r * kSortThreads + threadIdx.x;
+    const bool valid = i < n;
+    const uint32_t key = valid ? kin[i] : 0u;
+    const int32_t val = valid ? (vin ? vin[i] : i) : 0;
+    const uint32_t d = valid ? (key >> shift) & (kRadix - 1) : (uint32_t)kRadix;
+    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    const uint32_t rank = __popc(peers & lanemask_lt());
+    if (valid && rank == 0) wcnt[warp][d] = __popc(peers);
+    __syncthreads();
+    for (int dd = threadIdx.x; dd < kRadix; dd += blockDim.x) {
+      uint32_t acc = run[dd];
+#pragma unroll
+      for (int w = 0; w < kWarps; ++w) {
+        const uint32_t c = wcnt[w][dd];
+        wcnt[w][dd] = acc;
+        acc += c;
+      }
+      run[dd] = acc;
+    }
+    __syncthreads();
+    if (valid) {
+      const uint32_t pos = wcnt[warp][d] + rank;
+      kout[pos] = key;
+      vout[pos] = val;
+    }
+    __syncthreads();
+  }
+}
+
+__device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
+    if (lane >= o) v += t;
+  }
+  return v;
+}
+
+// Block-wide exclusive scan of one value per thread; returns the block total via *tot.
+__device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* tot) {
+  __shared__ uint32_t ws[33];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const uint32_t inc = warp_incl_scan(v);
+  if (lane == 31) ws[warp] = inc;
+  __syncthreads();
+  if (warp == 0) {
+    const uint32_t x = lane < nw ? ws[lane] : 0u;
+    const uint32_t xi = warp_incl_scan(x);
+    if (lane < nw) ws[lane] = xi - x;
+    if (lane == nw - 1) ws[32] = xi;
+  }
+  __syncthreads();
+  const uint32_t r = ws[warp] + inc - v;
+  if (tot) *tot = ws[32];
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_reduce(const uint32_t* __restrict__ in, size_t len,
+                                                              uint32_t* __restrict__ partial) {
+  const size_t base = (size_t)blockIdx.x * kScanTile + (size_t)threadIdx.x * kScanItems;
+  uint32_t s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k)
+    if (base + k < len) s += in[base + k];
+  uint32_t tot;
+  block_excl_scan(s, &tot);
+  if (threadIdx.x == 0) partial[blockIdx.x] = tot;
+}
+
+// Single block: exclusive scan of the per-block partials (any count, looped).
+__global__ void __launch_bounds__(1024) k_scan_partials(uint32_t* partial, int nparts, uint32_t* total) {
+  uint32_t carry = 0;
+  for (int base = 0; base < nparts; base += blockDim.x) {
+    const int i = base + threadIdx.x;
+    const uint32_t v = i < nparts ? partial[i] : 0u;
+    uint32_t tot;
+    const uint32_t ex = block_excl_scan(v, &tot);
+    if (i < nparts) partial[i] = carry + ex;
+    carry += tot;
+  }
+  if (threadIdx.x == 0 && total) *total = carry;
+}
+
+// `in` and `out` may alias (in-place scan): every thread reads its items before writing them.
+__global__ void __launch_bounds__(kScanThreads) k_scan_down(const uint32_t* in, size_t len,
+                                                            const uint32_t* __restrict__ partial,
+                                                            uint32_t* out) {
+  const size_t base = (size_t)blockIdx.x * kScanTile + (size_t)threadIdx.x * kScanItems;
+  uint32_t v[kScanItems];
+  uint32_t s = 0;
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    v[k] = base + k < len ? in[base + k] : 0u;
+    s += v[k];
+  }
+  uint32_t run = partial[blockIdx.x] + block_excl_scan(s, nullptr);
+#pragma unroll
+  for (int k = 0; k < kScanItems; ++k) {
+    if (base + k < len) out[base + k] = run;
+    run += v[k];
+  }
+}
+
+__global__ void k_offsets(const uint32_t* __restrict__ keys, int n, int nkeys, int32_t* __restrict__ off) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int pos = blockIdx.x * blockDim.x + threadIdx.x; pos <= n; pos += stride) {
+    const int prev = pos > 0 ? (int)keys[pos - 1] : -1;
+    const int cur = pos < n ? (int)keys[pos] : nkeys;
+    for (int b = prev + 1; b <= cur; ++b) off[b] = pos;
+  }
+}
+
+}  // namespace
+
+void exclusive_scan(const uint32_t* in, uint32_t* out, size_t len, uint32_t* scratch, uint32_t* total,
+                    cudaStream_t s) {
+  const int nb = (int)((len + kScanTile - 1) / kScanTile);
+  if (nb == 0) {
+    if (total) cudaMemsetAsync(total, 0, sizeof(uint32_t), s);
+    return;
+  }
+  k_scan_reduce<<<nb, kScanThreads, 0, s>>>(in, len, scratch);
+  k_scan_partials<<<1, 1024, 0, s>>>(scratch, nb, total);
+  k_scan_down<<<nb, kScanThreads, 0, s>>>(in, len, scratch, out);
+}
+
+int radix_sort_pairs(uint32_t* keys[2], int32_t* vals[2], bool vals_identity, int n, int bits,
+                     uint32_t* hist, uint32_t* scan_scratch, cudaStream_t s) {
+  const int nb = sort_blocks(n);
+  int cur = 0;
+  const int passes = bits <= 0 ? 1 : (bits + kRadixBits - 1) / kRadixBits;
+  for (int p = 0; p < passes; ++p) {
+    const int shift = p * kRadixBits;
+    k_radix_hist<<<nb, kSortThreads, 0, s>>>(keys[cur], n, shift, hist, nb);
+    exclusive_scan(hist, hist, (size_t)kRadix * nb, scan_scratch, nullptr, s);
+    const int32_t* vin = (p == 0 && vals_identity) ? nullptr : vals[cur];
+    k_radix_scatter<<<nb, kSortThreads, 0, s>>>(keys[cur], vin, keys[cur ^ 1], vals[cur ^ 1], n, shift,
+                                                hist, nb);
+    cur ^= 1;
+  }
+  return cur;
+}
+
+void offsets_from_sorted(const uint32_t* sorted_keys, int n, int nkeys, int32_t* offsets, cudaStream_t s) {
+  const int threads = 256;
+  int blocks = (n + 1 + threads - 1) / threads;
+  if (blocks > 148 * 16) blocks = 148 * 16;
+  k_offsets<<<blocks, threads, 0, s>>>(sorted_keys, n, nkeys, offsets);
+}
+
+}  // namespace clue_b200

@@ -1,0 +1,220 @@
+/*
+ * clue_b200.h -- C ABI of the B200-native CLUE clustering library (libclue_b200.so).
+ *
+ * Plain C types only (pointers, sizes, PODs); no CUDA or torch types appear in the
+ * signatures.  Streams are passed as `void*` holding a cudaStream_t (NULL = the
+ * legacy default stream of the current device).
+ *
+ * Every entry point returns a clue_status; on failure clue_last_error() returns a
+ * thread-local message.  The reference throws std::invalid_argument /
+ * std::out_of_range / std::runtime_error on the host; the C++ layer in
+ * include/CLUEstering/ maps the status codes back onto those exception types.
+ *
+ * Reference interfaces replaced (paths relative to the reference project root):
+ *   clue_make_clusters  <- clue::Clusterer::make_clusters (4 overloads)
+ *                          include/CLUEstering/core/Clusterer.hpp:114-169,
+ *                          pipeline include/CLUEstering/core/detail/Clusterer.hpp:134-217
+ *   clue_params         <- Clusterer ctor / setParameters / setWrappedCoordinates
+ *                          include/CLUEstering/core/Clusterer.hpp:84-103,174-182
+ *   clue_kernel         <- FlatKernel / ExponentialKernel / GaussianKernel
+ *                          include/CLUEstering/core/ConvolutionalKernel.hpp:14-85
+ *   clue_metric         <- the six metrics of include/CLUEstering/core/DistanceMetrics.hpp:33-230
+ *   clue_context_*      <- the Clusterer's reusable tiles / seeds / followers buffers
+ *                          include/CLUEstering/core/Clusterer.hpp:47-49
+ *   clue_device_alloc / clue_memcpy_* / clue_stream_*
+ *                       <- PointsDevice storage and copyToHost / copyToDevice
+ *                          include/CLUEstering/data_structures/PointsDevice.hpp:19-107,129-194
+ *   clue_get_clusters   <- clue::get_clusters (cluster -> points association map)
+ *                          include/CLUEstering/utils/detail/get_clusters.hpp:21-46
+ *   clue_batch_*        <- no reference counterpart: many independent events in one launch
+ */
+#ifndef CLUE_B200_H
+#define CLUE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CLUE_MAX_DIM 10
+#define CLUE_ABI_VERSION 1
+
+typedef enum clue_status {
+  CLUE_OK = 0,
+  CLUE_ERR_INVALID_ARG = 1,    /* std::invalid_argument in the reference */
+  CLUE_ERR_OUT_OF_MEMORY = 2,  /* device allocation failed */
+  CLUE_ERR_CAPACITY = 3,       /* request larger than a fixed capacity */
+  CLUE_ERR_TIMEOUT = 4,        /* a bounded device wait gave up */
+  CLUE_ERR_CUDA = 5,           /* CUDA runtime error (message holds the CUDA error string) */
+  CLUE_ERR_NOT_SUPPORTED = 6,  /* option not available in this build */
+  CLUE_ERR_NONFINITE = 7,      /* NaN or Inf in coordinates or weights */
+  CLUE_ERR_OUT_OF_RANGE = 8    /* std::out_of_range in the reference */
+} clue_status;
+
+typedef enum clue_kernel_type {
+  CLUE_KERNEL_FLAT = 0,        /* par[0] = flat height */
+  CLUE_KERNEL_EXPONENTIAL = 1, /* par[0] = avg, par[1] = amplitude */
+  CLUE_KERNEL_GAUSSIAN = 2     /* par[0] = avg, par[1] = std, par[2] = amplitude */
+} clue_kernel_type;
+
+typedef struct clue_kernel {
+  int32_t type;
+  float par[3];
+} clue_kernel;
+
+typedef enum clue_metric_type {
+  CLUE_METRIC_EUCLIDEAN = 0,
+  CLUE_METRIC_WEIGHTED_EUCLIDEAN = 1, /* par[d] = weight of dimension d */
+  CLUE_METRIC_PERIODIC_EUCLIDEAN = 2, /* par[d] = period of dimension d (0 = not periodic) */
+  CLUE_METRIC_MANHATTAN = 3,
+  CLUE_METRIC_CHEBYSHEV = 4,
+  CLUE_METRIC_WEIGHTED_CHEBYSHEV = 5  /* par[d] = weight of dimension d */
+} clue_metric_type;
+
+typedef struct clue_metric {
+  int32_t type;
+  float par[CLUE_MAX_DIM];
+} clue_metric;
+
+typedef enum clue_tiebreak {
+  CLUE_TIE_REFERENCE = 0, /* nearest higher keeps the first strict minimum in tile order */
+  CLUE_TIE_RHO_INDEX = 1  /* equal distances resolved by higher rho, then lower index */
+} clue_tiebreak;
+
+typedef struct clue_params {
+  float dc;       /* density radius, > 0 */
+  float rhoc;     /* seed density threshold, >= 0 */
+  float dm;       /* nearest-higher search radius, > 0 (reference default: dc) */
+  float seed_dc;  /* seed distance threshold, > 0 (reference default: dc) */
+  int32_t points_per_tile;        /* > 0 (reference default 128) */
+  uint8_t wrapped[CLUE_MAX_DIM];  /* 1 = periodic coordinate */
+  /* Seed list capacity.  < 0: every seed is kept.  >= 0: the reference's SeedArray
+   * policy -- capacity = max(seed_capacity, number of points without a nearest
+   * higher); seeds beyond it (in index order) are dropped and their followers get
+   * label -1, as in include/CLUEstering/data_structures/internal/SeedArray.hpp:33-41. */
+  int64_t seed_capacity;
+  int32_t tiebreak;               /* clue_tiebreak */
+  int32_t reserved;
+} clue_params;
+
+/* Output arrays, caller-owned, n elements each, all in the memory space given by
+ * `memory` in clue_make_clusters.  Only cluster_index is required. */
+typedef struct clue_outputs {
+  int32_t* cluster_index;  /* cluster label, -1 for outliers / unassigned */
+  int32_t* is_seed;        /* 1 for seeds */
+  float* rho;              /* local density */
+  int32_t* nearest_higher; /* index of the nearest higher point, -1 for seeds and outliers */
+  float* delta;            /* distance to the nearest higher (FLT_MAX when none was found) */
+} clue_outputs;
+
+typedef struct clue_run_info {
+  int64_t n_seeds;             /* points flagged as seeds */
+  int64_t n_clusters;          /* seeds kept in the seed list (= clusters labelled) */
+  int64_t dropped_seeds;       /* seeds beyond the seed capacity */
+  int64_t seed_capacity_used;  /* -1 when every seed is kept */
+  int64_t n_tiles;             /* tiles of the reference grid */
+  int64_t n_per_dim;
+  int64_t label_rounds;        /* pointer-jumping rounds that changed a parent */
+} clue_run_info;
+
+typedef enum clue_memory { CLUE_MEM_DEVICE = 0, CLUE_MEM_HOST = 1 } clue_memory;
+
+typedef struct clue_context_s* clue_context;
+
+/* ---- version / errors ---------------------------------------------------- */
+int32_t clue_abi_version(void);
+const char* clue_last_error(void);
+const char* clue_status_string(clue_status s);
+
+/* ---- parameter validation (host only, no GPU needed) -------------------- */
+/* Clusterer ctor / setParameters rules: include/CLUEstering/core/detail/Clusterer.hpp:24-51. */
+clue_status clue_check_params(const clue_params* p);
+/* Kernel ctor rules: include/CLUEstering/core/detail/ConvolutionalKernel.hpp:10-53
+ * (Gaussian avg >= 0 is accepted; the reference rejects avg == 0). */
+clue_status clue_check_kernel(const clue_kernel* k);
+clue_status clue_check_metric(const clue_metric* m, int32_t ndim);
+/* Reference tile grid shape for n points (include/CLUEstering/core/detail/SetupTiles.hpp:23-26). */
+clue_status clue_grid_shape(int32_t n, int32_t points_per_tile, int32_t ndim, int32_t* n_per_dim,
+                            int32_t* n_tiles);
+/* Metric / kernel evaluation on the host, for known-answer tests of the plugins
+ * (include/CLUEstering/core/DistanceMetrics.hpp, core/detail/ConvolutionalKernel.hpp). */
+float clue_metric_eval(const clue_metric* m, int32_t ndim, const float* a, const float* b);
+float clue_kernel_eval(const clue_kernel* k, float dist, int32_t i, int32_t j);
+
+/* ---- devices, memory, streams ------------------------------------------- */
+clue_status clue_device_count(int32_t* count);
+clue_status clue_device_alloc(int32_t device, size_t bytes, void** ptr);
+clue_status clue_device_free(void* ptr);
+clue_status clue_host_alloc_pinned(size_t bytes, void** ptr);
+clue_status clue_host_free_pinned(void* ptr);
+clue_status clue_memcpy_htod(void* dst, const void* src, size_t bytes, void* stream);
+clue_status clue_memcpy_dtoh(void* dst, const void* src, size_t bytes, void* stream);
+clue_status clue_memcpy_dtod(void* dst, const void* src, size_t bytes, void* stream);
+clue_status clue_stream_create(int32_t device, void** stream);
+clue_status clue_stream_destroy(void* stream);
+clue_status clue_stream_synchronize(void* stream);
+
+/* ---- clustering ----------------------------------------------------------- */
+/* A context owns reusable device workspace (tile CSR, sorted point records, seed and
+ * label buffers) on one device; buffers only grow.  Not thread-safe: one caller
+ * at a time, like a reference Clusterer. */
+clue_status clue_context_create(int32_t device, clue_context* ctx);
+clue_status clue_context_destroy(clue_context ctx);
+/* Pre-size the workspace for up to n points of ndim dimensions (optional). */
+clue_status clue_context_reserve(clue_context ctx, int32_t ndim, int32_t n, int32_t points_per_tile);
+/* Bytes of device workspace the context currently holds. */
+size_t clue_context_workspace_bytes(clue_context ctx);
+
+/*
+ * Run the five CLUE stages on n points of ndim (1..10) dimensions.
+ * coords: SoA, coords[d * n + i];  weight: n floats.  Both in `memory` space, as are
+ * the outputs.  With CLUE_MEM_HOST the library copies through pinned staging
+ * buffers on `stream`.  Blocks until the results are in `out` (the reference's
+ * make_clusters waits as well); `info` may be NULL.
+ * Non-finite coordinates or weights are rejected with CLUE_ERR_NONFINITE
+ * (the reference's behaviour there is undefined: static_cast<int>(NaN)).
+ */
+clue_status clue_make_clusters(clue_context ctx, const clue_params* params, const clue_kernel* kernel,
+                               const clue_metric* metric, int32_t ndim, int32_t n,
+                               const float* coords, const float* weight, const clue_outputs* out,
+                               int32_t memory, void* stream, clue_run_info* info);
+
+/*
+ * Same pipeline, device memory only, without any host synchronisation: every launch is
+ * enqueued on `stream` and the call returns.  Nothing is allocated if the context was
+ * reserved for (ndim, n) beforehand, so the call can be captured in a CUDA graph.
+ * Run information and the non-finite check land in a device-side status block that
+ * clue_context_read_info() copies back (it synchronises the stream).
+ */
+clue_status clue_make_clusters_async(clue_context ctx, const clue_params* params,
+                                     const clue_kernel* kernel, const clue_metric* metric,
+                                     int32_t ndim, int32_t n, const float* coords,
+                                     const float* weight, const clue_outputs* out, void* stream);
+clue_status clue_context_read_info(clue_context ctx, void* stream, clue_run_info* info);
+
+/* Per-stage device timing of the following runs (CUDA events on the run's stream):
+ * stage 0 = tile build (bounding box, bins, sort, records), 1 = local density,
+ * 2 = nearest higher, 3 = seeds + labels + output scatter.  Off by default. */
+#define CLUE_N_STAGES 4
+clue_status clue_context_set_timing(clue_context ctx, int32_t enable);
+/* Milliseconds of each stage of the last timed run (synchronises on its last event). */
+clue_status clue_context_stage_times(clue_context ctx, float* ms, int32_t n_stages);
+/* Kernels this context has launched so far (all runs). */
+uint64_t clue_context_kernel_launches(clue_context ctx);
+
+/*
+ * Cluster -> points association map (CSR) from device labels: offsets[n_clusters + 1],
+ * points[n_clustered] (point indexes ascending inside each cluster).  All device
+ * pointers; `offsets` must hold max_label + 2 entries and `points` n entries.
+ * n_clusters_out / n_clustered_out are written on the host (synchronises).
+ */
+clue_status clue_get_clusters(clue_context ctx, int32_t n, const int32_t* cluster_index,
+                              int32_t* offsets, int32_t* points, int32_t* n_clusters_out,
+                              int32_t* n_clustered_out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CLUE_B200_H */

@@ -1,0 +1,62 @@
+"""Helpers shared by the parity tests: run the GPU library and the CPU oracle on one input."""
+from __future__ import annotations
+
+import numpy as np
+
+from oracle import oracle as O
+
+KERNEL_NAMES = {"flat": 0, "exp": 1, "gaus": 2}
+METRIC_NAMES = list(O.METRICS.keys())
+
+
+def oracle_cfg(dc, rhoc, dm=None, seed_dc=None, ppbin=128, kernel=("flat", (0.5,)),
+               metric=("euclidean", ()), wrapped=(), seed_capacity=0, tiebreak="reference"):
+    return O.Config(dc=dc, rhoc=rhoc, dm=dm, seed_dc=seed_dc, ppbin=ppbin, kernel=kernel[0],
+                    kernel_par=tuple(kernel[1]), metric=metric[0], metric_par=tuple(metric[1]),
+                    wrapped=tuple(wrapped), seed_capacity=seed_capacity, tiebreak=tiebreak)
+
+
+def gpu_args(dc, rhoc, dm=None, seed_dc=None, ppbin=128, kernel=("flat", (0.5,)),
+             metric=("euclidean", ()), wrapped=(), seed_capacity=0, tiebreak="reference"):
+    from cluestering_alpaka3_b200 import capi
+    params = capi.Params(dc=dc, rhoc=rhoc, dm=dm, seed_dc=seed_dc, points_per_tile=ppbin,
+                         wrapped=tuple(wrapped), seed_capacity=seed_capacity,
+                         tiebreak=capi.TIE_REFERENCE if tiebreak == "reference" else capi.TIE_RHO_INDEX)
+    k = capi.Kernel(KERNEL_NAMES[kernel[0]], tuple(kernel[1]))
+    m = capi.Metric(METRIC_NAMES.index(metric[0]), tuple(metric[1]))
+    return params, k, m
+
+
+def run_both(ctx, coords, weight, **kw):
+    cfg = oracle_cfg(**kw)
+    ref = O.run(coords, weight, cfg)
+    params, k, m = gpu_args(**kw)
+    got = ctx.make_clusters_host(coords, weight, params, k, m)
+    return ref, got
+
+
+def assert_exact(ref, got, check_rho=True):
+    """Bit-exact comparison of every output of the pipeline."""
+    np.testing.assert_array_equal(got.is_seed, ref.is_seed, err_msg="is_seed")
+    np.testing.assert_array_equal(got.nearest_higher, ref.nearest_higher, err_msg="nearest_higher")
+    np.testing.assert_array_equal(got.cluster_index, ref.cluster_index, err_msg="cluster_index")
+    if check_rho:
+        np.testing.assert_array_equal(got.rho.view(np.uint32), ref.rho.view(np.uint32), err_msg="rho bits")
+        np.testing.assert_array_equal(got.delta.view(np.uint32), ref.delta.view(np.uint32),
+                                      err_msg="delta bits")
+    assert got.info.n_clusters == ref.stats["n_clusters"]
+    assert got.info.n_seeds == ref.stats["n_seeds"]
+    assert got.info.dropped_seeds == ref.stats["dropped_seeds"]
+
+
+def random_blobs(rng, n, ndim, nblobs=8, extent=100.0, sigma=1.0, noise=0.1, weights="uniform"):
+    per = int(n * (1 - noise)) // nblobs
+    centres = rng.uniform(0.1 * extent, 0.9 * extent, size=(nblobs, ndim))
+    blobs = (centres[:, None, :] + rng.normal(0, sigma, size=(nblobs, per, ndim))).reshape(-1, ndim)
+    rest = rng.uniform(0, extent, size=(n - per * nblobs, ndim))
+    c = np.concatenate([blobs, rest]).T.astype(np.float32)
+    if weights == "ones":
+        w = np.ones(n, np.float32)
+    else:
+        w = rng.uniform(0.5, 1.5, size=n).astype(np.float32)
+    return np.ascontiguousarray(c), w

