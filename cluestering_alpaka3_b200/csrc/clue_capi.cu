@@ -103,7 +103,7 @@ clue_status workspace_reserve(Workspace& ws, int ndim, size_t n, size_t ntiles) 
   const size_t w = std::max(words, ws.cap_words);
   const size_t nb = (size_t)sort_blocks((int)n);
   const size_t hist_len = (size_t)kRadix * nb;
-  const size_t scan_words = scan_scratch_words(std::max(hist_len, n)) + 1;
+  const size_t scan_words = scan_scratch_words(std::max(std::max(hist_len, n), ntiles)) + 1;
   struct Item {
     void** ptr;
     size_t bytes;
@@ -127,6 +127,11 @@ clue_status workspace_reserve(Workspace& ws, int ndim, size_t n, size_t ntiles) 
       {(void**)&nw.is_seed_s, n * 4},
       {(void**)&nw.seed_flag, n * 4},
       {(void**)&nw.seed_total, 16},
+      {(void**)&nw.ord_rho, n * 4},
+      {(void**)&nw.ord_nh, n * 4},
+      {(void**)&nw.chunk_count, (ntiles + 1) * 4},
+      {(void**)&nw.chunk_tile, (n / kChunkPoints + ntiles + 1) * 4},
+      {(void**)&nw.chunk_total, 16},
   };
   size_t total = 0;
   for (auto& it : items) total = align_up(total, 256) + align_up(it.bytes, 256);
@@ -552,6 +557,10 @@ static clue_status read_info(Workspace& ws, const KParams& kp, cudaStream_t s, c
   CLUE_CUDA_TRY(cudaMemcpyAsync(total, ws.seed_total, 4, cudaMemcpyDeviceToHost, s));
   CLUE_CUDA_TRY(cudaStreamSynchronize(s));
   unresolved = h->unresolved[3] != 0;
+  if (h->stage_timeout) {
+    set_error("a bulk-copy wait in the density / nearest-higher sweep timed out");
+    return CLUE_ERR_TIMEOUT;
+  }
   if (h->nonfinite) {
     set_error("coordinates or weights contain NaN or Inf");
     return CLUE_ERR_NONFINITE;

@@ -64,7 +64,8 @@ struct DevStatus {
   uint32_t n_seeds;
   uint32_t unresolved[64];   // label rounds that left an unresolved parent chain
   uint32_t label_rounds;
-  uint32_t pad[3];
+  uint32_t stage_timeout;  // a bulk-copy wait in a staged sweep gave up
+  uint32_t pad[2];
 };
 
 // float -> int32 truncation with x86 cvttss2si semantics (NaN and out-of-range give

@@ -17,6 +17,7 @@
 // whole warp walks the same candidate sequence, so every candidate record is one
 // broadcast 16-byte load per warp.
 #include "clue_internal.h"
+#include "clue_tma.cuh"
 
 #ifndef CLUE_NDIM
 #error "CLUE_NDIM must be defined"
@@ -26,8 +27,12 @@ namespace clue_b200 {
 namespace {
 
 constexpr int kTileThreads = 128;
-constexpr int kTileWarps = kTileThreads / 32;
-constexpr int kCap = 2048;  // home points signature-sorted per pass
+constexpr int kChunkWarps = kTileThreads / 32;
+constexpr int kChunk = kChunkPoints;      // home points per CTA in the density / nearest-higher sweeps
+static_assert(kChunkPoints == kTileThreads, "one home point per thread");
+constexpr int kCap = 2048;                // home points signature-sorted per pass
+constexpr int kStageWords = 1024;         // float4 words per staging buffer (16 KiB)
+constexpr int kMaxSeg = 32;               // tile segments per staged piece
 
 struct InPtrs {
   const float* c[kMaxDim];
@@ -255,6 +260,246 @@ __global__ void __launch_bounds__(256) k_gather(InPtrs in, int n, const int32_t*
   }
 }
 
+// ---- work orders and chunks --------------------------------------------------
+// Every tile's points are ordered twice by search-box signature (radius dc for the
+// density, dm for the nearest higher) and cut into chunks of kChunk home points; one CTA
+// processes one chunk, so a heavy tile is spread over many CTAs.
+template <int N>
+__global__ void __launch_bounds__(kTileThreads) k_order(const KParams kp, const DevGrid* __restrict__ g,
+                                                        const int32_t* __restrict__ off,
+                                                        const float4* __restrict__ rec_w,
+                                                        int32_t* __restrict__ ord_rho, int32_t* __restrict__ ord_nh,
+                                                        uint32_t* __restrict__ chunk_count) {
+  __shared__ int32_t s_order[kCap];
+  __shared__ uint8_t s_key[kCap];
+  __shared__ int32_t s_hist[N <= 4 ? (1 << (2 * N)) : 1];
+  for (int t = blockIdx.x; t < kp.ntiles; t += gridDim.x) {
+    const int beg = off[t], end = off[t + 1];
+    if (threadIdx.x == 0) chunk_count[t] = (uint32_t)((end - beg + kChunk - 1) / kChunk);
+    if (beg == end) continue;
+    int hb[N];
+    home_bins<N>(kp, t, hb);
+    for (int cb = beg; cb < end; cb += kCap) {
+      const int cnt = min(kCap, end - cb);
+      signature_sort<N>(kp, g, rec_w, cb, cnt, kp.dc, hb, s_order, s_key, s_hist);
+      for (int k = threadIdx.x; k < cnt; k += blockDim.x) ord_rho[cb + k] = cb + s_order[k];
+      __syncthreads();
+      signature_sort<N>(kp, g, rec_w, cb, cnt, kp.dm, hb, s_order, s_key, s_hist);
+      for (int k = threadIdx.x; k < cnt; k += blockDim.x) ord_nh[cb + k] = cb + s_order[k];
+      __syncthreads();
+    }
+  }
+}
+
+__global__ void k_chunk_map(int ntiles, const int32_t* __restrict__ off, const uint32_t* __restrict__ chunk_off,
+                            int32_t* __restrict__ chunk_tile) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntiles; t += stride) {
+    const int nch = (off[t + 1] - off[t] + kChunk - 1) / kChunk;
+    const uint32_t c0 = chunk_off[t];
+    for (int c = 0; c < nch; ++c) chunk_tile[c0 + c] = t;
+  }
+}
+
+// ---- staged sweep over the search-box tiles of one chunk ------------------------
+// The CTA's 4 warps (128 home points of one tile) walk the union of their search boxes
+// in the reference's lexicographic tile order.  Thread 0 packs consecutive tile segments
+// into pieces of at most kStageWords float4 words and copies each piece into shared memory
+// with bulk copies (TMA) completing on an mbarrier; two buffers alternate so the copy of
+// piece p + 1 overlaps the scan of piece p.  Each warp scans only the segments of tiles in
+// its own union; each lane only counts candidates of tiles inside its own box.
+
+template <int N>
+struct StageSmem {
+  float4 buf[2][kStageWords];
+  int32_t seg_v[2][kMaxSeg][N];
+  int32_t seg_qb[2][kMaxSeg];
+  int32_t seg_cnt[2][kMaxSeg];
+  int32_t seg_boff[2][kMaxSeg];
+  int32_t nseg[2];
+  int32_t wlo[kChunkWarps][N], whi[kChunkWarps][N];
+  int32_t ulo[N], uhi[N];
+  int32_t any_valid;
+  alignas(8) uint64_t full[2];
+};
+
+// Thread-0 iterator over the tiles of the CTA union that some warp needs.
+template <int N>
+struct TileIter {
+  int v[N];
+  bool started = false;
+  int q = 0, qe = 0;
+
+  __device__ bool needed(const StageSmem<N>& sm) const {
+    for (int w = 0; w < kChunkWarps; ++w) {
+      bool in = true;
+#pragma unroll
+      for (int d = 0; d < N; ++d) in = in && v[d] >= sm.wlo[w][d] && v[d] <= sm.whi[w][d];
+      if (in) return true;
+    }
+    return false;
+  }
+
+  // Advances to the next needed, non-empty tile; false when the union is exhausted.
+  __device__ bool next(const KParams& kp, const int32_t* __restrict__ off, const StageSmem<N>& sm) {
+    while (true) {
+      if (!started) {
+#pragma unroll
+        for (int d = 0; d < N; ++d) v[d] = sm.ulo[d];
+        started = true;
+      } else {
+        int d = N - 1;
+        for (; d >= 0; --d) {
+          if (v[d] < sm.uhi[d]) {
+            ++v[d];
+            break;
+          }
+          v[d] = sm.ulo[d];
+        }
+        if (d < 0) return false;
+      }
+      if (!needed(sm)) continue;
+      int u = 0;
+#pragma unroll
+      for (int d = 0; d < N; ++d) u += kp.stride[d] * wrap_bin(v[d], kp.nperdim);
+      q = off[u];
+      qe = off[u + 1];
+      if (qe > q) return true;
+    }
+  }
+};
+
+// Builds piece b (thread 0 only) and issues its bulk copies; returns the words staged.
+template <int N>
+__device__ int build_piece(const KParams& kp, const int32_t* __restrict__ off, const float4* __restrict__ rec,
+                           StageSmem<N>& sm, TileIter<N>& it, bool& done, int b) {
+  constexpr int W = Rec<N>::kWords;
+  constexpr int cap = kStageWords / W;
+  int nseg = 0, fill = 0;
+  while (!done && nseg < kMaxSeg && fill < cap) {
+    if (it.q >= it.qe) {
+      if (!it.next(kp, off, sm)) {
+        done = true;
+        break;
+      }
+    }
+    const int take = min(it.qe - it.q, cap - fill);
+#pragma unroll
+    for (int d = 0; d < N; ++d) sm.seg_v[b][nseg][d] = it.v[d];
+    sm.seg_qb[b][nseg] = it.q;
+    sm.seg_cnt[b][nseg] = take;
+    sm.seg_boff[b][nseg] = fill;
+    ++nseg;
+    fill += take;
+    it.q += take;
+  }
+  sm.nseg[b] = nseg;
+  if (fill > 0) {
+    mbar_arrive_expect_tx(&sm.full[b], (uint32_t)(fill * W * 16));
+    for (int s = 0; s < nseg; ++s)
+      bulk_g2s(&sm.buf[b][sm.seg_boff[b][s] * W], rec + (size_t)sm.seg_qb[b][s] * W,
+               (uint32_t)(sm.seg_cnt[b][s] * W * 16), &sm.full[b]);
+  }
+  return fill;
+}
+
+constexpr uint64_t kWaitLimitNs = 1000000000ull;  // 1 s per bulk-copy wait
+
+// Runs the staged sweep; `vis(seg_inbox, c, payload, q)` is called for every staged
+// candidate of a segment the warp needs.  Returns false if a bulk copy did not complete
+// within the wait limit (the caller reports it and the CTA exits).
+template <int N, class Visit>
+__device__ bool staged_sweep(const KParams& kp, const int32_t* __restrict__ off, const float4* __restrict__ rec,
+                             StageSmem<N>& sm, const int* lo, const int* hi, bool valid, Visit&& vis) {
+  constexpr int W = Rec<N>::kWords;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int wl[N], wh[N];
+  const bool warp_valid = __any_sync(0xffffffffu, valid);
+#pragma unroll
+  for (int d = 0; d < N; ++d) {
+    wl[d] = warp_min_i(valid ? lo[d] : INT_MAX);
+    wh[d] = warp_max_i(valid ? hi[d] : INT_MIN);
+  }
+  if (lane == 0) {
+#pragma unroll
+    for (int d = 0; d < N; ++d) {
+      sm.wlo[warp][d] = wl[d];
+      sm.whi[warp][d] = wh[d];
+    }
+  }
+  if (threadIdx.x == 0) {
+    mbar_init(&sm.full[0], 1);
+    mbar_init(&sm.full[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int any = 0;
+#pragma unroll
+    for (int d = 0; d < N; ++d) {
+      int a = INT_MAX, z = INT_MIN;
+      for (int w = 0; w < kChunkWarps; ++w) {
+        a = min(a, sm.wlo[w][d]);
+        z = max(z, sm.whi[w][d]);
+      }
+      sm.ulo[d] = a;
+      sm.uhi[d] = z;
+    }
+    for (int w = 0; w < kChunkWarps; ++w) any |= sm.wlo[w][0] != INT_MAX;
+    sm.any_valid = any;
+  }
+  __syncthreads();
+  TileIter<N> it;
+  bool done = sm.any_valid == 0;
+  int has_next = 0;
+  if (threadIdx.x == 0) has_next = build_piece<N>(kp, off, rec, sm, it, done, 0) > 0;
+  __shared__ int s_has[2];
+  if (threadIdx.x == 0) s_has[0] = has_next;
+  __syncthreads();
+  bool ok = true;
+  for (int p = 0; s_has[p & 1]; ++p) {
+    const int b = p & 1;
+    if (threadIdx.x == 0) s_has[b ^ 1] = build_piece<N>(kp, off, rec, sm, it, done, b ^ 1) > 0;
+    if (!mbar_wait_bounded(&sm.full[b], (uint32_t)((p >> 1) & 1), kWaitLimitNs)) {
+      ok = false;
+      break;
+    }
+    const int nseg = sm.nseg[b];
+    for (int s = 0; s < nseg; ++s) {
+      bool wneed = warp_valid, inbox = valid;
+#pragma unroll
+      for (int d = 0; d < N; ++d) {
+        const int vd = sm.seg_v[b][s][d];
+        wneed = wneed && vd >= wl[d] && vd <= wh[d];
+        inbox = inbox && vd >= lo[d] && vd <= hi[d];
+      }
+      if (!wneed) continue;
+      const float4* sb = &sm.buf[b][sm.seg_boff[b][s] * W];
+      const int qb = sm.seg_qb[b][s], cnt = sm.seg_cnt[b][s];
+      vis(inbox, sb, qb, cnt);
+    }
+    __syncthreads();
+  }
+  return ok;
+}
+
+template <int N>
+__device__ __forceinline__ void unpack_rec(const float4* r, float* c, float& payload) {
+  constexpr int W = Rec<N>::kWords;
+  float buf[4 * W];
+#pragma unroll
+  for (int k = 0; k < W; ++k) {
+    const float4 v = r[k];
+    buf[4 * k + 0] = v.x;
+    buf[4 * k + 1] = v.y;
+    buf[4 * k + 2] = v.z;
+    buf[4 * k + 3] = v.w;
+  }
+#pragma unroll
+  for (int d = 0; d < N; ++d) c[d] = buf[d];
+  payload = buf[Rec<N>::kPayload];
+}
+
 // ---- stage 2: local density --------------------------------------------------
 // rho_i accumulates, in the reference's candidate order (search-box tiles
 // lexicographically, ascending index inside a tile), term = k(d, i, j) * w_j for every
@@ -262,81 +507,61 @@ __global__ void __launch_bounds__(256) k_gather(InPtrs in, int n, const int32_t*
 template <int N, int MT>
 __global__ void __launch_bounds__(kTileThreads) k_density(const KParams kp, const DevGrid* __restrict__ g,
                                                           const int32_t* __restrict__ off,
+                                                          const int32_t* __restrict__ ord,
+                                                          const int32_t* __restrict__ chunk_tile,
+                                                          const uint32_t* __restrict__ chunk_off,
+                                                          const uint32_t* __restrict__ chunk_total,
                                                           const float4* __restrict__ rec_w,
-                                                          float4* __restrict__ rec_r) {
+                                                          float4* __restrict__ rec_r, DevStatus* st) {
   using M = Metric<N, MT>;
-  __shared__ int32_t s_order[kCap];
-  __shared__ uint8_t s_key[kCap];
-  __shared__ int32_t s_hist[N <= 4 ? (1 << (2 * N)) : 1];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  constexpr int W = Rec<N>::kWords;
+  __shared__ StageSmem<N> sm;
+  const int w = blockIdx.x;
+  if (w >= (int)*chunk_total) return;
+  const int t = chunk_tile[w];
+  const int beg = off[t];
+  const int start = (w - (int)chunk_off[t]) * kChunk;
+  const int cnt = min(kChunk, off[t + 1] - beg - start);
+  const int k = threadIdx.x;
+  const bool valid = k < cnt;
+  const int pos = ord[beg + start + (valid ? k : 0)];
+  float x[N], wi;
+  load_rec<N>(rec_w, pos, x, wi);
+  int hb[N], lo[N], hi[N];
+  home_bins<N>(kp, t, hb);
+  lane_box<N>(kp, g, x, kp.dc, hb, lo, hi);
   const bool flat = kp.kernel_type == CLUE_KERNEL_FLAT;
-  for (int t = blockIdx.x; t < kp.ntiles; t += gridDim.x) {
-    const int beg = off[t], end = off[t + 1];
-    if (beg == end) continue;
-    int hb[N];
-    home_bins<N>(kp, t, hb);
-    for (int cb = beg; cb < end; cb += kCap) {
-      const int cnt = min(kCap, end - cb);
-      signature_sort<N>(kp, g, rec_w, cb, cnt, kp.dc, hb, s_order, s_key, s_hist);
-      for (int slice = warp; slice * 32 < cnt; slice += kTileWarps) {
-        const int k = slice * 32 + lane;
-        const bool valid = k < cnt;
-        const int pos = cb + (valid ? s_order[k] : 0);
-        float x[N], wi;
-        load_rec<N>(rec_w, pos, x, wi);
-        int lo[N], hi[N], ulo[N], uhi[N];
-        lane_box<N>(kp, g, x, kp.dc, hb, lo, hi);
-#pragma unroll
-        for (int d = 0; d < N; ++d) {
-          ulo[d] = warp_min_i(valid ? lo[d] : INT_MAX);
-          uhi[d] = warp_max_i(valid ? hi[d] : INT_MIN);
-        }
-        float rho = 0.0f;
-        int v[N];
-#pragma unroll
-        for (int d = 0; d < N; ++d) v[d] = ulo[d];
-        while (true) {
-          bool inbox = valid;
-          int u = 0;
-#pragma unroll
-          for (int d = 0; d < N; ++d) {
-            inbox = inbox && v[d] >= lo[d] && v[d] <= hi[d];
-            u += kp.stride[d] * wrap_bin(v[d], kp.nperdim);
-          }
-          if (__any_sync(0xffffffffu, inbox)) {
-            const int qb = off[u], qe = off[u + 1];
+  const float kflat = kp.kpar[0];
+  const float tdc = kp.t_dc;
+  float rho = 0.0f;
+  const bool ok = staged_sweep<N>(kp, off, rec_w, sm, lo, hi, valid,
+                                  [&](bool inbox, const float4* sb, int qb, int n_) {
+    if (flat) {
 #pragma unroll 4
-            for (int q = qb; q < qe; ++q) {
-              float c[N], wj;
-              load_rec<N>(rec_w, q, c, wj);
-              const float s = M::partial(x, c, kp.mpar);
-              if (inbox && s <= kp.t_dc) {
-                float term;
-                if (flat) {
-                  term = (q == pos) ? wj : fmul(kp.kpar[0], wj);
-                } else {
-                  const float kv = (q == pos) ? 1.0f : kernel_value(kp.kernel_type, kp.kpar, M::finish(s));
-                  term = fmul(kv, wj);
-                }
-                rho = fadd(rho, term);
-              }
-            }
-          }
-          int d = N - 1;
-          for (; d >= 0; --d) {
-            if (v[d] < uhi[d]) {
-              ++v[d];
-              break;
-            }
-            v[d] = ulo[d];
-          }
-          if (d < 0) break;
-        }
-        if (valid) store_rec<N>(rec_r, pos, x, rho);
+      for (int j = 0; j < n_; ++j) {
+        float c[N], wj;
+        unpack_rec<N>(sb + j * W, c, wj);
+        const float s = M::partial(x, c, kp.mpar);
+        const float term = (qb + j == pos) ? wj : fmul(kflat, wj);
+        if (inbox && s <= tdc) rho = fadd(rho, term);
       }
-      __syncthreads();
+    } else {
+      for (int j = 0; j < n_; ++j) {
+        float c[N], wj;
+        unpack_rec<N>(sb + j * W, c, wj);
+        const float s = M::partial(x, c, kp.mpar);
+        if (inbox && s <= tdc) {
+          const float kv = (qb + j == pos) ? 1.0f : kernel_value(kp.kernel_type, kp.kpar, M::finish(s));
+          rho = fadd(rho, fmul(kv, wj));
+        }
+      }
     }
+  });
+  if (!ok) {
+    if (threadIdx.x == 0) atomicOr(&st->stage_timeout, 1u);
+    return;
   }
+  if (valid) store_rec<N>(rec_r, pos, x, rho);
 }
 
 // ---- stage 3: nearest higher -------------------------------------------------
@@ -347,105 +572,80 @@ __global__ void __launch_bounds__(kTileThreads) k_density(const KParams kp, cons
 template <int N, int MT, int TIE>
 __global__ void __launch_bounds__(kTileThreads) k_nearest_higher(
     const KParams kp, const DevGrid* __restrict__ g, const int32_t* __restrict__ off,
+    const int32_t* __restrict__ ord, const int32_t* __restrict__ chunk_tile,
+    const uint32_t* __restrict__ chunk_off, const uint32_t* __restrict__ chunk_total,
     const float4* __restrict__ rec_r, const int32_t* __restrict__ perm, int32_t* __restrict__ nh_s,
     float* __restrict__ delta_s, DevStatus* st) {
   using M = Metric<N, MT>;
-  __shared__ int32_t s_order[kCap];
-  __shared__ uint8_t s_key[kCap];
-  __shared__ int32_t s_hist[N <= 4 ? (1 << (2 * N)) : 1];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int t = blockIdx.x; t < kp.ntiles; t += gridDim.x) {
-    const int beg = off[t], end = off[t + 1];
-    if (beg == end) continue;
-    int hb[N];
-    home_bins<N>(kp, t, hb);
-    for (int cb = beg; cb < end; cb += kCap) {
-      const int cnt = min(kCap, end - cb);
-      signature_sort<N>(kp, g, rec_r, cb, cnt, kp.dm, hb, s_order, s_key, s_hist);
-      for (int slice = warp; slice * 32 < cnt; slice += kTileWarps) {
-        const int k = slice * 32 + lane;
-        const bool valid = k < cnt;
-        const int pos = cb + (valid ? s_order[k] : 0);
-        float x[N], rho_i;
-        load_rec<N>(rec_r, pos, x, rho_i);
-        const int orig_i = perm[pos];
-        int lo[N], hi[N], ulo[N], uhi[N];
-        lane_box<N>(kp, g, x, kp.dm, hb, lo, hi);
-#pragma unroll
-        for (int d = 0; d < N; ++d) {
-          ulo[d] = warp_min_i(valid ? lo[d] : INT_MAX);
-          uhi[d] = warp_max_i(valid ? hi[d] : INT_MIN);
-        }
-        float delta = FLT_MAX, s_best = INFINITY, rho_best = 0.0f;
-        int nh = -1, orig_best = INT_MAX;
-        int v[N];
-#pragma unroll
-        for (int d = 0; d < N; ++d) v[d] = ulo[d];
-        while (true) {
-          bool inbox = valid;
-          int u = 0;
-#pragma unroll
-          for (int d = 0; d < N; ++d) {
-            inbox = inbox && v[d] >= lo[d] && v[d] <= hi[d];
-            u += kp.stride[d] * wrap_bin(v[d], kp.nperdim);
-          }
-          if (__any_sync(0xffffffffu, inbox)) {
-            const int qb = off[u], qe = off[u + 1];
+  constexpr int W = Rec<N>::kWords;
+  __shared__ StageSmem<N> sm;
+  const int w = blockIdx.x;
+  if (w >= (int)*chunk_total) return;
+  const int t = chunk_tile[w];
+  const int beg = off[t];
+  const int start = (w - (int)chunk_off[t]) * kChunk;
+  const int cnt = min(kChunk, off[t + 1] - beg - start);
+  const int k = threadIdx.x;
+  const bool valid = k < cnt;
+  const int pos = ord[beg + start + (valid ? k : 0)];
+  float x[N], rho_i;
+  load_rec<N>(rec_r, pos, x, rho_i);
+  const int orig_i = perm[pos];
+  int hb[N], lo[N], hi[N];
+  home_bins<N>(kp, t, hb);
+  lane_box<N>(kp, g, x, kp.dm, hb, lo, hi);
+  const float tdm = kp.t_dm;
+  float delta = FLT_MAX, s_best = INFINITY, rho_best = 0.0f;
+  int nh = -1, orig_best = INT_MAX;
+  const bool ok = staged_sweep<N>(kp, off, rec_r, sm, lo, hi, valid,
+                                  [&](bool inbox, const float4* sb, int qb, int n_) {
+    if (!__any_sync(0xffffffffu, inbox)) return;
 #pragma unroll 4
-            for (int q = qb; q < qe; ++q) {
-              float c[N], rho_j;
-              load_rec<N>(rec_r, q, c, rho_j);
-              const float s = M::partial(x, c, kp.mpar);
-              bool cand = inbox && s <= kp.t_dm && rho_j >= rho_i;
-              if (TIE == CLUE_TIE_REFERENCE) cand = cand && s < s_best;
-              if (cand) {
-                int orig_j = -1;
-                bool higher = rho_j > rho_i;
-                if (!higher && rho_j > 0.0f) {
-                  orig_j = __ldg(perm + q);
-                  higher = orig_j > orig_i;
-                }
-                if (higher) {
-                  const float dist = M::finish(s);
-                  if (dist < delta) {
-                    delta = dist;
-                    s_best = s;
-                    nh = q;
-                    rho_best = rho_j;
-                    orig_best = orig_j;
-                  } else if (TIE == CLUE_TIE_RHO_INDEX && dist == delta) {
-                    if (orig_j < 0) orig_j = __ldg(perm + q);
-                    if (orig_best < 0) orig_best = __ldg(perm + nh);
-                    if (rho_j > rho_best || (rho_j == rho_best && orig_j < orig_best)) {
-                      nh = q;
-                      rho_best = rho_j;
-                      orig_best = orig_j;
-                    }
-                  }
-                }
-              }
+    for (int j = 0; j < n_; ++j) {
+      float c[N], rho_j;
+      unpack_rec<N>(sb + j * W, c, rho_j);
+      const float s = M::partial(x, c, kp.mpar);
+      bool cand = inbox && s <= tdm && rho_j >= rho_i;
+      if (TIE == CLUE_TIE_REFERENCE) cand = cand && s < s_best;
+      if (cand) {
+        const int q = qb + j;
+        int orig_j = -1;
+        bool higher = rho_j > rho_i;
+        if (!higher && rho_j > 0.0f) {
+          orig_j = __ldg(perm + q);
+          higher = orig_j > orig_i;
+        }
+        if (higher) {
+          const float dist = M::finish(s);
+          if (dist < delta) {
+            delta = dist;
+            s_best = s;
+            nh = q;
+            rho_best = rho_j;
+            orig_best = orig_j;
+          } else if (TIE == CLUE_TIE_RHO_INDEX && dist == delta) {
+            if (orig_j < 0) orig_j = __ldg(perm + q);
+            if (orig_best < 0) orig_best = __ldg(perm + nh);
+            if (rho_j > rho_best || (rho_j == rho_best && orig_j < orig_best)) {
+              nh = q;
+              rho_best = rho_j;
+              orig_best = orig_j;
             }
           }
-          int d = N - 1;
-          for (; d >= 0; --d) {
-            if (v[d] < uhi[d]) {
-              ++v[d];
-              break;
-            }
-            v[d] = ulo[d];
-          }
-          if (d < 0) break;
         }
-        if (valid) {
-          nh_s[pos] = nh;
-          delta_s[pos] = delta;
-        }
-        const uint32_t none = __ballot_sync(0xffffffffu, valid && nh < 0);
-        if (lane == 0 && none) atomicAdd(&st->seed_candidates, (uint32_t)__popc(none));
       }
-      __syncthreads();
     }
+  });
+  if (!ok) {
+    if (threadIdx.x == 0) atomicOr(&st->stage_timeout, 1u);
+    return;
   }
+  if (valid) {
+    nh_s[pos] = nh;
+    delta_s[pos] = delta;
+  }
+  const uint32_t none = __ballot_sync(0xffffffffu, valid && nh < 0);
+  if ((threadIdx.x & 31) == 0 && none) atomicAdd(&st->seed_candidates, (uint32_t)__popc(none));
 }
 
 // ---- stage 4: seeds (KernelFindClusters) ---------------------------------------
@@ -547,18 +747,24 @@ int grid_for(int n, int threads) {
   return b < 1 ? 1 : (b > cap ? cap : b);
 }
 
+inline int chunk_grid(const KParams& kp) { return kp.n / kChunk + kp.ntiles + 1; }
+
 template <int N, int MT>
 void launch_density(const KParams& kp, Workspace& ws, cudaStream_t s) {
-  k_density<N, MT><<<kp.ntiles, kTileThreads, 0, s>>>(kp, ws.grid, ws.offsets, ws.rec_w, ws.rec_r);
+  k_density<N, MT><<<chunk_grid(kp), kTileThreads, 0, s>>>(kp, ws.grid, ws.offsets, ws.ord_rho, ws.chunk_tile,
+                                                            ws.chunk_count, ws.chunk_total, ws.rec_w, ws.rec_r,
+                                                            ws.status);
 }
 template <int N, int MT>
 void launch_nh(const KParams& kp, Workspace& ws, cudaStream_t s) {
   if (kp.tiebreak == CLUE_TIE_RHO_INDEX)
-    k_nearest_higher<N, MT, CLUE_TIE_RHO_INDEX><<<kp.ntiles, kTileThreads, 0, s>>>(
-        kp, ws.grid, ws.offsets, ws.rec_r, ws.perm, ws.nh_s, ws.delta_s, ws.status);
+    k_nearest_higher<N, MT, CLUE_TIE_RHO_INDEX><<<chunk_grid(kp), kTileThreads, 0, s>>>(
+        kp, ws.grid, ws.offsets, ws.ord_nh, ws.chunk_tile, ws.chunk_count, ws.chunk_total, ws.rec_r, ws.perm,
+        ws.nh_s, ws.delta_s, ws.status);
   else
-    k_nearest_higher<N, MT, CLUE_TIE_REFERENCE><<<kp.ntiles, kTileThreads, 0, s>>>(
-        kp, ws.grid, ws.offsets, ws.rec_r, ws.perm, ws.nh_s, ws.delta_s, ws.status);
+    k_nearest_higher<N, MT, CLUE_TIE_REFERENCE><<<chunk_grid(kp), kTileThreads, 0, s>>>(
+        kp, ws.grid, ws.offsets, ws.ord_nh, ws.chunk_tile, ws.chunk_count, ws.chunk_total, ws.rec_r, ws.perm,
+        ws.nh_s, ws.delta_s, ws.status);
 }
 template <int N, int MT>
 void launch_seeds(const KParams& kp, Workspace& ws, int n, cudaStream_t s) {
@@ -605,6 +811,10 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
   ws.sorted_keys = ws.keys[cur];
   offsets_from_sorted(ws.sorted_keys, n, kp.ntiles, ws.offsets, s);
   k_gather<N><<<grid_for(n, 256), 256, 0, s>>>(in, n, ws.perm, ws.rec_w);
+  k_order<N><<<kp.ntiles, kTileThreads, 0, s>>>(kp, ws.grid, ws.offsets, ws.rec_w, ws.ord_rho, ws.ord_nh,
+                                                ws.chunk_count);
+  exclusive_scan(ws.chunk_count, ws.chunk_count, (size_t)kp.ntiles, ws.scan_scratch, ws.chunk_total, s);
+  k_chunk_map<<<grid_for(kp.ntiles, 256), 256, 0, s>>>(kp.ntiles, ws.offsets, ws.chunk_count, ws.chunk_tile);
 
   stage_mark(ws, 1, s);
   CLUE_METRIC_SWITCH(a.metric, launch_density, kp, ws, s);
@@ -618,9 +828,10 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
   k_finalize<N><<<grid_for(n, 256), 256, 0, s>>>(kp, n, ws.par, ws.is_seed_s, ws.seed_flag, ws.perm, ws.nh_s,
                                                  ws.rec_r, ws.delta_s, ws.status, a.out);
   stage_mark(ws, 4, s);
-  // init, bbox, grid, bin, sort, offsets, gather, density, nh, seeds, scan, jumps, finalize
-  ws.launches += 4 + radix_sort_launches(bits_for((uint32_t)(kp.ntiles - 1))) + 2 + 3 + kScanLaunches +
-                 kJumpLaunches + 1;
+  // init, bbox, grid, bin, sort, offsets, gather, order, scan, chunk map, density, nh, seeds, scan,
+  // jumps, finalize
+  ws.launches += 4 + radix_sort_launches(bits_for((uint32_t)(kp.ntiles - 1))) + 2 + 1 + kScanLaunches + 1 + 3 +
+                 kScanLaunches + kJumpLaunches + 1;
   CLUE_CUDA_TRY(cudaGetLastError());
   return CLUE_OK;
 }

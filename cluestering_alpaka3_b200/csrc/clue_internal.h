@@ -29,6 +29,7 @@ constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortThreads * kSortItems;  // keys per radix block
 constexpr int kRadixBits = 8;
 constexpr int kRadix = 1 << kRadixBits;
+constexpr int kChunkPoints = 128;  // home points per CTA of the density / nearest-higher sweeps
 constexpr int kScanThreads = 256;
 constexpr int kScanItems = 8;
 constexpr int kScanTile = kScanThreads * kScanItems;
@@ -102,6 +103,11 @@ struct Workspace {
   int32_t* is_seed_s = nullptr;
   uint32_t* seed_flag = nullptr;  // original order, then exclusive-scanned to ranks
   uint32_t* seed_total = nullptr;
+  int32_t* ord_rho = nullptr;     // per-tile home order for the density sweep
+  int32_t* ord_nh = nullptr;      // per-tile home order for the nearest-higher sweep
+  uint32_t* chunk_count = nullptr;  // [ntiles] chunks per tile, then exclusive-scanned
+  int32_t* chunk_tile = nullptr;  // [max chunks] tile of every chunk
+  uint32_t* chunk_total = nullptr;
 
   // host staging for CLUE_MEM_HOST calls
   void* pinned = nullptr;

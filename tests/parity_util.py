@@ -51,9 +51,10 @@ def assert_exact(ref, got, check_rho=True):
 
 def random_blobs(rng, n, ndim, nblobs=8, extent=100.0, sigma=1.0, noise=0.1, weights="uniform"):
     per = int(n * (1 - noise)) // nblobs
-    centres = rng.uniform(0.1 * extent, 0.9 * extent, size=(nblobs, ndim))
+    lo, hi = sorted((0.0, float(extent)))
+    centres = rng.uniform(lo + 0.1 * (hi - lo), hi - 0.1 * (hi - lo), size=(nblobs, ndim))
     blobs = (centres[:, None, :] + rng.normal(0, sigma, size=(nblobs, per, ndim))).reshape(-1, ndim)
-    rest = rng.uniform(0, extent, size=(n - per * nblobs, ndim))
+    rest = rng.uniform(lo, hi, size=(n - per * nblobs, ndim))
     c = np.concatenate([blobs, rest]).T.astype(np.float32)
     if weights == "ones":
         w = np.ones(n, np.float32)
