@@ -36,7 +36,7 @@ EXPORTED = [
     "clue_context_create", "clue_context_destroy", "clue_context_reserve",
     "clue_context_workspace_bytes", "clue_make_clusters", "clue_make_clusters_async",
     "clue_context_read_info", "clue_get_clusters", "clue_context_set_timing",
-    "clue_context_stage_times", "clue_context_kernel_launches",
+    "clue_context_stage_times", "clue_context_kernel_launches", "clue_make_clusters_noalloc",
 ]
 
 
@@ -122,6 +122,10 @@ def _load() -> ctypes.CDLL:
         "clue_context_set_timing": ([vp, i32], ctypes.c_int),
         "clue_context_stage_times": ([vp, ctypes.POINTER(f32), i32], ctypes.c_int),
         "clue_context_kernel_launches": ([vp], ctypes.c_uint64),
+        "clue_make_clusters_noalloc": ([ctypes.POINTER(_Params), ctypes.POINTER(_Kernel),
+                                        ctypes.POINTER(_Metric), i32, i32, vp, vp,
+                                        ctypes.POINTER(_Outputs), vp, ctypes.POINTER(_RunInfo)],
+                                       ctypes.c_int),
         "clue_get_clusters": ([vp, i32, vp, vp, vp, ctypes.POINTER(i32), ctypes.POINTER(i32), vp],
                               ctypes.c_int),
     }

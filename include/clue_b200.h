@@ -205,6 +205,25 @@ clue_status clue_context_stage_times(clue_context ctx, float* ms, int32_t n_stag
 uint64_t clue_context_kernel_launches(clue_context ctx);
 
 /*
+ * clue_make_clusters_noalloc -- no counterpart in the reference.
+ * The same pipeline for callers that cannot allocate device memory (a runtime that owns all
+ * device memory through its own pool, a plugin inside another framework, or a
+ * latency-critical path that cannot afford cudaMalloc's implicit synchronisation).  Inputs
+ * and outputs are the caller's device buffers; every intermediate buffer lives in one
+ * fixed 6 MiB file-scope device array, so the call allocates nothing.
+ * Limits: n <= 32768 points and at most 65536 tiles; larger requests return
+ * CLUE_ERR_CAPACITY.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current: make that first call before any stream
+ * capture.  All calls on a device share the array (it keeps the last call's contents);
+ * calls that overlap on the GPU race and must be serialised by the caller.  Blocks until
+ * the results are in `out`; `info` may be NULL.
+ */
+clue_status clue_make_clusters_noalloc(const clue_params* params, const clue_kernel* kernel,
+                                       const clue_metric* metric, int32_t ndim, int32_t n,
+                                       const float* coords, const float* weight,
+                                       const clue_outputs* out, void* stream, clue_run_info* info);
+
+/*
  * Cluster -> points association map (CSR) from device labels: offsets[n_clusters + 1],
  * points[n_clustered] (point indexes ascending inside each cluster).  All device
  * pointers; `offsets` must hold max_label + 2 entries and `points` n entries.
