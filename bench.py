@@ -42,8 +42,23 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
+class Events:
+    """A batched workload: events concatenated into one SoA buffer with offsets."""
+
+    def __init__(self, name, events, dc, rhoc, dm, kernel):
+        self.name = name
+        self.events = events
+        self.offsets = np.concatenate([[0], np.cumsum([e[0].shape[1] for e in events])]).astype(np.int32)
+        self.coords = np.ascontiguousarray(np.concatenate([e[0] for e in events], axis=1))
+        self.weight = np.ascontiguousarray(np.concatenate([e[1] for e in events]))
+        self.dc, self.rhoc, self.dm, self.kernel = dc, rhoc, dm, kernel
+
+
 def make_workload(name: str, rank: int):
     from cluestering_alpaka3_b200 import synthetic
+    if name == "calo4096":
+        evs, p = synthetic.calo_events(4096, seed=4000 + rank)
+        return Events("calo4096", evs, p["dc"], p["rhoc"], p["dm"], p["kernel"])
     if name == "blobs2d_1m":
         return synthetic.blobs_2d_1m(seed=2000 + rank)
     if name == "blobs2d_16k":
@@ -93,13 +108,32 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+CPU_SAMPLE_EVENTS = 512
+
+
 def cpu_baseline_run(wl, nthreads: int):
+    """The CPU restatement on the workload (batched workloads: its first CPU_SAMPLE_EVENTS
+    events, each clustered alone).  Returns (seconds, points, last result)."""
     from oracle import oracle as O
     kname, kpar = wl.kernel
     cfg = O.Config(dc=wl.dc, rhoc=wl.rhoc, dm=wl.dm, kernel=kname, kernel_par=kpar, nthreads=nthreads)
+    if isinstance(wl, Events):
+        pts, r = 0, None
+        t0 = time.perf_counter()
+        for c, w in wl.events[:CPU_SAMPLE_EVENTS]:
+            r = O.run(c, w, cfg)
+            pts += c.shape[1]
+        return time.perf_counter() - t0, pts, r
     t0 = time.perf_counter()
     r = O.run(wl.coords, wl.weight, cfg)
-    return time.perf_counter() - t0, r
+    return time.perf_counter() - t0, wl.coords.shape[1], r
+
+
+def sample_text(wl) -> str:
+    if isinstance(wl, Events):
+        n = int(wl.offsets[min(CPU_SAMPLE_EVENTS, len(wl.events))])
+        return f"first {CPU_SAMPLE_EVENTS} of {len(wl.events)} {wl.name} events ({n} points), each clustered alone"
+    return f"full {wl.name} workload ({wl.coords.shape[1]} points)"
 
 
 def reference_arm(args, rank: int):
@@ -112,14 +146,13 @@ def reference_arm(args, rank: int):
     wl = make_workload(args.workload, 0)
     n = wl.coords.shape[1]
     cores = os.cpu_count() or 1
-    for _ in range(max(1, min(args.warmup, 1))):
-        cpu_baseline_run(wl, cores)
-    times = []
+    cpu_baseline_run(wl, cores)
+    times, pts = [], 0
     for _ in range(args.steps):
-        dt, _ = cpu_baseline_run(wl, cores)
+        dt, pts, _ = cpu_baseline_run(wl, cores)
         times.append(dt)
     tot = sum(times)
-    v = n * len(times) / tot
+    v = pts * len(times) / tot
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "points/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -127,7 +160,7 @@ def reference_arm(args, rank: int):
             "config": {"workload": wl.name, "n_points": n, "ndim": wl.coords.shape[0], "dc": wl.dc,
                        "rhoc": wl.rhoc, "dm": wl.dm, "kernel": list(wl.kernel)},
             "cpu_baseline": {"value": v, "unit": "points/s", "cores": cores, "kind": "port",
-                             "sample": f"full {wl.name} workload ({n} points) per step"},
+                             "sample": sample_text(wl) + " per step, OpenMP over points"},
             "e2e": {"value": v, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -138,7 +171,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="blobs2d_1m")
+    ap.add_argument("--workload", default="calo4096",
+                    choices=["calo4096", "blobs2d_16k", "blobs2d_1m", "blobs3d_4m"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
 
@@ -156,45 +190,48 @@ def main():
     torch.cuda.set_device(local)
     if world > 1:
         from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
 
     from cluestering_alpaka3_b200 import bytes_model, capi
 
     wl = make_workload(args.workload, rank)
+    batched = isinstance(wl, Events)
     ndim, n = wl.coords.shape
+    dev = f"cuda:{local}"
     kname, kpar = wl.kernel
     kernel = {"flat": capi.FlatKernel, "exp": capi.ExponentialKernel, "gaus": capi.GaussianKernel}[kname](*kpar)
     params = capi.Params(dc=wl.dc, rhoc=wl.rhoc, dm=wl.dm)
     metric = capi.Metric()
 
     ctx = capi.Context(local)
-    ctx.reserve(ndim, n)
     stream = torch.cuda.Stream(device=local)
     sp = stream.cuda_stream
-    dcoords = torch.from_numpy(wl.coords).cuda(local)
-    dweight = torch.from_numpy(wl.weight).cuda(local)
-    outs = {k: torch.empty(n, dtype=dt, device=f"cuda:{local}") for k, dt in
+    dcoords = torch.from_numpy(wl.coords).to(dev)
+    dweight = torch.from_numpy(wl.weight).to(dev)
+    outs = {k: torch.empty(n, dtype=dt, device=dev) for k, dt in
             (("cluster_index", torch.int32), ("is_seed", torch.int32), ("rho", torch.float32),
              ("nearest_higher", torch.int32), ("delta", torch.float32))}
     optr = {k: v.data_ptr() for k, v in outs.items()}
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    E = len(wl.offsets) - 1 if batched else 1
+    offsets = wl.offsets if batched else np.array([0, n], np.int32)
+    ncl = torch.zeros(E, dtype=torch.int32, device=dev)
 
-    def step_device():
-        ctx.make_clusters_device(dcoords.data_ptr(), dweight.data_ptr(), ndim, n, optr, params, kernel,
-                                 metric, stream=sp, blocking=False)
+    # the step: one replay of the whole pipeline captured in a CUDA graph
+    graph = ctx.capture_batch(dcoords.data_ptr(), dweight.data_ptr(), ndim, offsets, optr, params, kernel, metric,
+                              ncl_ptr=ncl.data_ptr(), stream=sp)
+
+    def step():
+        graph.launch(sp)
 
     torch.cuda.synchronize()
     for _ in range(args.warmup):
-        step_device()
-    info = ctx.read_info(sp)
+        step()
     torch.cuda.synchronize()
 
     # ---- timed device-resident steps --------------------------------------
-    ctx.set_timing(True)
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    stage_ms = np.zeros(4)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -204,44 +241,72 @@ def main():
         with torch.cuda.stream(stream):
             flush.zero_()
             starts[k].record(stream)
-        step_device()
+        step()
         with torch.cuda.stream(stream):
             ends[k].record(stream)
-        stage_ms += np.array(ctx.stage_times())
     torch.cuda.synchronize()
     clk = clocks.stop()
-    launches = ctx.kernel_launches - launches0
-    ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    ms = [s_.elapsed_time(e_) for s_, e_ in zip(starts, ends)]
     total_ms = float(sum(ms))
     if world > 1:
-        t = torch.tensor([total_ms], device=f"cuda:{local}")
+        t = torch.tensor([total_ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
         dist.barrier()
-    ctx.set_timing(False)
     value = world * n * args.steps / (total_ms / 1e3)
+    n_clusters = int(ncl.sum().item())
+
+    # launches per graph replay = the launches the capture enqueued
+    ctx.batch_device(dcoords.data_ptr(), dweight.data_ptr(), ndim, offsets, optr, params, kernel, metric,
+                     stream=sp, blocking=False)
+    per_step_launches = ctx.kernel_launches - launches0
+    launches = per_step_launches * args.steps
+
+    # ---- per-stage device times of the same pipeline (events around stages) ------
+    ctx.set_timing(True)
+    stage_ms = np.zeros(4)
+    for _ in range(3):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        ctx.batch_device(dcoords.data_ptr(), dweight.data_ptr(), ndim, offsets, optr, params, kernel, metric,
+                         stream=sp, blocking=False)
+        stage_ms += np.array(ctx.stage_times())
+    ctx.set_timing(False)
+    stage_avg = stage_ms / 3
+
+    # ---- the plain per-event launch loop on the same events -----------------------
+    plain = None
+    if batched:
+        torch.cuda.synchronize()
+        ev_ms = ctx.events_loop(dcoords.data_ptr(), dweight.data_ptr(), ndim, offsets, optr, params, kernel,
+                                metric, stream=sp, event_times=True)
+        ev_ms = ctx.events_loop(dcoords.data_ptr(), dweight.data_ptr(), ndim, offsets, optr, params, kernel,
+                                metric, stream=sp, event_times=True)
+        loop_ms = float(ev_ms.sum())
+        plain = {"points_per_s": n / (loop_ms / 1e3), "ms_per_pass": loop_ms,
+                 "event_latency_ms": {"p50": float(np.percentile(ev_ms, 50)),
+                                      "p99": float(np.percentile(ev_ms, 99))}}
 
     # ---- end to end through the C ABI with pinned host buffers ----------------
     hc = torch.from_numpy(wl.coords).pin_memory().numpy()
     hw = torch.from_numpy(wl.weight).pin_memory().numpy()
     for _ in range(2):
-        res = ctx.make_clusters_host(hc, hw, params, kernel, metric, stream=sp)
+        res, hncl = ctx.batch_host(hc, hw, offsets, params, kernel, metric, stream=sp)
     e2e_ms = []
     for _ in range(args.steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        res = ctx.make_clusters_host(hc, hw, params, kernel, metric, stream=sp)
+        res, hncl = ctx.batch_host(hc, hw, offsets, params, kernel, metric, stream=sp)
         e2e_ms.append(1e3 * (time.perf_counter() - t0))
     e2e_total = float(sum(e2e_ms))
     if world > 1:
-        t = torch.tensor([e2e_total], device=f"cuda:{local}")
+        t = torch.tensor([e2e_total], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_total = float(t.item())
 
     # ---- roofline of the dominant kernel (local density) ------------------------
     peak, peak_kind = load_peaks()
-    B = bytes_model.algorithmic_bytes(wl.coords, wl.dc, wl.dm)
-    stage_avg = stage_ms / args.steps
+    B = bytes_model.algorithmic_bytes(wl.coords, wl.dc, wl.dm, offsets)
     dens_ms = float(stage_avg[1])
     achieved = B["density_kernel"] / (dens_ms / 1e3) / 1e9
     traffic = None
@@ -253,36 +318,41 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
-        dt, ref = cpu_baseline_run(wl, cores)
-        same = bool(np.array_equal(ref.cluster_index, res.cluster_index))
-        cpu = {"value": n / dt, "unit": "points/s", "cores": cores, "kind": "port",
-               "sample": f"full {wl.name} workload ({n} points), OpenMP over points",
-               "labels_equal_to_gpu": same}
+        dt, pts, ref = cpu_baseline_run(wl, cores)
+        cpu = {"value": pts / dt, "unit": "points/s", "cores": cores, "kind": "port",
+               "sample": sample_text(wl) + ", OpenMP over points"}
+        if not batched:
+            cpu["labels_equal_to_gpu"] = bool(np.array_equal(ref.cluster_index, res.cluster_index))
 
     if rank == 0:
+        step_ms = total_ms / args.steps
+        config = {"workload": wl.name, "n_points": n, "ndim": ndim, "dc": wl.dc, "rhoc": wl.rhoc, "dm": wl.dm,
+                  "kernel": [kname, list(kpar)], "metric": "euclidean", "points_per_tile": 128,
+                  "l2": "flushed between steps (256 MiB write)",
+                  "parallelism": "replicas" if world > 1 else "single", "n_clusters": n_clusters,
+                  "step": "one CUDA-graph replay of the whole pipeline"}
+        if batched:
+            config.update({"n_events": E, "batched_points_per_s": value / world,
+                           "plain_loop": plain, "batched_vs_plain": (value / world) / plain["points_per_s"],
+                           "batched_event_latency_ms": {"p50": step_ms, "p99": step_ms}})
         line = {
             "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": wl.name, "n_points": n, "ndim": ndim, "dc": wl.dc, "rhoc": wl.rhoc,
-                       "dm": wl.dm, "kernel": [kname, list(kpar)], "metric": "euclidean",
-                       "l2": "flushed between steps (256 MiB write)",
-                       "parallelism": "replicas" if world > 1 else "single",
-                       "n_clusters": int(info.n_clusters), "n_tiles": int(info.n_tiles)},
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config,
             "e2e": {"value": world * n * args.steps / (e2e_total / 1e3), "unit": "points/s",
-                    "h2d_bytes_per_step": int(n * (ndim + 1) * 4),
-                    "d2h_bytes_per_step": int(n * 5 * 4)},
+                    "h2d_bytes_per_step": int(n * (ndim + 1) * 4 + 12 * E + 264 * E),
+                    "d2h_bytes_per_step": int(n * 5 * 4 + 4 * E)},
             "roofline": {"bound": "hbm", "kernel": "k_density", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                         "traffic": traffic, "algorithmic_bytes": B["density_kernel"],
-                         "launch_ms": dens_ms},
+                         "traffic": traffic, "algorithmic_bytes": B["density_kernel"], "launch_ms": dens_ms},
             "stage_ms": {"tiles": stage_avg[0], "density": stage_avg[1], "nearest_higher": stage_avg[2],
                          "seeds_labels": stage_avg[3]},
             "b_alg_total": B["total"],
-            "pipeline_hbm_frac": B["total"] / (total_ms / args.steps / 1e3) / 1e9 / peak,
+            "pipeline_hbm_frac": B["total"] / (step_ms / 1e3) / 1e9 / peak,
             "cpu_baseline": cpu, "clocks": clk, "gpu_launches": int(launches),
         }
         print(json.dumps(line), flush=True)
+    graph.close()
     ctx.close()
     if world > 1:
         dist.destroy_process_group()

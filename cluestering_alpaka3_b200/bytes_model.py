@@ -25,18 +25,24 @@ def term1(n: int, ndim: int) -> dict:
     }
 
 
-def neighbour_traffic(coords: np.ndarray, r: float) -> int:
-    """sum_c sum_{c' in 3^N(c)} |c'| * (4N + 4) on a grid of edge r (0 when it cannot be keyed)."""
+def neighbour_traffic(coords: np.ndarray, r: float, offsets=None) -> int:
+    """sum_c sum_{c' in 3^N(c)} |c'| * (4N + 4) on a grid of edge r (0 when it cannot be keyed).
+    With `offsets` (event boundaries) every event has its own grid and cells never span events."""
     ndim, n = coords.shape
-    mn = coords.min(axis=1).astype(np.float64)
-    cells = np.floor((coords.astype(np.float64) - mn[:, None]) / r).astype(np.int64) + 1
+    if offsets is None:
+        offsets = np.array([0, n])
+    offsets = np.asarray(offsets, np.int64)
+    E = len(offsets) - 1
+    ev = np.repeat(np.arange(E, dtype=np.int64), np.diff(offsets))
+    mn = np.minimum.reduceat(coords.astype(np.float64), offsets[:-1], axis=1)
+    cells = np.floor((coords.astype(np.float64) - mn[:, ev]) / r).astype(np.int64) + 1
     extent = cells.max(axis=1) + 2
-    if float(np.prod(extent.astype(np.float64))) > 2.0 ** 62:
+    if float(np.prod(extent.astype(np.float64))) * E > 2.0 ** 62:
         return 0
     mult = np.ones(ndim, np.int64)
     for d in range(ndim - 2, -1, -1):
         mult[d] = mult[d + 1] * extent[d + 1]
-    keys = (cells * mult[:, None]).sum(axis=0)
+    keys = (cells * mult[:, None]).sum(axis=0) + ev * int(mult[0] * extent[0])
     uk, cnt = np.unique(keys, return_counts=True)
     offs = np.array(np.meshgrid(*[[-1, 0, 1]] * ndim, indexing="ij")).reshape(ndim, -1)
     total = 0
@@ -49,11 +55,11 @@ def neighbour_traffic(coords: np.ndarray, r: float) -> int:
     return total * (4 * ndim + 4)
 
 
-def algorithmic_bytes(coords: np.ndarray, dc: float, dm: float) -> dict:
+def algorithmic_bytes(coords: np.ndarray, dc: float, dm: float, offsets=None) -> dict:
     ndim, n = coords.shape
     t1 = term1(n, ndim)
-    rho2 = neighbour_traffic(coords, dc)
-    nh2 = neighbour_traffic(coords, dm)
+    rho2 = neighbour_traffic(coords, dc, offsets)
+    nh2 = neighbour_traffic(coords, dm, offsets)
     out = dict(t1)
     out["density_neighbours"] = rho2
     out["nearest_higher_neighbours"] = nh2

@@ -37,6 +37,8 @@ EXPORTED = [
     "clue_context_workspace_bytes", "clue_make_clusters", "clue_make_clusters_async",
     "clue_context_read_info", "clue_get_clusters", "clue_context_set_timing",
     "clue_context_stage_times", "clue_context_kernel_launches", "clue_make_clusters_noalloc",
+    "clue_batch_make_clusters", "clue_batch_make_clusters_async", "clue_graph_capture_batch",
+    "clue_graph_launch", "clue_graph_destroy", "clue_events_loop",
 ]
 
 
@@ -129,6 +131,14 @@ def _load() -> ctypes.CDLL:
         "clue_get_clusters": ([vp, i32, vp, vp, vp, ctypes.POINTER(i32), ctypes.POINTER(i32), vp],
                               ctypes.c_int),
     }
+    batch_args = [vp, ctypes.POINTER(_Params), ctypes.POINTER(_Kernel), ctypes.POINTER(_Metric), i32, i32, vp,
+                  vp, vp, ctypes.POINTER(_Outputs), vp]
+    sig["clue_batch_make_clusters"] = (batch_args + [i32, vp, ctypes.POINTER(_RunInfo)], ctypes.c_int)
+    sig["clue_batch_make_clusters_async"] = (batch_args + [vp], ctypes.c_int)
+    sig["clue_graph_capture_batch"] = (batch_args + [vp, ctypes.POINTER(vp)], ctypes.c_int)
+    sig["clue_graph_launch"] = ([vp, vp], ctypes.c_int)
+    sig["clue_events_loop"] = (batch_args[:-1] + [vp, vp], ctypes.c_int)
+    sig["clue_graph_destroy"] = ([vp], ctypes.c_int)
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
         f.argtypes = args
@@ -362,7 +372,111 @@ class Context:
     def kernel_launches(self) -> int:
         return lib.clue_context_kernel_launches(self.handle)
 
+    def _batch_structs(self, ndim, params, kernel, metric, event_offsets):
+        off = np.ascontiguousarray(event_offsets, dtype=np.int32)
+        return (params.struct(), (kernel or FlatKernel(0.5)).struct(), (metric or Metric()).struct(ndim), off)
+
+    def batch_host(self, coords: np.ndarray, weight: np.ndarray, event_offsets, params: Params,
+                   kernel: Kernel | None = None, metric: Metric | None = None, stream: int = 0):
+        """Cluster concatenated events (host arrays); returns (Result, n_clusters per event)."""
+        c = np.ascontiguousarray(coords, dtype=np.float32)
+        if c.ndim == 1:
+            c = c[None, :]
+        ndim, n = c.shape
+        w = np.ascontiguousarray(weight, dtype=np.float32)
+        p, k, m, off = self._batch_structs(ndim, params, kernel, metric, event_offsets)
+        E = len(off) - 1
+        res = Result(np.empty(n, np.int32), np.empty(n, np.int32), np.empty(n, np.float32),
+                     np.empty(n, np.int32), np.empty(n, np.float32))
+        out = _Outputs()
+        for name in ("cluster_index", "is_seed", "rho", "nearest_higher", "delta"):
+            setattr(out, name, getattr(res, name).ctypes.data)
+        ncl = np.empty(E, np.int32)
+        info = _RunInfo()
+        check(lib.clue_batch_make_clusters(self.handle, ctypes.byref(p), ctypes.byref(k), ctypes.byref(m), ndim,
+                                           E, off.ctypes.data, c.ctypes.data, w.ctypes.data, ctypes.byref(out),
+                                           ncl.ctypes.data, MEM_HOST, ctypes.c_void_p(stream),
+                                           ctypes.byref(info)))
+        res.info = RunInfo(**{f: getattr(info, f) for f, _ in _RunInfo._fields_})
+        return res, ncl
+
+    def batch_device(self, coords_ptr: int, weight_ptr: int, ndim: int, event_offsets, out_ptrs: dict,
+                     params: Params, kernel: Kernel | None = None, metric: Metric | None = None,
+                     ncl_ptr: int = 0, stream: int = 0, blocking: bool = True):
+        p, k, m, off = self._batch_structs(ndim, params, kernel, metric, event_offsets)
+        E = len(off) - 1
+        out = _Outputs()
+        for name in ("cluster_index", "is_seed", "rho", "nearest_higher", "delta"):
+            setattr(out, name, out_ptrs.get(name) or None)
+        if blocking:
+            info = _RunInfo()
+            check(lib.clue_batch_make_clusters(self.handle, ctypes.byref(p), ctypes.byref(k), ctypes.byref(m),
+                                               ndim, E, off.ctypes.data, ctypes.c_void_p(coords_ptr),
+                                               ctypes.c_void_p(weight_ptr), ctypes.byref(out),
+                                               ctypes.c_void_p(ncl_ptr or None), MEM_DEVICE,
+                                               ctypes.c_void_p(stream), ctypes.byref(info)))
+            return RunInfo(**{f: getattr(info, f) for f, _ in _RunInfo._fields_})
+        check(lib.clue_batch_make_clusters_async(self.handle, ctypes.byref(p), ctypes.byref(k), ctypes.byref(m),
+                                                 ndim, E, off.ctypes.data, ctypes.c_void_p(coords_ptr),
+                                                 ctypes.c_void_p(weight_ptr), ctypes.byref(out),
+                                                 ctypes.c_void_p(ncl_ptr or None), ctypes.c_void_p(stream)))
+        return None
+
+    def capture_batch(self, coords_ptr: int, weight_ptr: int, ndim: int, event_offsets, out_ptrs: dict,
+                      params: Params, kernel: Kernel | None = None, metric: Metric | None = None,
+                      ncl_ptr: int = 0, stream: int = 0) -> "Graph":
+        """Capture the batched pipeline into a CUDA graph (stream must not be the default stream)."""
+        p, k, m, off = self._batch_structs(ndim, params, kernel, metric, event_offsets)
+        E = len(off) - 1
+        out = _Outputs()
+        for name in ("cluster_index", "is_seed", "rho", "nearest_higher", "delta"):
+            setattr(out, name, out_ptrs.get(name) or None)
+        h = ctypes.c_void_p()
+        check(lib.clue_graph_capture_batch(self.handle, ctypes.byref(p), ctypes.byref(k), ctypes.byref(m), ndim,
+                                           E, off.ctypes.data, ctypes.c_void_p(coords_ptr),
+                                           ctypes.c_void_p(weight_ptr), ctypes.byref(out),
+                                           ctypes.c_void_p(ncl_ptr or None), ctypes.c_void_p(stream),
+                                           ctypes.byref(h)))
+        return Graph(h)
+
+    def events_loop(self, coords_ptr: int, weight_ptr: int, ndim: int, event_offsets, out_ptrs: dict,
+                    params: Params, kernel: Kernel | None = None, metric: Metric | None = None,
+                    stream: int = 0, event_times: bool = False):
+        """The plain pipeline once per event (clue_events_loop); returns per-event ms if asked."""
+        p, k, m, off = self._batch_structs(ndim, params, kernel, metric, event_offsets)
+        E = len(off) - 1
+        out = _Outputs()
+        for name in ("cluster_index", "is_seed", "rho", "nearest_higher", "delta"):
+            setattr(out, name, out_ptrs.get(name) or None)
+        ms = np.zeros(E, np.float32) if event_times else None
+        check(lib.clue_events_loop(self.handle, ctypes.byref(p), ctypes.byref(k), ctypes.byref(m), ndim, E,
+                                   off.ctypes.data, ctypes.c_void_p(coords_ptr), ctypes.c_void_p(weight_ptr),
+                                   ctypes.byref(out), ctypes.c_void_p(stream),
+                                   ms.ctypes.data if ms is not None else None))
+        return ms
+
     def read_info(self, stream: int = 0) -> RunInfo:
         info = _RunInfo()
         check(lib.clue_context_read_info(self.handle, ctypes.c_void_p(stream), ctypes.byref(info)))
         return RunInfo(**{f: getattr(info, f) for f, _ in _RunInfo._fields_})
+
+
+class Graph:
+    """An executable CUDA graph of the batched pipeline (clue_graph_capture_batch)."""
+
+    def __init__(self, handle):
+        self.handle = handle
+
+    def launch(self, stream: int = 0):
+        check(lib.clue_graph_launch(self.handle, ctypes.c_void_p(stream)))
+
+    def close(self):
+        if self.handle:
+            lib.clue_graph_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

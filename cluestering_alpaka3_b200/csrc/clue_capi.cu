@@ -6,6 +6,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "clue_internal.h"
 
@@ -95,11 +96,21 @@ float threshold_for(float r, bool root) {
 
 static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
-clue_status workspace_reserve(Workspace& ws, int ndim, size_t n, size_t ntiles) {
+// Box lower bounds of the metrics hold when no weight is negative (or NaN).
+int lower_bounds_ok(const clue_metric* m, int ndim) {
+  if (m->type == CLUE_METRIC_WEIGHTED_EUCLIDEAN || m->type == CLUE_METRIC_WEIGHTED_CHEBYSHEV)
+    for (int d = 0; d < ndim; ++d)
+      if (!(m->par[d] >= 0.0f)) return 0;
+  return 1;
+}
+
+clue_status workspace_reserve(Workspace& ws, int ndim, size_t n, size_t ntiles, size_t n_events) {
   const size_t words = (size_t)((ndim + 1 + 3) / 4);
-  if (n <= ws.cap_n && ntiles <= ws.cap_tiles && words <= ws.cap_words && ws.arena) return CLUE_OK;
+  if (n <= ws.cap_n && ntiles <= ws.cap_tiles && words <= ws.cap_words && n_events <= ws.cap_events && ws.arena)
+    return CLUE_OK;
   n = std::max(n, ws.cap_n);
   ntiles = std::max(ntiles, ws.cap_tiles);
+  n_events = std::max(n_events, ws.cap_events);
   const size_t w = std::max(words, ws.cap_words);
   const size_t nb = (size_t)sort_blocks((int)n);
   const size_t hist_len = (size_t)kRadix * nb;
@@ -109,8 +120,9 @@ clue_status workspace_reserve(Workspace& ws, int ndim, size_t n, size_t ntiles) 
     size_t bytes;
   };
   Workspace nw = ws;
+  void* evtab = nullptr;
   Item items[] = {
-      {(void**)&nw.grid, sizeof(DevGrid)},
+      {&evtab, event_table_bytes(n_events)},
       {(void**)&nw.status, sizeof(DevStatus)},
       {(void**)&nw.keys[0], n * 4},
       {(void**)&nw.keys[1], n * 4},
@@ -127,6 +139,7 @@ clue_status workspace_reserve(Workspace& ws, int ndim, size_t n, size_t ntiles) 
       {(void**)&nw.is_seed_s, n * 4},
       {(void**)&nw.seed_flag, n * 4},
       {(void**)&nw.seed_total, 16},
+      {(void**)&nw.blk, (n / 32 + 1) * 6 * 16},
       {(void**)&nw.ord_rho, n * 4},
       {(void**)&nw.ord_nh, n * 4},
       {(void**)&nw.chunk_count, (ntiles + 1) * 4},
@@ -148,7 +161,7 @@ clue_status workspace_reserve(Workspace& ws, int ndim, size_t n, size_t ntiles) 
   if (e != cudaSuccess) {
     cudaGetLastError();
     cudaSetDevice(prev);
-    ws.cap_n = ws.cap_tiles = ws.cap_words = 0;
+    ws.cap_n = ws.cap_tiles = ws.cap_words = ws.cap_events = 0;
     set_error(std::string("workspace allocation of ") + std::to_string(total) + " bytes failed: " +
               cudaGetErrorString(e));
     return CLUE_ERR_OUT_OF_MEMORY;
@@ -159,11 +172,26 @@ clue_status workspace_reserve(Workspace& ws, int ndim, size_t n, size_t ntiles) 
     *it.ptr = static_cast<char*>(arena) + offset;
     offset += align_up(it.bytes, 256);
   }
+  event_table_carve(evtab, n_events, &nw.ev, &nw.ev_pt, &nw.ev_tile);
   nw.arena = arena;
   nw.arena_bytes = total;
   nw.cap_n = n;
   nw.cap_tiles = ntiles;
   nw.cap_words = w;
+  nw.cap_events = n_events;
+  if (nw.pinned_bytes < event_table_bytes(n_events)) {
+    if (nw.pinned) cudaFreeHost(nw.pinned);
+    nw.pinned = nullptr;
+    nw.pinned_bytes = 0;
+    e = cudaMallocHost(&nw.pinned, event_table_bytes(n_events));
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      cudaSetDevice(prev);
+      set_error("pinned event-table allocation failed");
+      return CLUE_ERR_OUT_OF_MEMORY;
+    }
+    nw.pinned_bytes = event_table_bytes(n_events);
+  }
   if (!nw.status_host) {
     e = cudaMallocHost((void**)&nw.status_host, sizeof(DevStatus) + 64);
     if (e != cudaSuccess) {
@@ -192,11 +220,12 @@ static clue_status reserve_stage(Workspace& ws, size_t bytes) {
 }
 
 void workspace_release(Workspace& ws) {
-  for (auto& e : ws.ev)
+  for (auto& e : ws.tev)
     if (e) cudaEventDestroy(e);
   if (ws.arena) cudaFree(ws.arena);
   if (ws.dstage) cudaFree(ws.dstage);
   if (ws.status_host) cudaFreeHost(ws.status_host);
+  if (ws.pinned) cudaFreeHost(ws.pinned);
   ws = Workspace{};
 }
 
@@ -525,14 +554,16 @@ static clue_status prepare(clue_context ctx, const clue_params* params, const cl
   kp.rhoc = params->rhoc;
   kp.t_dc = threshold_for(params->dc, root);
   kp.t_dm = threshold_for(params->dm, root);
+  kp.lb_ok = lower_bounds_ok(metric, ndim);
   kp.kernel_type = kernel->type;
   for (int k = 0; k < 3; ++k) kp.kpar[k] = kernel->par[k];
   for (int d = 0; d < ndim; ++d) kp.mpar[d] = metric->par[d];
-  kp.nperdim = npd;
+  kp.nperdim0 = npd;
   kp.ntiles = nt;
+  kp.n_events = 1;
   int64_t s = 1;
   for (int d = ndim - 1; d >= 0; --d) {
-    kp.stride[d] = (int32_t)s;
+    kp.stride0[d] = (int32_t)s;
     s *= npd;
   }
   for (int d = 0; d < ndim; ++d) kp.wrapped[d] = params->wrapped[d] ? 1 : 0;
@@ -545,6 +576,8 @@ static clue_status prepare(clue_context ctx, const clue_params* params, const cl
   for (int d = 0; d < ndim; ++d) a.coords[d] = coords + (size_t)d * n;
   a.weight = weight;
   a.out = *out;
+  a.ev_n_seeds = nullptr;
+  a.ev_n_clusters = nullptr;
   ctx->ws.last_kp = kp;
   return workspace_reserve(ctx->ws, ndim, (size_t)n, (size_t)nt);
 }
@@ -570,11 +603,11 @@ static clue_status read_info(Workspace& ws, const KParams& kp, cudaStream_t s, c
     const int64_t cap = kp.seed_capacity < 0 ? -1
                                              : std::max<int64_t>(kp.seed_capacity, (int64_t)h->seed_candidates);
     info->n_seeds = nseeds;
-    info->n_clusters = cap < 0 ? nseeds : std::min(nseeds, cap);
+    info->n_clusters = h->n_clusters;
     info->dropped_seeds = nseeds - info->n_clusters;
-    info->seed_capacity_used = cap;
+    info->seed_capacity_used = kp.n_events == 1 ? cap : (kp.seed_capacity < 0 ? -1 : -2);
     info->n_tiles = kp.ntiles;
-    info->n_per_dim = kp.nperdim;
+    info->n_per_dim = kp.n_events == 1 ? kp.nperdim0 : 0;
     info->label_rounds = h->label_rounds;
   }
   return CLUE_OK;
@@ -673,7 +706,7 @@ clue_status clue_context_set_timing(clue_context ctx, int32_t enable) {
   int prev = 0;
   CLUE_CUDA_TRY(cudaGetDevice(&prev));
   CLUE_CUDA_TRY(cudaSetDevice(ctx->ws.device));
-  for (auto& e : ctx->ws.ev)
+  for (auto& e : ctx->ws.tev)
     if (!e) {
       cudaError_t err = cudaEventCreate(&e);
       if (err != cudaSuccess) {
@@ -688,13 +721,13 @@ clue_status clue_context_set_timing(clue_context ctx, int32_t enable) {
 }
 
 clue_status clue_context_stage_times(clue_context ctx, float* ms, int32_t n_stages) {
-  if (!ctx || !ms || !ctx->ws.ev[CLUE_N_STAGES]) {
+  if (!ctx || !ms || !ctx->ws.tev[CLUE_N_STAGES]) {
     set_error("timing not enabled");
     return CLUE_ERR_INVALID_ARG;
   }
-  CLUE_CUDA_TRY(cudaEventSynchronize(ctx->ws.ev[CLUE_N_STAGES]));
+  CLUE_CUDA_TRY(cudaEventSynchronize(ctx->ws.tev[CLUE_N_STAGES]));
   for (int k = 0; k < n_stages && k < CLUE_N_STAGES; ++k)
-    CLUE_CUDA_TRY(cudaEventElapsedTime(&ms[k], ctx->ws.ev[k], ctx->ws.ev[k + 1]));
+    CLUE_CUDA_TRY(cudaEventElapsedTime(&ms[k], ctx->ws.tev[k], ctx->ws.tev[k + 1]));
   return CLUE_OK;
 }
 
@@ -707,3 +740,378 @@ clue_status clue_get_clusters(clue_context, int32_t, const int32_t*, int32_t*, i
 }
 
 }  // extern "C"
+
+namespace clue_b200 {
+
+// Validates a batched request, computes every event's reference grid on the host
+// (SetupTiles.hpp:23-26, same arithmetic as a plain call), reserves the workspace and fills the
+// pinned event table.  Device pointers in `a` are left for the caller to set.
+static clue_status prepare_batch(clue_context ctx, const clue_params* params, const clue_kernel* kernel,
+                                 const clue_metric* metric, int32_t ndim, int32_t n_events,
+                                 const int32_t* ev_off, const clue_outputs* out, RunArgs& a) {
+  if (!ctx) {
+    set_error("context is null");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  clue_status st;
+  if ((st = clue_check_params(params)) != CLUE_OK) return st;
+  if ((st = clue_check_kernel(kernel)) != CLUE_OK) return st;
+  if ((st = clue_check_metric(metric, ndim)) != CLUE_OK) return st;
+  if (n_events <= 0 || !ev_off || !out || !out->cluster_index) {
+    set_error("n_events must be positive; event_offsets and out->cluster_index must be non-null");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  if (ev_off[0] != 0) {
+    set_error("event_offsets[0] must be 0");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  int64_t tiles = 0;
+  for (int e = 0; e < n_events; ++e) {
+    const int64_t ne = (int64_t)ev_off[e + 1] - ev_off[e];
+    if (ne <= 0) {
+      set_error("every event needs at least one point (event " + std::to_string(e) + ")");
+      return CLUE_ERR_INVALID_ARG;
+    }
+    int32_t npd, nt;
+    grid_shape((int32_t)ne, params->points_per_tile, ndim, &npd, &nt);
+    if (nt <= 0) {
+      set_error("tile grid too large");
+      return CLUE_ERR_CAPACITY;
+    }
+    tiles += nt;
+  }
+  const int64_t n = ev_off[n_events];
+  if (tiles > 2147483000ll || n > 2147483000ll) {
+    set_error("batch too large (points or tiles exceed 2^31)");
+    return CLUE_ERR_CAPACITY;
+  }
+  Workspace& ws = ctx->ws;
+  if ((st = workspace_reserve(ws, ndim, (size_t)n, (size_t)tiles, (size_t)n_events)) != CLUE_OK) return st;
+  EvGrid* heg;
+  int32_t *hpt, *htile;
+  event_table_carve(ws.pinned, ws.cap_events, &heg, &hpt, &htile);
+  int32_t tb = 0;
+  for (int e = 0; e < n_events; ++e) {
+    const int32_t ne = ev_off[e + 1] - ev_off[e];
+    int32_t npd, nt;
+    grid_shape(ne, params->points_per_tile, ndim, &npd, &nt);
+    EvGrid g;
+    std::memset(&g, 0, sizeof(g));
+    int64_t sd = 1;
+    for (int d = ndim - 1; d >= 0; --d) {
+      g.stride[d] = (int32_t)sd;
+      sd *= npd;
+    }
+    g.nperdim = npd;
+    g.ntiles = nt;
+    g.tile_base = tb;
+    g.pt_base = ev_off[e];
+    g.pt_count = ne;
+    heg[e] = g;
+    hpt[e] = ev_off[e];
+    htile[e] = tb;
+    tb += nt;
+  }
+  hpt[n_events] = (int32_t)n;
+  htile[n_events] = tb;
+
+  KParams& kp = a.kp;
+  std::memset(&kp, 0, sizeof(kp));
+  const bool root = metric->type == CLUE_METRIC_EUCLIDEAN || metric->type == CLUE_METRIC_WEIGHTED_EUCLIDEAN ||
+                    metric->type == CLUE_METRIC_PERIODIC_EUCLIDEAN;
+  kp.dc = params->dc;
+  kp.dm = params->dm;
+  kp.seed_dc = params->seed_dc;
+  kp.rhoc = params->rhoc;
+  kp.t_dc = threshold_for(params->dc, root);
+  kp.t_dm = threshold_for(params->dm, root);
+  kp.lb_ok = lower_bounds_ok(metric, ndim);
+  kp.kernel_type = kernel->type;
+  for (int k = 0; k < 3; ++k) kp.kpar[k] = kernel->par[k];
+  for (int d = 0; d < ndim; ++d) kp.mpar[d] = metric->par[d];
+  for (int d = 0; d < ndim; ++d) kp.wrapped[d] = params->wrapped[d] ? 1 : 0;
+  kp.tiebreak = params->tiebreak;
+  kp.seed_capacity = params->seed_capacity;
+  kp.n = (int32_t)n;
+  kp.n_events = n_events;
+  kp.ntiles = (int32_t)tiles;
+  kp.nperdim0 = heg[0].nperdim;
+  for (int d = 0; d < kMaxDim; ++d) kp.stride0[d] = heg[0].stride[d];
+  a.ndim = ndim;
+  a.n = (int32_t)n;
+  a.metric = metric->type;
+  a.out = *out;
+  a.ev_n_seeds = nullptr;
+  a.ev_n_clusters = nullptr;
+  ws.last_kp = kp;
+  return CLUE_OK;
+}
+
+// Copies the event table of an E-event batch from the pinned staging to the device.
+static clue_status upload_events(Workspace& ws, int E, cudaStream_t s) {
+  if (E <= 1) return CLUE_OK;  // a single event's table is written by the first kernel
+  EvGrid* heg;
+  int32_t *hpt, *htile;
+  event_table_carve(ws.pinned, ws.cap_events, &heg, &hpt, &htile);
+  CLUE_CUDA_TRY(cudaMemcpyAsync(ws.ev, heg, (size_t)E * sizeof(EvGrid), cudaMemcpyHostToDevice, s));
+  CLUE_CUDA_TRY(cudaMemcpyAsync(ws.ev_pt, hpt, (size_t)(E + 1) * 4, cudaMemcpyHostToDevice, s));
+  CLUE_CUDA_TRY(cudaMemcpyAsync(ws.ev_tile, htile, (size_t)(E + 1) * 4, cudaMemcpyHostToDevice, s));
+  return CLUE_OK;
+}
+
+}  // namespace clue_b200
+
+struct clue_graph_s {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int device = 0;
+};
+
+extern "C" {
+
+clue_status clue_batch_make_clusters(clue_context ctx, const clue_params* params, const clue_kernel* kernel,
+                                     const clue_metric* metric, int32_t ndim, int32_t n_events,
+                                     const int32_t* event_offsets, const float* coords, const float* weight,
+                                     const clue_outputs* out, int32_t* ev_n_clusters, int32_t memory,
+                                     void* stream, clue_run_info* info) {
+  RunArgs a;
+  clue_status st = prepare_batch(ctx, params, kernel, metric, ndim, n_events, event_offsets, out, a);
+  if (st != CLUE_OK) return st;
+  if (!coords || !weight) {
+    set_error("coords and weight must be non-null");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  Workspace& ws = ctx->ws;
+  int prev = 0;
+  CLUE_CUDA_TRY(cudaGetDevice(&prev));
+  CLUE_CUDA_TRY(cudaSetDevice(ws.device));
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t nn = (size_t)a.n;
+  clue_outputs dev_out = *out;
+  int32_t* dev_ncl = ev_n_clusters;
+  if (memory == CLUE_MEM_HOST) {
+    st = reserve_stage(ws, (nn * (size_t)(ndim + 1) + 5 * nn + (size_t)n_events) * 4);
+    if (st != CLUE_OK) {
+      cudaSetDevice(prev);
+      return st;
+    }
+    float* dcoords = static_cast<float*>(ws.dstage);
+    float* dweight = dcoords + nn * ndim;
+    int32_t* o = reinterpret_cast<int32_t*>(dweight + nn);
+    CLUE_CUDA_TRY(cudaMemcpyAsync(dcoords, coords, nn * ndim * 4, cudaMemcpyHostToDevice, s));
+    CLUE_CUDA_TRY(cudaMemcpyAsync(dweight, weight, nn * 4, cudaMemcpyHostToDevice, s));
+    for (int d = 0; d < ndim; ++d) a.coords[d] = dcoords + (size_t)d * nn;
+    a.weight = dweight;
+    dev_out.cluster_index = o;
+    dev_out.is_seed = out->is_seed ? o + nn : nullptr;
+    dev_out.rho = out->rho ? reinterpret_cast<float*>(o + 2 * nn) : nullptr;
+    dev_out.nearest_higher = out->nearest_higher ? o + 3 * nn : nullptr;
+    dev_out.delta = out->delta ? reinterpret_cast<float*>(o + 4 * nn) : nullptr;
+    dev_ncl = ev_n_clusters ? o + 5 * nn : nullptr;
+  } else {
+    for (int d = 0; d < ndim; ++d) a.coords[d] = coords + (size_t)d * nn;
+    a.weight = weight;
+  }
+  a.out = dev_out;
+  a.ev_n_clusters = dev_ncl;
+  st = upload_events(ws, n_events, s);
+  if (st == CLUE_OK) st = run_pipeline_dispatch(ws, a, s);
+  bool unresolved = false;
+  if (st == CLUE_OK) st = read_info(ws, a.kp, s, info, unresolved);
+  if (st == CLUE_OK && unresolved) {
+    st = finish_labels_dispatch(ws, a, s, 4);
+    if (st == CLUE_OK) st = read_info(ws, a.kp, s, info, unresolved);
+  }
+  if (st == CLUE_OK && memory == CLUE_MEM_HOST) {
+    auto back = [&](void* dst, const void* src, size_t cnt) -> cudaError_t {
+      return dst ? cudaMemcpyAsync(dst, src, cnt * 4, cudaMemcpyDeviceToHost, s) : cudaSuccess;
+    };
+    cudaError_t e = back(out->cluster_index, dev_out.cluster_index, nn);
+    if (e == cudaSuccess) e = back(out->is_seed, dev_out.is_seed, nn);
+    if (e == cudaSuccess) e = back(out->rho, dev_out.rho, nn);
+    if (e == cudaSuccess) e = back(out->nearest_higher, dev_out.nearest_higher, nn);
+    if (e == cudaSuccess) e = back(out->delta, dev_out.delta, nn);
+    if (e == cudaSuccess) e = back(ev_n_clusters, dev_ncl, (size_t)n_events);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+      set_error(std::string("copy back: ") + cudaGetErrorString(e));
+      st = CLUE_ERR_CUDA;
+    }
+  }
+  if (st == CLUE_OK && info) info->n_per_dim = 0;
+  cudaSetDevice(prev);
+  return st;
+}
+
+clue_status clue_batch_make_clusters_async(clue_context ctx, const clue_params* params,
+                                           const clue_kernel* kernel, const clue_metric* metric, int32_t ndim,
+                                           int32_t n_events, const int32_t* event_offsets, const float* coords,
+                                           const float* weight, const clue_outputs* out, int32_t* ev_n_clusters,
+                                           void* stream) {
+  RunArgs a;
+  clue_status st = prepare_batch(ctx, params, kernel, metric, ndim, n_events, event_offsets, out, a);
+  if (st != CLUE_OK) return st;
+  if (!coords || !weight) {
+    set_error("coords and weight must be non-null");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  for (int d = 0; d < ndim; ++d) a.coords[d] = coords + (size_t)d * a.n;
+  a.weight = weight;
+  a.ev_n_clusters = ev_n_clusters;
+  cudaStream_t s = (cudaStream_t)stream;
+  st = upload_events(ctx->ws, n_events, s);
+  if (st != CLUE_OK) return st;
+  return run_pipeline_dispatch(ctx->ws, a, s);
+}
+
+clue_status clue_graph_capture_batch(clue_context ctx, const clue_params* params, const clue_kernel* kernel,
+                                     const clue_metric* metric, int32_t ndim, int32_t n_events,
+                                     const int32_t* event_offsets, const float* coords, const float* weight,
+                                     const clue_outputs* out, int32_t* ev_n_clusters, void* stream,
+                                     clue_graph* graph) {
+  if (!graph || !stream) {
+    set_error("graph capture needs an output handle and a non-default stream");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  RunArgs a;
+  clue_status st = prepare_batch(ctx, params, kernel, metric, ndim, n_events, event_offsets, out, a);
+  if (st != CLUE_OK) return st;
+  if (!coords || !weight) {
+    set_error("coords and weight must be non-null");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  for (int d = 0; d < ndim; ++d) a.coords[d] = coords + (size_t)d * a.n;
+  a.weight = weight;
+  a.ev_n_clusters = ev_n_clusters;
+  cudaStream_t s = (cudaStream_t)stream;
+  Workspace& ws = ctx->ws;
+  const bool timing = ws.timing;
+  ws.timing = false;
+  auto* g = new (std::nothrow) clue_graph_s;
+  if (!g) return CLUE_ERR_OUT_OF_MEMORY;
+  g->device = ws.device;
+  cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    st = upload_events(ws, n_events, s);
+    if (st == CLUE_OK) st = run_pipeline_dispatch(ws, a, s);
+    e = cudaStreamEndCapture(s, &g->graph);
+  }
+  ws.timing = timing;
+  if (e == cudaSuccess && st == CLUE_OK) e = cudaGraphInstantiate(&g->exec, g->graph, 0);
+  if (e != cudaSuccess || st != CLUE_OK) {
+    if (e != cudaSuccess) set_error(std::string("graph capture: ") + cudaGetErrorString(e));
+    cudaGetLastError();
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
+    return st != CLUE_OK ? st : CLUE_ERR_CUDA;
+  }
+  *graph = g;
+  return CLUE_OK;
+}
+
+clue_status clue_graph_launch(clue_graph graph, void* stream) {
+  if (!graph || !graph->exec) return CLUE_ERR_INVALID_ARG;
+  CLUE_CUDA_TRY(cudaGraphLaunch(graph->exec, (cudaStream_t)stream));
+  return CLUE_OK;
+}
+
+clue_status clue_graph_destroy(clue_graph graph) {
+  if (!graph) return CLUE_OK;
+  if (graph->exec) cudaGraphExecDestroy(graph->exec);
+  if (graph->graph) cudaGraphDestroy(graph->graph);
+  delete graph;
+  return CLUE_OK;
+}
+
+}  // extern "C"
+
+extern "C" clue_status clue_events_loop(clue_context ctx, const clue_params* params, const clue_kernel* kernel,
+                                        const clue_metric* metric, int32_t ndim, int32_t n_events,
+                                        const int32_t* event_offsets, const float* coords, const float* weight,
+                                        const clue_outputs* out, void* stream, float* event_ms) {
+  if (!ctx || n_events <= 0 || !event_offsets || !coords || !weight || !out || !out->cluster_index) {
+    set_error("invalid events loop request");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  clue_status st;
+  if ((st = clue_check_params(params)) != CLUE_OK) return st;
+  if ((st = clue_check_kernel(kernel)) != CLUE_OK) return st;
+  if ((st = clue_check_metric(metric, ndim)) != CLUE_OK) return st;
+  const int64_t n_total = event_offsets[n_events];
+  int32_t nmax = 0, tmax = 0;
+  for (int e = 0; e < n_events; ++e) {
+    const int32_t ne = event_offsets[e + 1] - event_offsets[e];
+    if (ne <= 0) {
+      set_error("every event needs at least one point");
+      return CLUE_ERR_INVALID_ARG;
+    }
+    int32_t npd, nt;
+    grid_shape(ne, params->points_per_tile, ndim, &npd, &nt);
+    nmax = std::max(nmax, ne);
+    tmax = std::max(tmax, nt);
+  }
+  Workspace& ws = ctx->ws;
+  if ((st = workspace_reserve(ws, ndim, (size_t)nmax, (size_t)tmax, 1)) != CLUE_OK) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  std::vector<cudaEvent_t> evs;
+  if (event_ms) {
+    evs.resize((size_t)n_events + 1);
+    for (auto& e : evs) CLUE_CUDA_TRY(cudaEventCreate(&e));
+    CLUE_CUDA_TRY(cudaEventRecord(evs[0], s));
+  }
+  const bool root = metric->type == CLUE_METRIC_EUCLIDEAN || metric->type == CLUE_METRIC_WEIGHTED_EUCLIDEAN ||
+                    metric->type == CLUE_METRIC_PERIODIC_EUCLIDEAN;
+  for (int e = 0; e < n_events && st == CLUE_OK; ++e) {
+    const int32_t b = event_offsets[e], ne = event_offsets[e + 1] - b;
+    RunArgs a;
+    std::memset(&a, 0, sizeof(a));
+    KParams& kp = a.kp;
+    int32_t npd, nt;
+    grid_shape(ne, params->points_per_tile, ndim, &npd, &nt);
+    kp.dc = params->dc;
+    kp.dm = params->dm;
+    kp.seed_dc = params->seed_dc;
+    kp.rhoc = params->rhoc;
+    kp.t_dc = threshold_for(params->dc, root);
+    kp.t_dm = threshold_for(params->dm, root);
+  kp.lb_ok = lower_bounds_ok(metric, ndim);
+    kp.kernel_type = kernel->type;
+    for (int k = 0; k < 3; ++k) kp.kpar[k] = kernel->par[k];
+    for (int d = 0; d < ndim; ++d) kp.mpar[d] = metric->par[d];
+    for (int d = 0; d < ndim; ++d) kp.wrapped[d] = params->wrapped[d] ? 1 : 0;
+    kp.tiebreak = params->tiebreak;
+    kp.seed_capacity = params->seed_capacity;
+    kp.n = ne;
+    kp.n_events = 1;
+    kp.ntiles = nt;
+    kp.nperdim0 = npd;
+    int64_t sd = 1;
+    for (int d = ndim - 1; d >= 0; --d) {
+      kp.stride0[d] = (int32_t)sd;
+      sd *= npd;
+    }
+    a.ndim = ndim;
+    a.n = ne;
+    a.metric = metric->type;
+    for (int d = 0; d < ndim; ++d) a.coords[d] = coords + (size_t)d * n_total + b;
+    a.weight = weight + b;
+    a.out.cluster_index = out->cluster_index + b;
+    a.out.is_seed = out->is_seed ? out->is_seed + b : nullptr;
+    a.out.rho = out->rho ? out->rho + b : nullptr;
+    a.out.nearest_higher = out->nearest_higher ? out->nearest_higher + b : nullptr;
+    a.out.delta = out->delta ? out->delta + b : nullptr;
+    st = run_pipeline_dispatch(ws, a, s);
+    if (event_ms) cudaEventRecord(evs[(size_t)e + 1], s);
+  }
+  if (event_ms) {
+    cudaError_t err = cudaEventSynchronize(evs.back());
+    for (int e = 0; e < n_events && err == cudaSuccess; ++e) err = cudaEventElapsedTime(&event_ms[e], evs[e], evs[e + 1]);
+    for (auto& ev : evs) cudaEventDestroy(ev);
+    if (err != cudaSuccess) {
+      set_error(cudaGetErrorString(err));
+      return CLUE_ERR_CUDA;
+    }
+  }
+  return st;
+}

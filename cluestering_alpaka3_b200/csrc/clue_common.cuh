@@ -39,22 +39,40 @@ struct KParams {
   int32_t kernel_type;
   float kpar[3];
   float mpar[kMaxDim];
-  int32_t nperdim;
-  int32_t ntiles;
-  int32_t stride[kMaxDim];
   uint8_t wrapped[kMaxDim];
   int32_t tiebreak;
   int64_t seed_capacity;
-  int32_t n;
+  int32_t n;          // points over all events
+  int32_t n_events;   // events (1 for a plain make_clusters call)
+  int32_t ntiles;     // tiles over all events
+  // grid of the single event of a plain call (written to the event table by k_init)
+  int32_t nperdim0;
+  int32_t stride0[kMaxDim];
+  int32_t lb_ok;  // metric parameters allow box lower bounds (no negative weights)
 };
 
-// Tile grid geometry produced on the device from the bounding box.
-struct DevGrid {
+// Bounding box of 32 consecutive tile-sorted records: lo[N], hi[N], max payload.
+template <int N>
+struct Blk {
+  static constexpr int kWords = (2 * N + 1 + 3) / 4;
+};
+
+// Tile grid of one event.  The host fills nperdim, ntiles, strides and the point / tile
+// bases (the reference computes the grid shape on the host, SetupTiles.hpp:23-26); the
+// device fills the bounding box and tile sizes.
+struct EvGrid {
   uint32_t enc_min[kMaxDim];
   uint32_t enc_max[kMaxDim];
   float mn[kMaxDim];
   float mx[kMaxDim];
   float size[kMaxDim];
+  int32_t stride[kMaxDim];
+  int32_t nperdim;
+  int32_t ntiles;
+  int32_t tile_base;        // first global tile of the event
+  int32_t pt_base;          // first point of the event
+  int32_t pt_count;
+  uint32_t seed_candidates; // points of the event without nearest higher
 };
 
 // Device-side status block (counters and flags), read back once per call.
@@ -65,7 +83,8 @@ struct DevStatus {
   uint32_t unresolved[64];   // label rounds that left an unresolved parent chain
   uint32_t label_rounds;
   uint32_t stage_timeout;  // a bulk-copy wait in a staged sweep gave up
-  uint32_t pad[2];
+  uint32_t n_clusters;     // seeds kept in the seed lists, summed over events
+  uint32_t pad;
 };
 
 // float -> int32 truncation with x86 cvttss2si semantics (NaN and out-of-range give
@@ -158,6 +177,17 @@ struct Metric<N, CLUE_METRIC_EUCLIDEAN> {
     }
     return acc;
   }
+  // Lower bound of partial(x, c) over every c in the box [lo, hi], with the same monotone
+  // rounded operations, so lower() > t implies partial(x, c) > t for every c in the box.
+  CLUE_HD static float lower(const float* x, const float* lo, const float* hi, const float*) {
+    float acc = 0.0f;
+#pragma unroll
+    for (int d = N - 1; d >= 0; --d) {
+      const float gap = x[d] < lo[d] ? fsub(lo[d], x[d]) : (x[d] > hi[d] ? fsub(x[d], hi[d]) : 0.0f);
+      acc = fadd(fmul(gap, gap), acc);
+    }
+    return acc;
+  }
   CLUE_HD static float finish(float s) { return fsqrt(s); }
 };
 
@@ -170,6 +200,15 @@ struct Metric<N, CLUE_METRIC_WEIGHTED_EUCLIDEAN> {
     for (int d = N - 1; d >= 0; --d) {
       const float t = fmul(fmul(w[d], fsub(a[d], b[d])), fsub(a[d], b[d]));
       acc = fadd(t, acc);
+    }
+    return acc;
+  }
+  CLUE_HD static float lower(const float* x, const float* lo, const float* hi, const float* w) {
+    float acc = 0.0f;
+#pragma unroll
+    for (int d = N - 1; d >= 0; --d) {
+      const float gap = x[d] < lo[d] ? fsub(lo[d], x[d]) : (x[d] > hi[d] ? fsub(x[d], hi[d]) : 0.0f);
+      acc = fadd(fmul(fmul(w[d], gap), gap), acc);
     }
     return acc;
   }
@@ -190,6 +229,16 @@ struct Metric<N, CLUE_METRIC_PERIODIC_EUCLIDEAN> {
     }
     return acc;
   }
+  // Periodic dimensions contribute no bound; the others bound like the Euclidean metric.
+  CLUE_HD static float lower(const float* x, const float* lo, const float* hi, const float* period) {
+    float acc = 0.0f;
+#pragma unroll
+    for (int d = N - 1; d >= 0; --d) {
+      const float gap = x[d] < lo[d] ? fsub(lo[d], x[d]) : (x[d] > hi[d] ? fsub(x[d], hi[d]) : 0.0f);
+      acc = fadd(period[d] == 0.0f ? fmul(gap, gap) : 0.0f, acc);
+    }
+    return acc;
+  }
   CLUE_HD static float finish(float s) { return fsqrt(s); }
 };
 
@@ -200,6 +249,15 @@ struct Metric<N, CLUE_METRIC_MANHATTAN> {
     float acc = 0.0f;
 #pragma unroll
     for (int d = N - 1; d >= 0; --d) acc = fadd(fabsf(fsub(a[d], b[d])), acc);
+    return acc;
+  }
+  CLUE_HD static float lower(const float* x, const float* lo, const float* hi, const float*) {
+    float acc = 0.0f;
+#pragma unroll
+    for (int d = N - 1; d >= 0; --d) {
+      const float gap = x[d] < lo[d] ? fsub(lo[d], x[d]) : (x[d] > hi[d] ? fsub(x[d], hi[d]) : 0.0f);
+      acc = fadd(gap, acc);
+    }
     return acc;
   }
   CLUE_HD static float finish(float s) { return s; }
@@ -217,6 +275,15 @@ struct Metric<N, CLUE_METRIC_CHEBYSHEV> {
     }
     return m;
   }
+  CLUE_HD static float lower(const float* x, const float* lo, const float* hi, const float*) {
+    float m = 0.0f;
+#pragma unroll
+    for (int d = 0; d < N; ++d) {
+      const float gap = x[d] < lo[d] ? fsub(lo[d], x[d]) : (x[d] > hi[d] ? fsub(x[d], hi[d]) : 0.0f);
+      m = (m < gap) ? gap : m;
+    }
+    return m;
+  }
   CLUE_HD static float finish(float s) { return s; }
 };
 
@@ -228,6 +295,16 @@ struct Metric<N, CLUE_METRIC_WEIGHTED_CHEBYSHEV> {
 #pragma unroll
     for (int d = 0; d < N; ++d) {
       const float t = fmul(w[d], fabsf(fsub(a[d], b[d])));
+      m = (m < t) ? t : m;
+    }
+    return m;
+  }
+  CLUE_HD static float lower(const float* x, const float* lo, const float* hi, const float* w) {
+    float m = 0.0f;
+#pragma unroll
+    for (int d = 0; d < N; ++d) {
+      const float gap = x[d] < lo[d] ? fsub(lo[d], x[d]) : (x[d] > hi[d] ? fsub(x[d], hi[d]) : 0.0f);
+      const float t = fmul(w[d], gap);
       m = (m < t) ? t : m;
     }
     return m;

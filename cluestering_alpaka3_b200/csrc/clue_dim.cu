@@ -3,7 +3,7 @@
 // Compiled once per dimensionality (-DCLUE_NDIM=1..10) so the templates of one
 // dimension build in parallel.  Stage map against the reference's serial path
 // (include/CLUEstering/core/detail/Clusterer.hpp:134-171):
-//   k_bbox / k_grid      compute_tile_size        core/detail/ComputeTiles.hpp:13-27
+//   k_bbox_* / k_grid    compute_tile_size        core/detail/ComputeTiles.hpp:13-27
 //   k_bin + radix sort   Tiles::fill              data_structures/internal/Tiles.hpp:92-96
 //   k_density            KernelCalculateLocalDensity  core/detail/ClusteringKernels.hpp:66-107
 //   k_nearest_higher     KernelCalculateNearestHigher core/detail/ClusteringKernels.hpp:109-212
@@ -12,10 +12,15 @@
 //                        data_structures/internal/Followers.hpp:27-30,
 //                        core/detail/ClusteringKernels.hpp:246-281
 //
+// One call clusters E independent events (E = 1 for a plain make_clusters).  Event e owns
+// points [pt_base, pt_base + pt_count) and global tiles [tile_base, tile_base + ntiles) of its
+// own reference grid; tile keys are event-major, so one stable sort of (tile, index) pairs
+// orders every event by tile while keeping events contiguous.
+//
 // Layout in HBM: points are reordered by tile (stable: ascending index inside a tile)
-// into float4 records {coords..., payload}; one warp lane owns one home point and the
-// whole warp walks the same candidate sequence, so every candidate record is one
-// broadcast 16-byte load per warp.
+// into float4 records {coords..., payload}.  A CTA processes a chunk of 128 home points of
+// one tile; the candidate tiles of the chunk are staged into shared memory with bulk copies
+// and every candidate record is one broadcast 16-byte shared-memory load per warp.
 #include "clue_internal.h"
 #include "clue_tma.cuh"
 
@@ -28,15 +33,22 @@ namespace {
 
 constexpr int kTileThreads = 128;
 constexpr int kChunkWarps = kTileThreads / 32;
-constexpr int kChunk = kChunkPoints;      // home points per CTA in the density / nearest-higher sweeps
+constexpr int kChunk = kChunkPoints;  // home points per CTA in the density / nearest-higher sweeps
 static_assert(kChunkPoints == kTileThreads, "one home point per thread");
-constexpr int kCap = 2048;                // home points signature-sorted per pass
-constexpr int kStageWords = 1024;         // float4 words per staging buffer (16 KiB)
-constexpr int kMaxSeg = 32;               // tile segments per staged piece
+constexpr int kCap = 2048;         // home points signature-sorted per pass
+constexpr int kStageWords = 1024;  // float4 words per staging buffer (16 KiB)
+constexpr int kMaxSeg = 32;        // tile segments per staged piece
 
 struct InPtrs {
   const float* c[kMaxDim];
   const float* w;
+};
+
+// Event tables of one call.
+struct Events {
+  EvGrid* eg;            // [E]
+  const int32_t* pt;     // [E + 1] point offsets
+  const int32_t* tile;   // [E + 1] global tile offsets
 };
 
 __device__ __forceinline__ int warp_min_i(int v) {
@@ -58,6 +70,19 @@ __device__ __forceinline__ uint32_t warp_max_u(uint32_t v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v = max(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
+}
+
+// Largest e in [0, E) with base[e] <= x.
+__device__ __forceinline__ int find_event(const int32_t* __restrict__ base, int E, int x) {
+  int lo = 0, hi = E - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(base + mid) <= x)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
 }
 
 template <int N>
@@ -91,22 +116,40 @@ __device__ __forceinline__ void store_rec(float4* __restrict__ rec, int pos, con
     rec[(size_t)pos * W + k] = make_float4(buf[4 * k], buf[4 * k + 1], buf[4 * k + 2], buf[4 * k + 3]);
 }
 
+template <int N>
+__device__ __forceinline__ void unpack_rec(const float4* r, float* c, float& payload) {
+  constexpr int W = Rec<N>::kWords;
+  float buf[4 * W];
+#pragma unroll
+  for (int k = 0; k < W; ++k) {
+    const float4 v = r[k];
+    buf[4 * k + 0] = v.x;
+    buf[4 * k + 1] = v.y;
+    buf[4 * k + 2] = v.z;
+    buf[4 * k + 3] = v.w;
+  }
+#pragma unroll
+  for (int d = 0; d < N; ++d) c[d] = buf[d];
+  payload = buf[Rec<N>::kPayload];
+}
+
 // Search box of one point in "virtual" bins: the reference's [getBin(x - r), getBin(x + r)]
 // (TilesView.hpp:72-82, wrapped boxes extended by nperdim), shifted down by nperdim when a
 // wrapped box starts above the home bin, so that every lane of a warp expresses its box
 // in the same frame around the home tile.  The tile of virtual bin v is v mod nperdim.
 template <int N>
-__device__ __forceinline__ void lane_box(const KParams& kp, const DevGrid* __restrict__ g, const float* x,
+__device__ __forceinline__ void lane_box(const KParams& kp, const EvGrid* __restrict__ g, const float* x,
                                          float r, const int* hb, int* lo, int* hi) {
+  const int npd = g->nperdim;
 #pragma unroll
   for (int d = 0; d < N; ++d) {
     const bool wr = kp.wrapped[d] != 0;
-    int a = get_bin(fsub(x[d], r), g->mn[d], g->mx[d], g->size[d], wr, kp.nperdim);
-    int b = get_bin(fadd(x[d], r), g->mn[d], g->mx[d], g->size[d], wr, kp.nperdim);
-    if (wr && a > b) b += kp.nperdim;
+    int a = get_bin(fsub(x[d], r), g->mn[d], g->mx[d], g->size[d], wr, npd);
+    int b = get_bin(fadd(x[d], r), g->mn[d], g->mx[d], g->size[d], wr, npd);
+    if (wr && a > b) b += npd;
     if (wr && a > hb[d]) {
-      a -= kp.nperdim;
-      b -= kp.nperdim;
+      a -= npd;
+      b -= npd;
     }
     lo[d] = a;
     hi[d] = b;
@@ -114,9 +157,10 @@ __device__ __forceinline__ void lane_box(const KParams& kp, const DevGrid* __res
 }
 
 template <int N>
-__device__ __forceinline__ void home_bins(const KParams& kp, int t, int* hb) {
+__device__ __forceinline__ void home_bins(const EvGrid* __restrict__ g, int t, int* hb) {
+  const int lt = t - g->tile_base;
 #pragma unroll
-  for (int d = 0; d < N; ++d) hb[d] = (t / kp.stride[d]) % kp.nperdim;
+  for (int d = 0; d < N; ++d) hb[d] = (lt / g->stride[d]) % g->nperdim;
 }
 
 __device__ __forceinline__ int wrap_bin(int v, int npd) {
@@ -124,14 +168,25 @@ __device__ __forceinline__ int wrap_bin(int v, int npd) {
   return b < 0 ? b + npd : b;
 }
 
-// Orders the home points [cb, cb + cnt) of a tile by which neighbour tiles their search
-// box reaches (2 bits per dimension), so that the 32 lanes of a warp share one box.
+// Sub-cell bits per dimension of the spatial part of the home order.
 template <int N>
-__device__ void signature_sort(const KParams& kp, const DevGrid* __restrict__ g, const float4* __restrict__ rec,
-                               int cb, int cnt, float r, const int* hb, int32_t* s_order, uint8_t* s_key,
-                               int32_t* s_hist) {
+struct HomeKey {
+  static constexpr int kSubBits = N <= 2 ? 3 : (N == 3 ? 2 : (N == 4 ? 1 : 0));
+  static constexpr int kBits = N <= 4 ? 2 * N + N * kSubBits : 0;
+  static constexpr int kKeys = 1 << kBits;
+};
+
+// Orders the home points [cb, cb + cnt) of a tile by which neighbour tiles their search box
+// reaches (2 bits per dimension, so the 32 lanes of a warp share one box) and then by Morton
+// order of their sub-cell inside the tile (so a warp's points are close together and whole
+// candidate blocks can be skipped for every lane at once).
+template <int N>
+__device__ void home_sort(const KParams& kp, const EvGrid* __restrict__ g, const float4* __restrict__ rec, int cb,
+                          int cnt, float r, const int* hb, int32_t* s_order, uint16_t* s_key, int32_t* s_hist) {
   if constexpr (N <= 4) {
-    constexpr int K = 1 << (2 * N);
+    constexpr int SB = HomeKey<N>::kSubBits;
+    constexpr int K = HomeKey<N>::kKeys;
+    constexpr int S = 1 << SB;
     for (int e = threadIdx.x; e < K; e += blockDim.x) s_hist[e] = 0;
     __syncthreads();
     for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
@@ -139,10 +194,20 @@ __device__ void signature_sort(const KParams& kp, const DevGrid* __restrict__ g,
       load_rec<N>(rec, cb + k, x, pl);
       int lo[N], hi[N];
       lane_box<N>(kp, g, x, r, hb, lo, hi);
-      int key = 0;
+      int sig = 0, morton = 0;
 #pragma unroll
-      for (int d = 0; d < N; ++d) key |= ((lo[d] < hb[d] ? 1 : 0) | (hi[d] > hb[d] ? 2 : 0)) << (2 * d);
-      s_key[k] = (uint8_t)key;
+      for (int d = 0; d < N; ++d) {
+        sig |= ((lo[d] < hb[d] ? 1 : 0) | (hi[d] > hb[d] ? 2 : 0)) << (2 * d);
+        if (SB > 0) {
+          const float t0 = g->mn[d] + (float)hb[d] * g->size[d];
+          int sc = g->size[d] > 0.0f ? (int)((x[d] - t0) / g->size[d] * (float)S) : 0;
+          sc = sc < 0 ? 0 : (sc > S - 1 ? S - 1 : sc);
+#pragma unroll
+          for (int bit = 0; bit < SB; ++bit) morton |= ((sc >> bit) & 1) << (bit * N + d);
+        }
+      }
+      const int key = (sig << (N * SB)) | morton;
+      s_key[k] = (uint16_t)key;
       atomicAdd(&s_hist[key], 1);
     }
     __syncthreads();
@@ -170,21 +235,116 @@ __device__ void signature_sort(const KParams& kp, const DevGrid* __restrict__ g,
   }
 }
 
-// ---- stage 1: bounding box, grid, bins --------------------------------------
-
+// Bounding box (and largest payload) of every 32 consecutive tile-sorted records.
 template <int N>
-__global__ void k_init(DevGrid* g, DevStatus* st) {
-  const int t = threadIdx.x;
-  if (t < kMaxDim) {
-    g->enc_min[t] = 0xffffffffu;
-    g->enc_max[t] = 0u;
+__global__ void __launch_bounds__(256) k_block_bbox(const float4* __restrict__ rec, int n, float4* __restrict__ blk) {
+  constexpr int BW = Blk<N>::kWords;
+  const int lane = threadIdx.x & 31;
+  const int nblk = (n + 31) >> 5;
+  const int wstride = (gridDim.x * blockDim.x) >> 5;
+  for (int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nblk; b += wstride) {
+    const int q = (b << 5) + lane;
+    float x[N], pl;
+    if (q < n) {
+      load_rec<N>(rec, q, x, pl);
+    } else {
+      load_rec<N>(rec, b << 5, x, pl);  // duplicates the block's first record
+    }
+    float out[4 * BW];
+#pragma unroll
+    for (int k = 0; k < 4 * BW; ++k) out[k] = 0.0f;
+#pragma unroll
+    for (int d = 0; d < N; ++d) {
+      float a = x[d], z = x[d];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        a = fminf(a, __shfl_xor_sync(0xffffffffu, a, o));
+        z = fmaxf(z, __shfl_xor_sync(0xffffffffu, z, o));
+      }
+      out[d] = a;
+      out[N + d] = z;
+    }
+    float pm = pl;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) pm = fmaxf(pm, __shfl_xor_sync(0xffffffffu, pm, o));
+    out[2 * N] = pm;
+    if (lane < BW) {
+      float4 v;
+#pragma unroll
+      for (int k = 0; k < BW; ++k)
+        if (k == lane) v = make_float4(out[4 * k], out[4 * k + 1], out[4 * k + 2], out[4 * k + 3]);
+      blk[(size_t)b * BW + lane] = v;
+    }
   }
-  uint32_t* s = reinterpret_cast<uint32_t*>(st);
-  for (int k = t; k < (int)(sizeof(DevStatus) / 4); k += blockDim.x) s[k] = 0u;
 }
 
+// Walks the staged segment [qb, qb + n) block by block (blocks are 32 aligned records) and
+// calls inner(j0, j1) for the parts whose block some lane of the warp may need: the lane's
+// box holds the tile, the block's box lower bound is within `bound` (strictly below it when
+// `strict`) and the block's largest payload reaches `pmin`.
+template <int N, class M, class Inner>
+__device__ __forceinline__ void scan_blocks(const KParams& kp, const float4* __restrict__ blk, const float* x,
+                                            bool inbox, float bound, bool strict, float pmin, int qb, int n,
+                                            Inner&& inner) {
+  constexpr int BW = Blk<N>::kWords;
+  int j = 0;
+  while (j < n) {
+    const int b = (qb + j) >> 5;
+    const int je = min(n, ((b + 1) << 5) - qb);
+    bool need = inbox;
+    if (kp.lb_ok) {
+      float buf[4 * BW];
+#pragma unroll
+      for (int k = 0; k < BW; ++k) {
+        const float4 v = __ldg(blk + (size_t)b * BW + k);
+        buf[4 * k] = v.x;
+        buf[4 * k + 1] = v.y;
+        buf[4 * k + 2] = v.z;
+        buf[4 * k + 3] = v.w;
+      }
+      const float lb = M::lower(x, buf, buf + N, kp.mpar);
+      need = need && (strict ? lb < bound : lb <= bound) && buf[2 * N] >= pmin;
+    }
+    if (__any_sync(0xffffffffu, need)) inner(j, je);
+    j = je;
+  }
+}
+
+// ---- stage 1: bounding box, grid, bins --------------------------------------
+
+// Resets the per-call state; for a plain call also writes the event table of its one event.
 template <int N>
-__global__ void __launch_bounds__(256) k_bbox(InPtrs in, int n, DevGrid* g, DevStatus* st) {
+__global__ void k_init(const KParams kp, Events ev, int32_t* ev_pt, int32_t* ev_tile, DevStatus* st) {
+  if (blockIdx.x == 0) {
+    uint32_t* s = reinterpret_cast<uint32_t*>(st);
+    for (int k = threadIdx.x; k < (int)(sizeof(DevStatus) / 4); k += blockDim.x) s[k] = 0u;
+  }
+  const int stride = gridDim.x * blockDim.x;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < kp.n_events; e += stride) {
+    EvGrid& g = ev.eg[e];
+    for (int d = 0; d < kMaxDim; ++d) {
+      g.enc_min[d] = 0xffffffffu;
+      g.enc_max[d] = 0u;
+    }
+    g.seed_candidates = 0;
+    if (kp.n_events == 1) {
+      g.nperdim = kp.nperdim0;
+      g.ntiles = kp.ntiles;
+      g.tile_base = 0;
+      g.pt_base = 0;
+      g.pt_count = kp.n;
+      for (int d = 0; d < kMaxDim; ++d) g.stride[d] = kp.stride0[d];
+      ev_pt[0] = 0;
+      ev_pt[1] = kp.n;
+      ev_tile[0] = 0;
+      ev_tile[1] = kp.ntiles;
+    }
+  }
+}
+
+// Bounding box of a single event with grid-wide atomics.
+template <int N>
+__global__ void __launch_bounds__(256) k_bbox_single(InPtrs in, int n, EvGrid* g, DevStatus* st) {
   uint32_t emn[N], emx[N];
 #pragma unroll
   for (int d = 0; d < N; ++d) {
@@ -219,30 +379,87 @@ __global__ void __launch_bounds__(256) k_bbox(InPtrs in, int n, DevGrid* g, DevS
   if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&st->nonfinite, 1u);
 }
 
-// Tile size (max - min) / nperdim in FP32 (ComputeTiles.hpp:20-23).
+// Bounding box of many events: one CTA per event (grid-stride over events).
 template <int N>
-__global__ void k_grid(const KParams kp, DevGrid* g) {
-  const int d = threadIdx.x;
-  if (d < N) {
-    const float mn = dec_float(g->enc_min[d]);
-    const float mx = dec_float(g->enc_max[d]);
-    g->mn[d] = mn;
-    g->mx[d] = mx;
-    g->size[d] = fdiv(fsub(mx, mn), (float)kp.nperdim);
+__global__ void __launch_bounds__(256) k_bbox_events(InPtrs in, int E, EvGrid* eg, DevStatus* st) {
+  __shared__ uint32_t s_mn[8][N], s_mx[8][N];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int e = blockIdx.x; e < E; e += gridDim.x) {
+    const int b = eg[e].pt_base, cnt = eg[e].pt_count;
+    uint32_t emn[N], emx[N];
+#pragma unroll
+    for (int d = 0; d < N; ++d) {
+      emn[d] = 0xffffffffu;
+      emx[d] = 0u;
+    }
+    bool bad = false;
+    for (int i = b + threadIdx.x; i < b + cnt; i += blockDim.x) {
+#pragma unroll
+      for (int d = 0; d < N; ++d) {
+        const float x = in.c[d][i];
+        bad |= !isfinite(x);
+        const uint32_t en = enc_float(x);
+        emn[d] = min(emn[d], en);
+        emx[d] = max(emx[d], en);
+      }
+      bad |= !isfinite(in.w[i]);
+    }
+#pragma unroll
+    for (int d = 0; d < N; ++d) {
+      emn[d] = warp_min_u(emn[d]);
+      emx[d] = warp_max_u(emx[d]);
+    }
+    if (lane == 0) {
+#pragma unroll
+      for (int d = 0; d < N; ++d) {
+        s_mn[warp][d] = emn[d];
+        s_mx[warp][d] = emx[d];
+      }
+    }
+    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(&st->nonfinite, 1u);
+    __syncthreads();
+    if (threadIdx.x < N) {
+      const int d = threadIdx.x;
+      uint32_t a = 0xffffffffu, z = 0u;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+        a = min(a, s_mn[w][d]);
+        z = max(z, s_mx[w][d]);
+      }
+      eg[e].enc_min[d] = a;
+      eg[e].enc_max[d] = z;
+    }
+    __syncthreads();
   }
 }
 
-// Global bin of every point (TilesView.hpp:53-61, exact integer arithmetic).
+// Tile size (max - min) / nperdim in FP32 (ComputeTiles.hpp:20-23), per event.
 template <int N>
-__global__ void __launch_bounds__(256) k_bin(const KParams kp, InPtrs in, int n, const DevGrid* __restrict__ g,
+__global__ void k_grid(int E, EvGrid* eg) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += stride) {
+    EvGrid& g = eg[e];
+#pragma unroll
+    for (int d = 0; d < N; ++d) {
+      const float mn = dec_float(g.enc_min[d]);
+      const float mx = dec_float(g.enc_max[d]);
+      g.mn[d] = mn;
+      g.mx[d] = mx;
+      g.size[d] = fdiv(fsub(mx, mn), (float)g.nperdim);
+    }
+  }
+}
+
+// Event-major global tile key of every point (TilesView.hpp:53-61, exact integers).
+template <int N>
+__global__ void __launch_bounds__(256) k_bin(const KParams kp, InPtrs in, Events ev,
                                              uint32_t* __restrict__ keys) {
   const int stride = gridDim.x * blockDim.x;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    int gb = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kp.n; i += stride) {
+    const EvGrid* g = ev.eg + find_event(ev.pt, kp.n_events, i);
+    int gb = g->tile_base;
 #pragma unroll
     for (int d = 0; d < N; ++d)
-      gb += kp.stride[d] *
-            get_bin(in.c[d][i], g->mn[d], g->mx[d], g->size[d], kp.wrapped[d] != 0, kp.nperdim);
+      gb += g->stride[d] * get_bin(in.c[d][i], g->mn[d], g->mx[d], g->size[d], kp.wrapped[d] != 0, g->nperdim);
     keys[i] = (uint32_t)gb;
   }
 }
@@ -265,26 +482,27 @@ __global__ void __launch_bounds__(256) k_gather(InPtrs in, int n, const int32_t*
 // density, dm for the nearest higher) and cut into chunks of kChunk home points; one CTA
 // processes one chunk, so a heavy tile is spread over many CTAs.
 template <int N>
-__global__ void __launch_bounds__(kTileThreads) k_order(const KParams kp, const DevGrid* __restrict__ g,
+__global__ void __launch_bounds__(kTileThreads) k_order(const KParams kp, Events ev,
                                                         const int32_t* __restrict__ off,
                                                         const float4* __restrict__ rec_w,
                                                         int32_t* __restrict__ ord_rho, int32_t* __restrict__ ord_nh,
                                                         uint32_t* __restrict__ chunk_count) {
   __shared__ int32_t s_order[kCap];
-  __shared__ uint8_t s_key[kCap];
-  __shared__ int32_t s_hist[N <= 4 ? (1 << (2 * N)) : 1];
+  __shared__ uint16_t s_key[kCap];
+  __shared__ int32_t s_hist[N <= 4 ? HomeKey<N>::kKeys : 1];
   for (int t = blockIdx.x; t < kp.ntiles; t += gridDim.x) {
     const int beg = off[t], end = off[t + 1];
     if (threadIdx.x == 0) chunk_count[t] = (uint32_t)((end - beg + kChunk - 1) / kChunk);
     if (beg == end) continue;
+    const EvGrid* g = ev.eg + find_event(ev.tile, kp.n_events, t);
     int hb[N];
-    home_bins<N>(kp, t, hb);
+    home_bins<N>(g, t, hb);
     for (int cb = beg; cb < end; cb += kCap) {
       const int cnt = min(kCap, end - cb);
-      signature_sort<N>(kp, g, rec_w, cb, cnt, kp.dc, hb, s_order, s_key, s_hist);
+      home_sort<N>(kp, g, rec_w, cb, cnt, kp.dc, hb, s_order, s_key, s_hist);
       for (int k = threadIdx.x; k < cnt; k += blockDim.x) ord_rho[cb + k] = cb + s_order[k];
       __syncthreads();
-      signature_sort<N>(kp, g, rec_w, cb, cnt, kp.dm, hb, s_order, s_key, s_hist);
+      home_sort<N>(kp, g, rec_w, cb, cnt, kp.dm, hb, s_order, s_key, s_hist);
       for (int k = threadIdx.x; k < cnt; k += blockDim.x) ord_nh[cb + k] = cb + s_order[k];
       __syncthreads();
     }
@@ -320,6 +538,7 @@ struct StageSmem {
   int32_t wlo[kChunkWarps][N], whi[kChunkWarps][N];
   int32_t ulo[N], uhi[N];
   int32_t any_valid;
+  int32_t has[2];
   alignas(8) uint64_t full[2];
 };
 
@@ -341,7 +560,7 @@ struct TileIter {
   }
 
   // Advances to the next needed, non-empty tile; false when the union is exhausted.
-  __device__ bool next(const KParams& kp, const int32_t* __restrict__ off, const StageSmem<N>& sm) {
+  __device__ bool next(const EvGrid* __restrict__ g, const int32_t* __restrict__ off, const StageSmem<N>& sm) {
     while (true) {
       if (!started) {
 #pragma unroll
@@ -359,9 +578,9 @@ struct TileIter {
         if (d < 0) return false;
       }
       if (!needed(sm)) continue;
-      int u = 0;
+      int u = g->tile_base;
 #pragma unroll
-      for (int d = 0; d < N; ++d) u += kp.stride[d] * wrap_bin(v[d], kp.nperdim);
+      for (int d = 0; d < N; ++d) u += g->stride[d] * wrap_bin(v[d], g->nperdim);
       q = off[u];
       qe = off[u + 1];
       if (qe > q) return true;
@@ -371,14 +590,15 @@ struct TileIter {
 
 // Builds piece b (thread 0 only) and issues its bulk copies; returns the words staged.
 template <int N>
-__device__ int build_piece(const KParams& kp, const int32_t* __restrict__ off, const float4* __restrict__ rec,
-                           StageSmem<N>& sm, TileIter<N>& it, bool& done, int b) {
+__device__ int build_piece(const EvGrid* __restrict__ g, const int32_t* __restrict__ off,
+                           const float4* __restrict__ rec, StageSmem<N>& sm, TileIter<N>& it, bool& done,
+                           int b) {
   constexpr int W = Rec<N>::kWords;
   constexpr int cap = kStageWords / W;
   int nseg = 0, fill = 0;
   while (!done && nseg < kMaxSeg && fill < cap) {
     if (it.q >= it.qe) {
-      if (!it.next(kp, off, sm)) {
+      if (!it.next(g, off, sm)) {
         done = true;
         break;
       }
@@ -405,12 +625,13 @@ __device__ int build_piece(const KParams& kp, const int32_t* __restrict__ off, c
 
 constexpr uint64_t kWaitLimitNs = 1000000000ull;  // 1 s per bulk-copy wait
 
-// Runs the staged sweep; `vis(seg_inbox, c, payload, q)` is called for every staged
-// candidate of a segment the warp needs.  Returns false if a bulk copy did not complete
-// within the wait limit (the caller reports it and the CTA exits).
+// Runs the staged sweep; `vis(inbox, staged_records, first_position, count)` is called for
+// every staged segment of a tile the warp needs.  Returns false if a bulk copy did not
+// complete within the wait limit (the caller reports it and the CTA exits).
 template <int N, class Visit>
-__device__ bool staged_sweep(const KParams& kp, const int32_t* __restrict__ off, const float4* __restrict__ rec,
-                             StageSmem<N>& sm, const int* lo, const int* hi, bool valid, Visit&& vis) {
+__device__ bool staged_sweep(const EvGrid* __restrict__ g, const int32_t* __restrict__ off,
+                             const float4* __restrict__ rec, StageSmem<N>& sm, const int* lo, const int* hi,
+                             bool valid, Visit&& vis) {
   constexpr int W = Rec<N>::kWords;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int wl[N], wh[N];
@@ -451,15 +672,12 @@ __device__ bool staged_sweep(const KParams& kp, const int32_t* __restrict__ off,
   __syncthreads();
   TileIter<N> it;
   bool done = sm.any_valid == 0;
-  int has_next = 0;
-  if (threadIdx.x == 0) has_next = build_piece<N>(kp, off, rec, sm, it, done, 0) > 0;
-  __shared__ int s_has[2];
-  if (threadIdx.x == 0) s_has[0] = has_next;
+  if (threadIdx.x == 0) sm.has[0] = build_piece<N>(g, off, rec, sm, it, done, 0) > 0;
   __syncthreads();
   bool ok = true;
-  for (int p = 0; s_has[p & 1]; ++p) {
+  for (int p = 0; sm.has[p & 1]; ++p) {
     const int b = p & 1;
-    if (threadIdx.x == 0) s_has[b ^ 1] = build_piece<N>(kp, off, rec, sm, it, done, b ^ 1) > 0;
+    if (threadIdx.x == 0) sm.has[b ^ 1] = build_piece<N>(g, off, rec, sm, it, done, b ^ 1) > 0;
     if (!mbar_wait_bounded(&sm.full[b], (uint32_t)((p >> 1) & 1), kWaitLimitNs)) {
       ok = false;
       break;
@@ -474,30 +692,35 @@ __device__ bool staged_sweep(const KParams& kp, const int32_t* __restrict__ off,
         inbox = inbox && vd >= lo[d] && vd <= hi[d];
       }
       if (!wneed) continue;
-      const float4* sb = &sm.buf[b][sm.seg_boff[b][s] * W];
-      const int qb = sm.seg_qb[b][s], cnt = sm.seg_cnt[b][s];
-      vis(inbox, sb, qb, cnt);
+      vis(inbox, &sm.buf[b][sm.seg_boff[b][s] * W], sm.seg_qb[b][s], sm.seg_cnt[b][s]);
     }
     __syncthreads();
   }
   return ok;
 }
 
-template <int N>
-__device__ __forceinline__ void unpack_rec(const float4* r, float* c, float& payload) {
-  constexpr int W = Rec<N>::kWords;
-  float buf[4 * W];
-#pragma unroll
-  for (int k = 0; k < W; ++k) {
-    const float4 v = r[k];
-    buf[4 * k + 0] = v.x;
-    buf[4 * k + 1] = v.y;
-    buf[4 * k + 2] = v.z;
-    buf[4 * k + 3] = v.w;
-  }
-#pragma unroll
-  for (int d = 0; d < N; ++d) c[d] = buf[d];
-  payload = buf[Rec<N>::kPayload];
+// Chunk of the CTA: tile, event grid and home position of this thread.
+struct ChunkHome {
+  int t;
+  const EvGrid* g;
+  int pos;
+  bool valid;
+};
+
+__device__ __forceinline__ bool chunk_home(const KParams& kp, Events ev, const int32_t* __restrict__ off,
+                                           const int32_t* __restrict__ ord, const int32_t* __restrict__ chunk_tile,
+                                           const uint32_t* __restrict__ chunk_off,
+                                           const uint32_t* __restrict__ chunk_total, ChunkHome& h) {
+  const int w = blockIdx.x;
+  if (w >= (int)*chunk_total) return false;
+  h.t = chunk_tile[w];
+  h.g = ev.eg + find_event(ev.tile, kp.n_events, h.t);
+  const int beg = off[h.t];
+  const int start = (w - (int)chunk_off[h.t]) * kChunk;
+  const int cnt = min(kChunk, off[h.t + 1] - beg - start);
+  h.valid = (int)threadIdx.x < cnt;
+  h.pos = ord[beg + start + (h.valid ? (int)threadIdx.x : 0)];
+  return true;
 }
 
 // ---- stage 2: local density --------------------------------------------------
@@ -505,57 +728,54 @@ __device__ __forceinline__ void unpack_rec(const float4* r, float* c, float& pay
 // lexicographically, ascending index inside a tile), term = k(d, i, j) * w_j for every
 // candidate with d <= dc; candidates beyond dc contribute +-0 and are skipped.
 template <int N, int MT>
-__global__ void __launch_bounds__(kTileThreads) k_density(const KParams kp, const DevGrid* __restrict__ g,
+__global__ void __launch_bounds__(kTileThreads) k_density(const KParams kp, Events ev,
                                                           const int32_t* __restrict__ off,
                                                           const int32_t* __restrict__ ord,
                                                           const int32_t* __restrict__ chunk_tile,
                                                           const uint32_t* __restrict__ chunk_off,
                                                           const uint32_t* __restrict__ chunk_total,
                                                           const float4* __restrict__ rec_w,
+                                                          const float4* __restrict__ blk,
                                                           float4* __restrict__ rec_r, DevStatus* st) {
   using M = Metric<N, MT>;
   constexpr int W = Rec<N>::kWords;
   __shared__ StageSmem<N> sm;
-  const int w = blockIdx.x;
-  if (w >= (int)*chunk_total) return;
-  const int t = chunk_tile[w];
-  const int beg = off[t];
-  const int start = (w - (int)chunk_off[t]) * kChunk;
-  const int cnt = min(kChunk, off[t + 1] - beg - start);
-  const int k = threadIdx.x;
-  const bool valid = k < cnt;
-  const int pos = ord[beg + start + (valid ? k : 0)];
+  ChunkHome h;
+  if (!chunk_home(kp, ev, off, ord, chunk_tile, chunk_off, chunk_total, h)) return;
+  const int pos = h.pos;
+  const bool valid = h.valid;
   float x[N], wi;
   load_rec<N>(rec_w, pos, x, wi);
   int hb[N], lo[N], hi[N];
-  home_bins<N>(kp, t, hb);
-  lane_box<N>(kp, g, x, kp.dc, hb, lo, hi);
+  home_bins<N>(h.g, h.t, hb);
+  lane_box<N>(kp, h.g, x, kp.dc, hb, lo, hi);
   const bool flat = kp.kernel_type == CLUE_KERNEL_FLAT;
   const float kflat = kp.kpar[0];
   const float tdc = kp.t_dc;
   float rho = 0.0f;
-  const bool ok = staged_sweep<N>(kp, off, rec_w, sm, lo, hi, valid,
-                                  [&](bool inbox, const float4* sb, int qb, int n_) {
-    if (flat) {
+  const bool ok = staged_sweep<N>(h.g, off, rec_w, sm, lo, hi, valid, [&](bool inbox, const float4* sb, int qb, int n_) {
+    scan_blocks<N, M>(kp, blk, x, inbox, tdc, false, -INFINITY, qb, n_, [&](int j0, int j1) {
+      if (flat) {
 #pragma unroll 4
-      for (int j = 0; j < n_; ++j) {
-        float c[N], wj;
-        unpack_rec<N>(sb + j * W, c, wj);
-        const float s = M::partial(x, c, kp.mpar);
-        const float term = (qb + j == pos) ? wj : fmul(kflat, wj);
-        if (inbox && s <= tdc) rho = fadd(rho, term);
-      }
-    } else {
-      for (int j = 0; j < n_; ++j) {
-        float c[N], wj;
-        unpack_rec<N>(sb + j * W, c, wj);
-        const float s = M::partial(x, c, kp.mpar);
-        if (inbox && s <= tdc) {
-          const float kv = (qb + j == pos) ? 1.0f : kernel_value(kp.kernel_type, kp.kpar, M::finish(s));
-          rho = fadd(rho, fmul(kv, wj));
+        for (int j = j0; j < j1; ++j) {
+          float c[N], wj;
+          unpack_rec<N>(sb + j * W, c, wj);
+          const float s = M::partial(x, c, kp.mpar);
+          const float term = (qb + j == pos) ? wj : fmul(kflat, wj);
+          if (inbox && s <= tdc) rho = fadd(rho, term);
+        }
+      } else {
+        for (int j = j0; j < j1; ++j) {
+          float c[N], wj;
+          unpack_rec<N>(sb + j * W, c, wj);
+          const float s = M::partial(x, c, kp.mpar);
+          if (inbox && s <= tdc) {
+            const float kv = (qb + j == pos) ? 1.0f : kernel_value(kp.kernel_type, kp.kpar, M::finish(s));
+            rho = fadd(rho, fmul(kv, wj));
+          }
         }
       }
-    }
+    });
   });
   if (!ok) {
     if (threadIdx.x == 0) atomicOr(&st->stage_timeout, 1u);
@@ -571,37 +791,33 @@ __global__ void __launch_bounds__(kTileThreads) k_density(const KParams kp, cons
 // candidate with the smallest (distance, -rho, index) (TIE == CLUE_TIE_RHO_INDEX).
 template <int N, int MT, int TIE>
 __global__ void __launch_bounds__(kTileThreads) k_nearest_higher(
-    const KParams kp, const DevGrid* __restrict__ g, const int32_t* __restrict__ off,
-    const int32_t* __restrict__ ord, const int32_t* __restrict__ chunk_tile,
-    const uint32_t* __restrict__ chunk_off, const uint32_t* __restrict__ chunk_total,
-    const float4* __restrict__ rec_r, const int32_t* __restrict__ perm, int32_t* __restrict__ nh_s,
-    float* __restrict__ delta_s, DevStatus* st) {
+    const KParams kp, Events ev, const int32_t* __restrict__ off, const int32_t* __restrict__ ord,
+    const int32_t* __restrict__ chunk_tile, const uint32_t* __restrict__ chunk_off,
+    const uint32_t* __restrict__ chunk_total, const float4* __restrict__ rec_r, const float4* __restrict__ blk,
+    const int32_t* __restrict__ perm, int32_t* __restrict__ nh_s, float* __restrict__ delta_s, DevStatus* st) {
   using M = Metric<N, MT>;
   constexpr int W = Rec<N>::kWords;
   __shared__ StageSmem<N> sm;
-  const int w = blockIdx.x;
-  if (w >= (int)*chunk_total) return;
-  const int t = chunk_tile[w];
-  const int beg = off[t];
-  const int start = (w - (int)chunk_off[t]) * kChunk;
-  const int cnt = min(kChunk, off[t + 1] - beg - start);
-  const int k = threadIdx.x;
-  const bool valid = k < cnt;
-  const int pos = ord[beg + start + (valid ? k : 0)];
+  ChunkHome h;
+  if (!chunk_home(kp, ev, off, ord, chunk_tile, chunk_off, chunk_total, h)) return;
+  const int pos = h.pos;
+  const bool valid = h.valid;
   float x[N], rho_i;
   load_rec<N>(rec_r, pos, x, rho_i);
   const int orig_i = perm[pos];
   int hb[N], lo[N], hi[N];
-  home_bins<N>(kp, t, hb);
-  lane_box<N>(kp, g, x, kp.dm, hb, lo, hi);
+  home_bins<N>(h.g, h.t, hb);
+  lane_box<N>(kp, h.g, x, kp.dm, hb, lo, hi);
   const float tdm = kp.t_dm;
   float delta = FLT_MAX, s_best = INFINITY, rho_best = 0.0f;
   int nh = -1, orig_best = INT_MAX;
-  const bool ok = staged_sweep<N>(kp, off, rec_r, sm, lo, hi, valid,
-                                  [&](bool inbox, const float4* sb, int qb, int n_) {
+  const bool ok = staged_sweep<N>(h.g, off, rec_r, sm, lo, hi, valid, [&](bool inbox, const float4* sb, int qb, int n_) {
     if (!__any_sync(0xffffffffu, inbox)) return;
+    const bool strict = TIE == CLUE_TIE_REFERENCE;
+    scan_blocks<N, M>(kp, blk, x, inbox, fminf(tdm, s_best), strict && s_best <= tdm, rho_i, qb, n_,
+                      [&](int j0, int j1) {
 #pragma unroll 4
-    for (int j = 0; j < n_; ++j) {
+    for (int j = j0; j < j1; ++j) {
       float c[N], rho_j;
       unpack_rec<N>(sb + j * W, c, rho_j);
       const float s = M::partial(x, c, kp.mpar);
@@ -635,6 +851,7 @@ __global__ void __launch_bounds__(kTileThreads) k_nearest_higher(
         }
       }
     }
+    });
   });
   if (!ok) {
     if (threadIdx.x == 0) atomicOr(&st->stage_timeout, 1u);
@@ -645,7 +862,10 @@ __global__ void __launch_bounds__(kTileThreads) k_nearest_higher(
     delta_s[pos] = delta;
   }
   const uint32_t none = __ballot_sync(0xffffffffu, valid && nh < 0);
-  if ((threadIdx.x & 31) == 0 && none) atomicAdd(&st->seed_candidates, (uint32_t)__popc(none));
+  if ((threadIdx.x & 31) == 0 && none) {
+    atomicAdd(&st->seed_candidates, (uint32_t)__popc(none));
+    atomicAdd(const_cast<uint32_t*>(&h.g->seed_candidates), (uint32_t)__popc(none));
+  }
 }
 
 // ---- stage 4: seeds (KernelFindClusters) ---------------------------------------
@@ -701,28 +921,32 @@ __global__ void __launch_bounds__(256) k_jump(int32_t* par, int n, int iters, De
   if (blockIdx.x == 0 && threadIdx.x == 0) atomicMax(&st->label_rounds, (uint32_t)round + 1);
 }
 
-// Labels from the roots and scatter of every output back to the caller's order.
+// Seed list capacity of an event: every seed, or the reference's SeedArray capacity
+// max(seed_capacity, points without nearest higher) (SetupSeeds.hpp:10-20).
+__device__ __forceinline__ int64_t seed_cap(const KParams& kp, const EvGrid* g) {
+  if (kp.seed_capacity < 0) return INT64_MAX;
+  return kp.seed_capacity > (int64_t)g->seed_candidates ? kp.seed_capacity : (int64_t)g->seed_candidates;
+}
+
+// Labels from the roots (seed rank inside its event) and scatter of every output back to
+// the caller's order.
 template <int N>
-__global__ void __launch_bounds__(256) k_finalize(const KParams kp, int n, const int32_t* __restrict__ par,
+__global__ void __launch_bounds__(256) k_finalize(const KParams kp, Events ev, const int32_t* __restrict__ par,
                                                   const int32_t* __restrict__ is_seed_s,
                                                   const uint32_t* __restrict__ seed_rank,
                                                   const int32_t* __restrict__ perm,
                                                   const int32_t* __restrict__ nh_s,
                                                   const float4* __restrict__ rec_r,
-                                                  const float* __restrict__ delta_s, const DevStatus* st,
-                                                  clue_outputs out) {
-  const int64_t cap = kp.seed_capacity < 0
-                          ? INT64_MAX
-                          : (kp.seed_capacity > (int64_t)st->seed_candidates ? kp.seed_capacity
-                                                                             : (int64_t)st->seed_candidates);
+                                                  const float* __restrict__ delta_s, clue_outputs out) {
   const int stride = gridDim.x * blockDim.x;
-  for (int pos = blockIdx.x * blockDim.x + threadIdx.x; pos < n; pos += stride) {
+  for (int pos = blockIdx.x * blockDim.x + threadIdx.x; pos < kp.n; pos += stride) {
     const int p = par[pos];
     const int root = p >= 0 ? p : pos;
     int lab = -1;
     if (is_seed_s[root]) {
-      const uint32_t rk = seed_rank[perm[root]];
-      if ((int64_t)rk < cap) lab = (int)rk;
+      const int e = find_event(ev.pt, kp.n_events, pos);
+      const uint32_t rk = seed_rank[perm[root]] - seed_rank[ev.pt[e]];
+      if ((int64_t)rk < seed_cap(kp, ev.eg + e)) lab = (int)rk;
     }
     const int i = perm[pos];
     out.cluster_index[i] = lab;
@@ -741,6 +965,24 @@ __global__ void __launch_bounds__(256) k_finalize(const KParams kp, int n, const
   }
 }
 
+// Per-event seeds and clusters: n_seeds[e], n_clusters[e] (optional outputs) and the total of
+// clusters over all events in st->n_clusters.
+__global__ void k_event_info(const KParams kp, const EvGrid* __restrict__ eg, const int32_t* __restrict__ ev_pt,
+                             const uint32_t* __restrict__ seed_rank, const uint32_t* __restrict__ seed_total,
+                             int32_t* __restrict__ n_seeds, int32_t* __restrict__ n_clusters, DevStatus* st) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < kp.n_events; e += stride) {
+    const uint32_t a = seed_rank[ev_pt[e]];
+    const uint32_t b = e + 1 < kp.n_events ? seed_rank[ev_pt[e + 1]] : *seed_total;
+    const int64_t ns = (int64_t)(b - a);
+    const int64_t cap = seed_cap(kp, eg + e);
+    const int64_t nc = ns < cap ? ns : cap;
+    if (n_seeds) n_seeds[e] = (int32_t)ns;
+    if (n_clusters) n_clusters[e] = (int32_t)nc;
+    atomicAdd(&st->n_clusters, (uint32_t)nc);
+  }
+}
+
 int grid_for(int n, int threads) {
   int b = (n + threads - 1) / threads;
   const int cap = 148 * 32;
@@ -749,27 +991,29 @@ int grid_for(int n, int threads) {
 
 inline int chunk_grid(const KParams& kp) { return kp.n / kChunk + kp.ntiles + 1; }
 
+inline Events events_of(Workspace& ws) { return Events{ws.ev, ws.ev_pt, ws.ev_tile}; }
+
 template <int N, int MT>
 void launch_density(const KParams& kp, Workspace& ws, cudaStream_t s) {
-  k_density<N, MT><<<chunk_grid(kp), kTileThreads, 0, s>>>(kp, ws.grid, ws.offsets, ws.ord_rho, ws.chunk_tile,
-                                                            ws.chunk_count, ws.chunk_total, ws.rec_w, ws.rec_r,
-                                                            ws.status);
+  k_density<N, MT><<<chunk_grid(kp), kTileThreads, 0, s>>>(kp, events_of(ws), ws.offsets, ws.ord_rho,
+                                                            ws.chunk_tile, ws.chunk_count, ws.chunk_total,
+                                                            ws.rec_w, ws.blk, ws.rec_r, ws.status);
 }
 template <int N, int MT>
 void launch_nh(const KParams& kp, Workspace& ws, cudaStream_t s) {
   if (kp.tiebreak == CLUE_TIE_RHO_INDEX)
     k_nearest_higher<N, MT, CLUE_TIE_RHO_INDEX><<<chunk_grid(kp), kTileThreads, 0, s>>>(
-        kp, ws.grid, ws.offsets, ws.ord_nh, ws.chunk_tile, ws.chunk_count, ws.chunk_total, ws.rec_r, ws.perm,
-        ws.nh_s, ws.delta_s, ws.status);
+        kp, events_of(ws), ws.offsets, ws.ord_nh, ws.chunk_tile, ws.chunk_count, ws.chunk_total, ws.rec_r,
+        ws.blk, ws.perm, ws.nh_s, ws.delta_s, ws.status);
   else
     k_nearest_higher<N, MT, CLUE_TIE_REFERENCE><<<chunk_grid(kp), kTileThreads, 0, s>>>(
-        kp, ws.grid, ws.offsets, ws.ord_nh, ws.chunk_tile, ws.chunk_count, ws.chunk_total, ws.rec_r, ws.perm,
-        ws.nh_s, ws.delta_s, ws.status);
+        kp, events_of(ws), ws.offsets, ws.ord_nh, ws.chunk_tile, ws.chunk_count, ws.chunk_total, ws.rec_r,
+        ws.blk, ws.perm, ws.nh_s, ws.delta_s, ws.status);
 }
 template <int N, int MT>
-void launch_seeds(const KParams& kp, Workspace& ws, int n, cudaStream_t s) {
-  k_seeds<N, MT><<<grid_for(n, 256), 256, 0, s>>>(kp, n, ws.rec_r, ws.nh_s, ws.perm, ws.is_seed_s, ws.par,
-                                                  ws.seed_flag);
+void launch_seeds(const KParams& kp, Workspace& ws, cudaStream_t s) {
+  k_seeds<N, MT><<<grid_for(kp.n, 256), 256, 0, s>>>(kp, kp.n, ws.rec_r, ws.nh_s, ws.perm, ws.is_seed_s, ws.par,
+                                                     ws.seed_flag);
 }
 
 #define CLUE_METRIC_SWITCH(mt, FN, ...)                                           \
@@ -795,43 +1039,53 @@ constexpr int kJumpIters = 64;
 template <int N>
 clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
   const KParams& kp = a.kp;
-  const int n = a.n;
+  const int n = kp.n;
   InPtrs in{};
   for (int d = 0; d < N; ++d) in.c[d] = a.coords[d];
   in.w = a.weight;
+  const Events ev = events_of(ws);
 
   stage_mark(ws, 0, s);
-  k_init<N><<<1, 64, 0, s>>>(ws.grid, ws.status);
-  k_bbox<N><<<grid_for(n, 256), 256, 0, s>>>(in, n, ws.grid, ws.status);
-  k_grid<N><<<1, 32, 0, s>>>(kp, ws.grid);
-  k_bin<N><<<grid_for(n, 256), 256, 0, s>>>(kp, in, n, ws.grid, ws.keys[0]);
-  const int cur = radix_sort_pairs(ws.keys, ws.vals, true, n, bits_for((uint32_t)(kp.ntiles - 1)), ws.hist,
-                                   ws.scan_scratch, s);
+  k_init<N><<<grid_for(kp.n_events, 256), 256, 0, s>>>(kp, ev, ws.ev_pt, ws.ev_tile, ws.status);
+  if (kp.n_events == 1)
+    k_bbox_single<N><<<grid_for(n, 256), 256, 0, s>>>(in, n, ws.ev, ws.status);
+  else
+    k_bbox_events<N><<<kp.n_events < 148 * 16 ? kp.n_events : 148 * 16, 256, 0, s>>>(in, kp.n_events, ws.ev,
+                                                                                    ws.status);
+  k_grid<N><<<grid_for(kp.n_events, 256), 256, 0, s>>>(kp.n_events, ws.ev);
+  k_bin<N><<<grid_for(n, 256), 256, 0, s>>>(kp, in, ev, ws.keys[0]);
+  const int bits = bits_for((uint32_t)(kp.ntiles - 1));
+  const int cur = radix_sort_pairs(ws.keys, ws.vals, true, n, bits, ws.hist, ws.scan_scratch, s);
   ws.perm = ws.vals[cur];
   ws.sorted_keys = ws.keys[cur];
   offsets_from_sorted(ws.sorted_keys, n, kp.ntiles, ws.offsets, s);
   k_gather<N><<<grid_for(n, 256), 256, 0, s>>>(in, n, ws.perm, ws.rec_w);
-  k_order<N><<<kp.ntiles, kTileThreads, 0, s>>>(kp, ws.grid, ws.offsets, ws.rec_w, ws.ord_rho, ws.ord_nh,
+  k_order<N><<<kp.ntiles, kTileThreads, 0, s>>>(kp, ev, ws.offsets, ws.rec_w, ws.ord_rho, ws.ord_nh,
                                                 ws.chunk_count);
   exclusive_scan(ws.chunk_count, ws.chunk_count, (size_t)kp.ntiles, ws.scan_scratch, ws.chunk_total, s);
   k_chunk_map<<<grid_for(kp.ntiles, 256), 256, 0, s>>>(kp.ntiles, ws.offsets, ws.chunk_count, ws.chunk_tile);
 
+  k_block_bbox<N><<<grid_for(((n + 31) >> 5) * 32, 256), 256, 0, s>>>(ws.rec_w, n, ws.blk);
+
   stage_mark(ws, 1, s);
   CLUE_METRIC_SWITCH(a.metric, launch_density, kp, ws, s);
   stage_mark(ws, 2, s);
+  k_block_bbox<N><<<grid_for(((n + 31) >> 5) * 32, 256), 256, 0, s>>>(ws.rec_r, n, ws.blk);
   CLUE_METRIC_SWITCH(a.metric, launch_nh, kp, ws, s);
   stage_mark(ws, 3, s);
-  CLUE_METRIC_SWITCH(a.metric, launch_seeds, kp, ws, n, s);
+  CLUE_METRIC_SWITCH(a.metric, launch_seeds, kp, ws, s);
   exclusive_scan(ws.seed_flag, ws.seed_flag, (size_t)n, ws.scan_scratch, ws.seed_total, s);
   for (int r = 0; r < kJumpLaunches; ++r)
     k_jump<<<grid_for(n, 256), 256, 0, s>>>(ws.par, n, kJumpIters, ws.status, r);
-  k_finalize<N><<<grid_for(n, 256), 256, 0, s>>>(kp, n, ws.par, ws.is_seed_s, ws.seed_flag, ws.perm, ws.nh_s,
-                                                 ws.rec_r, ws.delta_s, ws.status, a.out);
+  k_finalize<N><<<grid_for(n, 256), 256, 0, s>>>(kp, ev, ws.par, ws.is_seed_s, ws.seed_flag, ws.perm, ws.nh_s,
+                                                 ws.rec_r, ws.delta_s, a.out);
+  k_event_info<<<grid_for(kp.n_events, 256), 256, 0, s>>>(kp, ws.ev, ws.ev_pt, ws.seed_flag, ws.seed_total,
+                                                         a.ev_n_seeds, a.ev_n_clusters, ws.status);
   stage_mark(ws, 4, s);
-  // init, bbox, grid, bin, sort, offsets, gather, order, scan, chunk map, density, nh, seeds, scan,
-  // jumps, finalize
-  ws.launches += 4 + radix_sort_launches(bits_for((uint32_t)(kp.ntiles - 1))) + 2 + 1 + kScanLaunches + 1 + 3 +
-                 kScanLaunches + kJumpLaunches + 1;
+  // init, bbox, grid, bin, sort, offsets, gather, order, scan, chunk map, 2 block boxes, density, nh,
+  // seeds, scan, jumps, finalize, event info
+  ws.launches += 4 + radix_sort_launches(bits) + 2 + 1 + kScanLaunches + 1 + 2 + 3 + kScanLaunches +
+                 kJumpLaunches + 1 + 1;
   CLUE_CUDA_TRY(cudaGetLastError());
   return CLUE_OK;
 }
@@ -840,7 +1094,7 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
 // unresolved (only for very deep nearest-higher chains); synchronises per launch.
 template <int N>
 clue_status finish_labels(Workspace& ws, const RunArgs& a, cudaStream_t s, int first_round) {
-  const int n = a.n;
+  const int n = a.kp.n;
   for (int r = first_round; r < 64; ++r) {
     k_jump<<<grid_for(n, 256), 256, 0, s>>>(ws.par, n, 1 << 12, ws.status, r);
     ++ws.launches;
@@ -849,8 +1103,8 @@ clue_status finish_labels(Workspace& ws, const RunArgs& a, cudaStream_t s, int f
     CLUE_CUDA_TRY(cudaStreamSynchronize(s));
     if (unres == 0) break;
   }
-  k_finalize<N><<<grid_for(n, 256), 256, 0, s>>>(a.kp, n, ws.par, ws.is_seed_s, ws.seed_flag, ws.perm, ws.nh_s,
-                                                 ws.rec_r, ws.delta_s, ws.status, a.out);
+  k_finalize<N><<<grid_for(n, 256), 256, 0, s>>>(a.kp, events_of(ws), ws.par, ws.is_seed_s, ws.seed_flag, ws.perm,
+                                                 ws.nh_s, ws.rec_r, ws.delta_s, a.out);
   ++ws.launches;
   CLUE_CUDA_TRY(cudaGetLastError());
   return CLUE_OK;

@@ -72,6 +72,8 @@ struct RunArgs {
   const float* weight;           // device
   clue_outputs out;              // device pointers (may be null except cluster_index)
   int32_t metric;
+  int32_t* ev_n_seeds;           // device [n_events] or null (batched calls)
+  int32_t* ev_n_clusters;        // device [n_events] or null (batched calls)
 };
 
 template <int N>
@@ -85,10 +87,15 @@ struct Workspace {
   int device = 0;
   // current capacities
   size_t cap_n = 0, cap_tiles = 0, cap_words = 0;
+  size_t cap_events = 0;
   void* arena = nullptr;
   size_t arena_bytes = 0;
 
-  DevGrid* grid = nullptr;
+  // event tables, one contiguous block: EvGrid[cap_events], ev_pt[cap_events + 1],
+  // ev_tile[cap_events + 1] (uploaded in one copy for batched calls)
+  EvGrid* ev = nullptr;
+  int32_t* ev_pt = nullptr;
+  int32_t* ev_tile = nullptr;
   DevStatus* status = nullptr;
   uint32_t* keys[2] = {nullptr, nullptr};
   int32_t* vals[2] = {nullptr, nullptr};
@@ -103,13 +110,14 @@ struct Workspace {
   int32_t* is_seed_s = nullptr;
   uint32_t* seed_flag = nullptr;  // original order, then exclusive-scanned to ranks
   uint32_t* seed_total = nullptr;
+  float4* blk = nullptr;          // bounding boxes of 32-record blocks of the sorted records
   int32_t* ord_rho = nullptr;     // per-tile home order for the density sweep
   int32_t* ord_nh = nullptr;      // per-tile home order for the nearest-higher sweep
   uint32_t* chunk_count = nullptr;  // [ntiles] chunks per tile, then exclusive-scanned
   int32_t* chunk_tile = nullptr;  // [max chunks] tile of every chunk
   uint32_t* chunk_total = nullptr;
 
-  // host staging for CLUE_MEM_HOST calls
+  // pinned host copy of the event tables (same layout as the device block)
   void* pinned = nullptr;
   size_t pinned_bytes = 0;
   DevStatus* status_host = nullptr;  // pinned mirror of *status
@@ -126,19 +134,28 @@ struct Workspace {
   // optional per-stage timing (clue_context_set_timing)
   bool timing = false;
   uint64_t launches = 0;  // kernels launched by this workspace (clue_context_kernel_launches)
-  cudaEvent_t ev[CLUE_N_STAGES + 1] = {};
+  cudaEvent_t tev[CLUE_N_STAGES + 1] = {};
 };
 
 // Records stage boundary k on s when timing is enabled.
 inline void stage_mark(Workspace& ws, int k, cudaStream_t s) {
-  if (ws.timing && ws.ev[k]) cudaEventRecord(ws.ev[k], s);
+  if (ws.timing && ws.tev[k]) cudaEventRecord(ws.tev[k], s);
 }
 
-clue_status workspace_reserve(Workspace& ws, int ndim, size_t n, size_t ntiles);
+clue_status workspace_reserve(Workspace& ws, int ndim, size_t n, size_t ntiles, size_t n_events = 1);
+
+// Bytes of the event-table block for `cap` events, and its three parts inside a block.
+inline size_t event_table_bytes(size_t cap) { return cap * sizeof(EvGrid) + 2 * (cap + 1) * sizeof(int32_t); }
+inline void event_table_carve(void* base, size_t cap, EvGrid** eg, int32_t** pt, int32_t** tile) {
+  *eg = static_cast<EvGrid*>(base);
+  *pt = reinterpret_cast<int32_t*>(static_cast<char*>(base) + cap * sizeof(EvGrid));
+  *tile = *pt + cap + 1;
+}
 void workspace_release(Workspace& ws);
 
 // Host helpers (clue_capi.cu)
 float threshold_for(float r, bool root);
+int lower_bounds_ok(const clue_metric* m, int ndim);
 void grid_shape(int32_t n, int32_t ppbin, int32_t ndim, int32_t* nperdim, int32_t* ntiles);
 
 }  // namespace clue_b200

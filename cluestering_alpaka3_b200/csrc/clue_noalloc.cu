@@ -65,6 +65,7 @@ size_t up256(size_t x) { return (x + 255) / 256 * 256; }
 
 // Carves the scratch array into the pipeline's buffers; false if it does not fit.
 bool carve(Workspace& ws, void* base, int ndim, size_t n, size_t ntiles) {
+  void* evtab = nullptr;
   const size_t w = (size_t)((ndim + 1 + 3) / 4);
   const size_t nb = (size_t)sort_blocks((int)n);
   const size_t hist_len = (size_t)kRadix * nb;
@@ -73,7 +74,7 @@ bool carve(Workspace& ws, void* base, int ndim, size_t n, size_t ntiles) {
     void** ptr;
     size_t bytes;
   } items[] = {
-      {(void**)&ws.grid, sizeof(DevGrid)},
+      {&evtab, event_table_bytes(1)},
       {(void**)&ws.status, sizeof(DevStatus)},
       {(void**)&ws.keys[0], n * 4},
       {(void**)&ws.keys[1], n * 4},
@@ -90,6 +91,7 @@ bool carve(Workspace& ws, void* base, int ndim, size_t n, size_t ntiles) {
       {(void**)&ws.is_seed_s, n * 4},
       {(void**)&ws.seed_flag, n * 4},
       {(void**)&ws.seed_total, 16},
+      {(void**)&ws.blk, (n / 32 + 1) * 6 * 16},
       {(void**)&ws.ord_rho, n * 4},
       {(void**)&ws.ord_nh, n * 4},
       {(void**)&ws.chunk_count, (ntiles + 1) * 4},
@@ -104,6 +106,8 @@ bool carve(Workspace& ws, void* base, int ndim, size_t n, size_t ntiles) {
     *it.ptr = static_cast<unsigned char*>(base) + o;
     o += up256(it.bytes);
   }
+  event_table_carve(evtab, 1, &ws.ev, &ws.ev_pt, &ws.ev_tile);
+  ws.cap_events = 1;
   ws.arena = base;
   ws.arena_bytes = total;
   ws.cap_n = n;
@@ -183,14 +187,16 @@ extern "C" clue_status clue_make_clusters_noalloc(const clue_params* params, con
   kp.rhoc = params->rhoc;
   kp.t_dc = threshold_for(params->dc, root);
   kp.t_dm = threshold_for(params->dm, root);
+  kp.lb_ok = lower_bounds_ok(metric, ndim);
   kp.kernel_type = kernel->type;
   for (int k = 0; k < 3; ++k) kp.kpar[k] = kernel->par[k];
   for (int d = 0; d < ndim; ++d) kp.mpar[d] = metric->par[d];
-  kp.nperdim = npd;
+  kp.nperdim0 = npd;
   kp.ntiles = nt;
+  kp.n_events = 1;
   int64_t stride = 1;
   for (int d = ndim - 1; d >= 0; --d) {
-    kp.stride[d] = (int32_t)stride;
+    kp.stride0[d] = (int32_t)stride;
     stride *= npd;
   }
   for (int d = 0; d < ndim; ++d) kp.wrapped[d] = params->wrapped[d] ? 1 : 0;
@@ -229,7 +235,7 @@ extern "C" clue_status clue_make_clusters_noalloc(const clue_params* params, con
     const int64_t cap = kp.seed_capacity < 0 ? -1
                                              : std::max<int64_t>(kp.seed_capacity, (int64_t)h.seed_candidates);
     info->n_seeds = nseeds;
-    info->n_clusters = cap < 0 ? nseeds : std::min(nseeds, cap);
+    info->n_clusters = h.n_clusters;
     info->dropped_seeds = nseeds - info->n_clusters;
     info->seed_capacity_used = cap;
     info->n_tiles = nt;

@@ -113,7 +113,7 @@ typedef struct clue_run_info {
   int64_t n_seeds;             /* points flagged as seeds */
   int64_t n_clusters;          /* seeds kept in the seed list (= clusters labelled) */
   int64_t dropped_seeds;       /* seeds beyond the seed capacity */
-  int64_t seed_capacity_used;  /* -1 when every seed is kept */
+  int64_t seed_capacity_used;  /* -1 when every seed is kept; -2: per event (batched call) */
   int64_t n_tiles;             /* tiles of the reference grid */
   int64_t n_per_dim;
   int64_t label_rounds;        /* pointer-jumping rounds that changed a parent */
@@ -203,6 +203,50 @@ clue_status clue_context_set_timing(clue_context ctx, int32_t enable);
 clue_status clue_context_stage_times(clue_context ctx, float* ms, int32_t n_stages);
 /* Kernels this context has launched so far (all runs). */
 uint64_t clue_context_kernel_launches(clue_context ctx);
+
+/* ---- batched events (no reference counterpart) -------------------------------
+ * Clusters n_events independent events in one pass.  Event e is the points
+ * [event_offsets[e], event_offsets[e + 1]) of the concatenated SoA input
+ * (coords[d * n_total + i], n_total = event_offsets[n_events]); event_offsets is a HOST array
+ * of n_events + 1 entries, every event holding at least one point.  Each event gets its
+ * own reference tile grid and its labels are numbered from 0 inside the event, exactly as if
+ * it had been clustered alone.  ev_n_clusters (optional, n_events entries, same memory space
+ * as the outputs) receives every event's cluster count; `info` holds the totals.
+ */
+clue_status clue_batch_make_clusters(clue_context ctx, const clue_params* params, const clue_kernel* kernel,
+                                     const clue_metric* metric, int32_t ndim, int32_t n_events,
+                                     const int32_t* event_offsets, const float* coords, const float* weight,
+                                     const clue_outputs* out, int32_t* ev_n_clusters, int32_t memory,
+                                     void* stream, clue_run_info* info);
+/* Device memory only, no host synchronisation (see clue_make_clusters_async). */
+clue_status clue_batch_make_clusters_async(clue_context ctx, const clue_params* params,
+                                           const clue_kernel* kernel, const clue_metric* metric, int32_t ndim,
+                                           int32_t n_events, const int32_t* event_offsets, const float* coords,
+                                           const float* weight, const clue_outputs* out, int32_t* ev_n_clusters,
+                                           void* stream);
+
+/* The plain single-event pipeline run once per event, back to back on `stream` (device
+ * memory; same inputs, outputs and per-event label numbering as the batched call, but the
+ * nearest-higher chain depth is limited to what the enqueued label rounds resolve).
+ * This is the per-event launch loop that the batched path replaces.  With event_ms non-NULL
+ * (host, n_events floats) the call synchronises and writes every event's device time. */
+clue_status clue_events_loop(clue_context ctx, const clue_params* params, const clue_kernel* kernel,
+                             const clue_metric* metric, int32_t ndim, int32_t n_events,
+                             const int32_t* event_offsets, const float* coords, const float* weight,
+                             const clue_outputs* out, void* stream, float* event_ms);
+
+/* The whole batched pipeline (event-table upload and every stage) captured once into an
+ * executable CUDA graph; each clue_graph_launch replays it on the same buffers.  Needs a
+ * non-default stream.  The context must not run other work between capture and the last
+ * launch that relies on its workspace. */
+typedef struct clue_graph_s* clue_graph;
+clue_status clue_graph_capture_batch(clue_context ctx, const clue_params* params, const clue_kernel* kernel,
+                                     const clue_metric* metric, int32_t ndim, int32_t n_events,
+                                     const int32_t* event_offsets, const float* coords, const float* weight,
+                                     const clue_outputs* out, int32_t* ev_n_clusters, void* stream,
+                                     clue_graph* graph);
+clue_status clue_graph_launch(clue_graph graph, void* stream);
+clue_status clue_graph_destroy(clue_graph graph);
 
 /*
  * clue_make_clusters_noalloc -- no counterpart in the reference.

@@ -519,7 +519,7 @@ static double kernel_f64(const oracle_params* p, double dist, int32_t i, int32_t
 }
 
 int oracle_rho_f64(const oracle_params* p, int32_t n, const float* coords, const float* weight,
-                   double* rho64) {
+                   double* rho64, uint8_t* near_dc, double rel_tol) {
   if (check_params(p, n)) return -1;
   grid_t g;
   int32_t *off = NULL, *idx = NULL;
@@ -536,15 +536,19 @@ int oracle_rho_f64(const oracle_params* p, int32_t n, const float* coords, const
     load_point(N, n, coords, i, xi);
     search_box(&g, xi, p->dc, lo, hi);
     double rho = 0.0;
+    int near = 0;
+    const double dc = (double)p->dc;
     BOX_LOOP_BEGIN(&g, lo, hi)
     for (int32_t q = off[tile_]; q < off[tile_ + 1]; ++q) {
       const int32_t j = idx[q];
       load_point(N, n, coords, j, xj);
       const double dist = metric_f64(p, xi, xj);
-      if (dist <= (double)p->dc) rho += kernel_f64(p, dist, i, j) * (double)weight[j];
+      if (dist <= dc) rho += kernel_f64(p, dist, i, j) * (double)weight[j];
+      if (fabs(dist - dc) <= rel_tol * dc) near = 1;
     }
     BOX_LOOP_END(&g, lo, hi)
     rho64[i] = rho;
+    if (near_dc) near_dc[i] = (uint8_t)near;
   }
   free(off);
   free(idx);

@@ -84,9 +84,11 @@ int oracle_tiles(const oracle_params* p, int32_t n, const float* coords, oracle_
                  int32_t* offsets, int32_t* indexes);
 
 /* Local density in FP64 over the same candidate sets (box from the FP32 grid), the
- * tolerance reference for rho. */
+ * tolerance reference for rho.  near_dc (may be NULL) flags points with a candidate whose
+ * FP64 distance lies within rel_tol * dc of dc: FP32 and FP64 may disagree on whether that
+ * candidate counts, so their rho is reported apart instead of held to the tolerance. */
 int oracle_rho_f64(const oracle_params* p, int32_t n, const float* coords, const float* weight,
-                   double* rho64);
+                   double* rho64, uint8_t* near_dc, double rel_tol);
 
 /* Distance metric on two points (ndim floats each), exposed for metric known-answer tests. */
 float oracle_metric(const oracle_params* p, const float* a, const float* b);

@@ -69,7 +69,7 @@ def _load():
                                      ctypes.POINTER(_Grid), ctypes.c_void_p, ctypes.c_void_p]
         lib.oracle_tiles.restype = ctypes.c_int
         lib.oracle_rho_f64.argtypes = [ctypes.POINTER(_Params), ctypes.c_int32, ctypes.c_void_p,
-                                       ctypes.c_void_p, ctypes.c_void_p]
+                                       ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double]
         lib.oracle_rho_f64.restype = ctypes.c_int
         lib.oracle_metric.argtypes = [ctypes.POINTER(_Params), ctypes.c_void_p, ctypes.c_void_p]
         lib.oracle_metric.restype = ctypes.c_float
@@ -183,17 +183,21 @@ def tiles(coords: np.ndarray, cfg: Config):
     return grid, off, idx
 
 
-def rho_f64(coords: np.ndarray, weight: np.ndarray, cfg: Config) -> np.ndarray:
+def rho_f64(coords: np.ndarray, weight: np.ndarray, cfg: Config, rel_tol: float = 1e-5,
+            with_near: bool = False):
+    """FP64 densities; with_near also returns the near-dc flags (see clue_oracle.h)."""
     lib = _load()
     c = _soa(coords)
     ndim, n = c.shape
     w = np.ascontiguousarray(weight, dtype=np.float32)
     out = np.empty(n, np.float64)
+    near = np.zeros(n, np.uint8)
     p = cfg.to_struct(ndim)
-    rc = lib.oracle_rho_f64(ctypes.byref(p), n, c.ctypes.data, w.ctypes.data, out.ctypes.data)
+    rc = lib.oracle_rho_f64(ctypes.byref(p), n, c.ctypes.data, w.ctypes.data, out.ctypes.data,
+                            near.ctypes.data, rel_tol)
     if rc != 0:
         raise ValueError(f"oracle_rho_f64 failed ({rc})")
-    return out
+    return (out, near.astype(bool)) if with_near else out
 
 
 def metric(a, b, cfg: Config) -> float:

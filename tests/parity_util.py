@@ -61,3 +61,19 @@ def random_blobs(rng, n, ndim, nblobs=8, extent=100.0, sigma=1.0, noise=0.1, wei
     else:
         w = rng.uniform(0.5, 1.5, size=n).astype(np.float32)
     return np.ascontiguousarray(c), w
+
+
+def tolerance_report(rho_gpu, rho_ref32, coords, weight, cfg, labels_gpu, labels_ref, rtol=1e-5):
+    """rho within rtol of FP64 except at points whose candidates sit within rtol of dc (counted);
+    returns a dict with the counts the tests assert on and report."""
+    rho64, near = O.rho_f64(coords, weight, cfg, rel_tol=rtol, with_near=True)
+    rel = np.abs(rho_gpu.astype(np.float64) - rho64) / np.maximum(np.abs(rho64), 1e-30)
+    rel32 = np.abs(rho_ref32.astype(np.float64) - rho64) / np.maximum(np.abs(rho64), 1e-30)
+    rhoc = cfg.rhoc
+    near_rhoc = np.abs(rho64 - rhoc) <= rtol * max(rhoc, 1e-30)
+    mism = labels_gpu != labels_ref
+    return {"max_rel_far": float(rel[~near].max()) if (~near).any() else 0.0,
+            "max_rel_far_oracle32": float(rel32[~near].max()) if (~near).any() else 0.0,
+            "near_dc": int(near.sum()), "near_rhoc": int(near_rhoc.sum()),
+            "rho_not_bitexact": int((rho_gpu.view(np.uint32) != rho_ref32.view(np.uint32)).sum()),
+            "label_mismatch": int(mism.sum()), "n": len(rho_gpu)}

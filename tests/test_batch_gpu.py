@@ -1,0 +1,126 @@
+"""Batched events: one pass over many events equals clustering every event alone.
+
+Each event is checked against the CPU oracle run on that event alone (bit for bit for the
+flat kernel; within tolerance for the exponential kernel), and the CUDA-graph replay of the
+batched pipeline is checked against the direct call.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from parity_util import gpu_args
+
+pytestmark = pytest.mark.gpu
+
+
+def make_events(seed, n_events, ndim=2, lo=100, hi=4000):
+    from cluestering_alpaka3_b200 import synthetic
+    rng = np.random.default_rng(seed)
+    sizes = np.clip(np.round(rng.lognormal(np.log(800), 1.0, size=n_events)), lo, hi).astype(int)
+    evs = []
+    for s in sizes:
+        if ndim == 2:
+            evs.append(synthetic.calo_event(rng, int(s)))
+        else:
+            evs.append(synthetic.blobs_4d_event(rng, int(s)) if ndim == 4 else
+                       (rng.normal(0, 3, size=(ndim, int(s))).astype(np.float32),
+                        rng.uniform(0.5, 1.5, int(s)).astype(np.float32)))
+    off = np.concatenate([[0], np.cumsum([e[0].shape[1] for e in evs])]).astype(np.int32)
+    coords = np.ascontiguousarray(np.concatenate([e[0] for e in evs], axis=1))
+    weight = np.concatenate([e[1] for e in evs])
+    return evs, off, coords, weight
+
+
+@pytest.mark.parametrize("ndim,kernel,params", [
+    (2, ("flat", (0.5,)), dict(dc=2.0, rhoc=4.0, dm=3.0)),
+    (4, ("flat", (0.5,)), dict(dc=2.5, rhoc=6.0, dm=2.5)),
+    (3, ("flat", (0.5,)), dict(dc=1.5, rhoc=2.0, dm=2.0, seed_dc=1.0)),
+])
+def test_batch_equals_events_alone_exact(gpu_context, ndim, kernel, params):
+    evs, off, coords, weight = make_events(31 + ndim, 40, ndim=ndim)
+    p, k, m = gpu_args(kernel=kernel, **params)
+    res, ncl = gpu_context.batch_host(coords, weight, off, p, k, m)
+    tot = 0
+    for e, (c, w) in enumerate(evs):
+        a, b = off[e], off[e + 1]
+        ref = O.run(c, w, O.Config(dc=params["dc"], rhoc=params["rhoc"], dm=params["dm"],
+                                   seed_dc=params.get("seed_dc"), kernel=kernel[0], kernel_par=kernel[1]))
+        np.testing.assert_array_equal(res.cluster_index[a:b], ref.cluster_index, err_msg=f"event {e}")
+        np.testing.assert_array_equal(res.is_seed[a:b], ref.is_seed)
+        np.testing.assert_array_equal(res.rho[a:b].view(np.uint32), ref.rho.view(np.uint32))
+        nh = res.nearest_higher[a:b]
+        np.testing.assert_array_equal(np.where(nh >= 0, nh - a, -1), ref.nearest_higher)
+        assert ncl[e] == ref.stats["n_clusters"]
+        tot += ref.stats["n_clusters"]
+    assert res.info.n_clusters == tot
+
+
+def test_batch_exponential_kernel_tolerance(gpu_context):
+    evs, off, coords, weight = make_events(7, 30)
+    kw = dict(dc=2.0, rhoc=4.0, dm=3.0, kernel=("exp", (1.0, 1.0)))
+    res, ncl = gpu_context.batch_host(coords, weight, off, *gpu_args(**kw))
+    from parity_util import tolerance_report
+    mism, near = 0, 0
+    for e, (c, w) in enumerate(evs):
+        a, b = off[e], off[e + 1]
+        cfg = O.Config(dc=2.0, rhoc=4.0, dm=3.0, kernel="exp", kernel_par=(1.0, 1.0))
+        ref = O.run(c, w, cfg)
+        rep = tolerance_report(res.rho[a:b], ref.rho, c, w, cfg, res.cluster_index[a:b], ref.cluster_index)
+        assert rep["max_rel_far"] <= 1e-5, (e, rep)
+        mism += rep["label_mismatch"]
+        near += rep["near_dc"]
+    print("label mismatches", mism, "points near dc", near)
+    assert mism <= max(2, off[-1] // 1000)
+
+
+def test_single_event_batch_equals_plain(gpu_context):
+    from cluestering_alpaka3_b200 import synthetic
+    wl = synthetic.blobs_2d_16k(n=10000)
+    p, k, m = gpu_args(dc=wl.dc, rhoc=wl.rhoc, dm=wl.dm)
+    plain = gpu_context.make_clusters_host(wl.coords, wl.weight, p, k, m)
+    res, ncl = gpu_context.batch_host(wl.coords, wl.weight, [0, wl.coords.shape[1]], p, k, m)
+    np.testing.assert_array_equal(res.cluster_index, plain.cluster_index)
+    np.testing.assert_array_equal(res.rho.view(np.uint32), plain.rho.view(np.uint32))
+    assert ncl[0] == plain.info.n_clusters
+
+
+def test_graph_replay_matches_direct(gpu_context):
+    import torch
+    evs, off, coords, weight = make_events(99, 64)
+    n = coords.shape[1]
+    p, k, m = gpu_args(dc=2.0, rhoc=4.0, dm=3.0)
+    direct, ncl = gpu_context.batch_host(coords, weight, off, p, k, m)
+    dc_ = torch.from_numpy(coords).cuda()
+    dw = torch.from_numpy(weight).cuda()
+    outs = {k_: torch.full((n,), -9, dtype=torch.int32, device="cuda") for k_ in ("cluster_index", "is_seed")}
+    ncl_d = torch.zeros(len(off) - 1, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.Stream()
+    g = gpu_context.capture_batch(dc_.data_ptr(), dw.data_ptr(), 2, off, {k_: v.data_ptr() for k_, v in outs.items()},
+                                  p, k, m, ncl_ptr=ncl_d.data_ptr(), stream=stream.cuda_stream)
+    for _ in range(3):
+        outs["cluster_index"].fill_(-9)
+        torch.cuda.synchronize()
+        g.launch(stream.cuda_stream)
+        stream.synchronize()
+        np.testing.assert_array_equal(outs["cluster_index"].cpu().numpy(), direct.cluster_index)
+        np.testing.assert_array_equal(outs["is_seed"].cpu().numpy(), direct.is_seed)
+        np.testing.assert_array_equal(ncl_d.cpu().numpy(), ncl)
+    g.close()
+
+
+def test_events_loop_matches_batch(gpu_context):
+    import torch
+    evs, off, coords, weight = make_events(5, 48)
+    n = coords.shape[1]
+    p, k, m = gpu_args(dc=2.0, rhoc=4.0, dm=3.0, kernel=("exp", (1.0, 1.0)))
+    direct, ncl = gpu_context.batch_host(coords, weight, off, p, k, m)
+    dc_ = torch.from_numpy(coords).cuda()
+    dw = torch.from_numpy(weight).cuda()
+    outs = {"cluster_index": torch.full((n,), -9, dtype=torch.int32, device="cuda"),
+            "rho": torch.zeros(n, dtype=torch.float32, device="cuda")}
+    ms = gpu_context.events_loop(dc_.data_ptr(), dw.data_ptr(), 2, off, {k_: v.data_ptr() for k_, v in outs.items()},
+                                 p, k, m, event_times=True)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(outs["cluster_index"].cpu().numpy(), direct.cluster_index)
+    np.testing.assert_array_equal(outs["rho"].cpu().numpy().view(np.uint32), direct.rho.view(np.uint32))
+    assert ms.shape == (len(off) - 1,) and (ms > 0).all()
