@@ -25,6 +25,7 @@ METRIC_EUCLIDEAN, METRIC_WEIGHTED_EUCLIDEAN, METRIC_PERIODIC_EUCLIDEAN, METRIC_M
     METRIC_CHEBYSHEV, METRIC_WEIGHTED_CHEBYSHEV = range(6)
 TIE_REFERENCE, TIE_RHO_INDEX = 0, 1
 MEM_DEVICE, MEM_HOST = 0, 1
+FLAG_REFERENCE_ORDER, FLAG_SPATIAL_DENSITY = 1, 2
 
 # Every symbol declared in include/clue_b200.h.
 EXPORTED = [
@@ -68,7 +69,7 @@ class _Params(ctypes.Structure):
     _fields_ = [("dc", ctypes.c_float), ("rhoc", ctypes.c_float), ("dm", ctypes.c_float),
                 ("seed_dc", ctypes.c_float), ("points_per_tile", ctypes.c_int32),
                 ("wrapped", ctypes.c_uint8 * MAX_DIM), ("seed_capacity", ctypes.c_int64),
-                ("tiebreak", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("tiebreak", ctypes.c_int32), ("flags", ctypes.c_int32)]
 
 
 class _Outputs(ctypes.Structure):
@@ -217,6 +218,7 @@ class Params:
     wrapped: tuple = ()
     seed_capacity: int = 0       # reference SeedArray policy; < 0 keeps every seed
     tiebreak: int = TIE_REFERENCE
+    flags: int = 0               # FLAG_REFERENCE_ORDER / FLAG_SPATIAL_DENSITY
 
     def struct(self) -> _Params:
         p = _Params()
@@ -229,6 +231,7 @@ class Params:
             p.wrapped[d] = 1 if w else 0
         p.seed_capacity = self.seed_capacity
         p.tiebreak = self.tiebreak
+        p.flags = self.flags
         check(lib.clue_check_params(ctypes.byref(p)))
         return p
 

@@ -140,6 +140,10 @@ clue_status workspace_reserve(Workspace& ws, int ndim, size_t n, size_t ntiles, 
       {(void**)&nw.seed_flag, n * 4},
       {(void**)&nw.seed_total, 16},
       {(void**)&nw.blk, (n / 32 + 1) * 6 * 16},
+      {(void**)&nw.mq_alt, n * 4},
+      {(void**)&nw.mkeys_alt, n * 4},
+      {(void**)&nw.rec_m, n * w * 16},
+      {(void**)&nw.sblk, (n / 1024 + 1) * 6 * 16},
       {(void**)&nw.ord_rho, n * 4},
       {(void**)&nw.ord_nh, n * 4},
       {(void**)&nw.chunk_count, (ntiles + 1) * 4},
@@ -555,6 +559,8 @@ static clue_status prepare(clue_context ctx, const clue_params* params, const cl
   kp.t_dc = threshold_for(params->dc, root);
   kp.t_dm = threshold_for(params->dm, root);
   kp.lb_ok = lower_bounds_ok(metric, ndim);
+  kp.flags = params->flags;
+  kp.ginv = kernel->type == CLUE_KERNEL_GAUSSIAN ? 1.0f / (2.0f * kernel->par[1] * kernel->par[1]) : 0.0f;
   kp.kernel_type = kernel->type;
   for (int k = 0; k < 3; ++k) kp.kpar[k] = kernel->par[k];
   for (int d = 0; d < ndim; ++d) kp.mpar[d] = metric->par[d];
@@ -826,6 +832,8 @@ static clue_status prepare_batch(clue_context ctx, const clue_params* params, co
   kp.t_dc = threshold_for(params->dc, root);
   kp.t_dm = threshold_for(params->dm, root);
   kp.lb_ok = lower_bounds_ok(metric, ndim);
+  kp.flags = params->flags;
+  kp.ginv = kernel->type == CLUE_KERNEL_GAUSSIAN ? 1.0f / (2.0f * kernel->par[1] * kernel->par[1]) : 0.0f;
   kp.kernel_type = kernel->type;
   for (int k = 0; k < 3; ++k) kp.kpar[k] = kernel->par[k];
   for (int d = 0; d < ndim; ++d) kp.mpar[d] = metric->par[d];
@@ -1076,6 +1084,8 @@ extern "C" clue_status clue_events_loop(clue_context ctx, const clue_params* par
     kp.t_dc = threshold_for(params->dc, root);
     kp.t_dm = threshold_for(params->dm, root);
   kp.lb_ok = lower_bounds_ok(metric, ndim);
+  kp.flags = params->flags;
+  kp.ginv = kernel->type == CLUE_KERNEL_GAUSSIAN ? 1.0f / (2.0f * kernel->par[1] * kernel->par[1]) : 0.0f;
     kp.kernel_type = kernel->type;
     for (int k = 0; k < 3; ++k) kp.kpar[k] = kernel->par[k];
     for (int d = 0; d < ndim; ++d) kp.mpar[d] = metric->par[d];

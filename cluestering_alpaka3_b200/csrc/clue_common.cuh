@@ -49,6 +49,8 @@ struct KParams {
   int32_t nperdim0;
   int32_t stride0[kMaxDim];
   int32_t lb_ok;  // metric parameters allow box lower bounds (no negative weights)
+  int32_t flags;  // clue_params.flags
+  float ginv;     // 1 / (2 std^2) of the Gaussian kernel (spatial-order density)
 };
 
 // Bounding box of 32 consecutive tile-sorted records: lo[N], hi[N], max payload.
@@ -313,6 +315,29 @@ struct Metric<N, CLUE_METRIC_WEIGHTED_CHEBYSHEV> {
 };
 
 // ---- convolutional kernels (core/detail/ConvolutionalKernel.hpp:16-65) -------
+#if defined(__CUDACC__)
+// Hardware approximations used by the spatial-order density (whose sums are not bit-exact):
+// sqrt.approx (about 1 ulp) and 2^x of x * log2(e) (ex2.approx, a few ulp); the relative error
+// of a term stays below 1e-6, well inside the 1e-5 tolerance on rho.
+__device__ __forceinline__ float sqrt_approx(float x) {
+  float y;
+  asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float exp_approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x * 1.4426950408889634f));
+  return y;
+}
+// Kernel value of the spatial-order density (distance from the pre-root metric value s).
+// ginv = 1 / (2 std^2) precomputed on the host.
+__device__ __forceinline__ float kernel_value_fast(int32_t type, const float* k, float ginv, float dist) {
+  if (type == CLUE_KERNEL_FLAT) return k[0];
+  if (type == CLUE_KERNEL_EXPONENTIAL) return k[1] * exp_approx(-k[0] * dist);
+  const float u = dist - k[0];
+  return k[2] * exp_approx(-u * u * ginv);
+}
+#endif
 // Value for a pair of distinct points; the self pair (i == j) is 1.
 CLUE_HD float kernel_value(int32_t type, const float* k, float dist) {
   if (type == CLUE_KERNEL_FLAT) return k[0];

@@ -35,7 +35,6 @@ constexpr int kTileThreads = 128;
 constexpr int kChunkWarps = kTileThreads / 32;
 constexpr int kChunk = kChunkPoints;  // home points per CTA in the density / nearest-higher sweeps
 static_assert(kChunkPoints == kTileThreads, "one home point per thread");
-constexpr int kCap = 2048;         // home points signature-sorted per pass
 constexpr int kStageWords = 1024;  // float4 words per staging buffer (16 KiB)
 constexpr int kMaxSeg = 32;        // tile segments per staged piece
 
@@ -168,73 +167,6 @@ __device__ __forceinline__ int wrap_bin(int v, int npd) {
   return b < 0 ? b + npd : b;
 }
 
-// Sub-cell bits per dimension of the spatial part of the home order.
-template <int N>
-struct HomeKey {
-  static constexpr int kSubBits = N <= 2 ? 3 : (N == 3 ? 2 : (N == 4 ? 1 : 0));
-  static constexpr int kBits = N <= 4 ? 2 * N + N * kSubBits : 0;
-  static constexpr int kKeys = 1 << kBits;
-};
-
-// Orders the home points [cb, cb + cnt) of a tile by which neighbour tiles their search box
-// reaches (2 bits per dimension, so the 32 lanes of a warp share one box) and then by Morton
-// order of their sub-cell inside the tile (so a warp's points are close together and whole
-// candidate blocks can be skipped for every lane at once).
-template <int N>
-__device__ void home_sort(const KParams& kp, const EvGrid* __restrict__ g, const float4* __restrict__ rec, int cb,
-                          int cnt, float r, const int* hb, int32_t* s_order, uint16_t* s_key, int32_t* s_hist) {
-  if constexpr (N <= 4) {
-    constexpr int SB = HomeKey<N>::kSubBits;
-    constexpr int K = HomeKey<N>::kKeys;
-    constexpr int S = 1 << SB;
-    for (int e = threadIdx.x; e < K; e += blockDim.x) s_hist[e] = 0;
-    __syncthreads();
-    for (int k = threadIdx.x; k < cnt; k += blockDim.x) {
-      float x[N], pl;
-      load_rec<N>(rec, cb + k, x, pl);
-      int lo[N], hi[N];
-      lane_box<N>(kp, g, x, r, hb, lo, hi);
-      int sig = 0, morton = 0;
-#pragma unroll
-      for (int d = 0; d < N; ++d) {
-        sig |= ((lo[d] < hb[d] ? 1 : 0) | (hi[d] > hb[d] ? 2 : 0)) << (2 * d);
-        if (SB > 0) {
-          const float t0 = g->mn[d] + (float)hb[d] * g->size[d];
-          int sc = g->size[d] > 0.0f ? (int)((x[d] - t0) / g->size[d] * (float)S) : 0;
-          sc = sc < 0 ? 0 : (sc > S - 1 ? S - 1 : sc);
-#pragma unroll
-          for (int bit = 0; bit < SB; ++bit) morton |= ((sc >> bit) & 1) << (bit * N + d);
-        }
-      }
-      const int key = (sig << (N * SB)) | morton;
-      s_key[k] = (uint16_t)key;
-      atomicAdd(&s_hist[key], 1);
-    }
-    __syncthreads();
-    if (threadIdx.x < 32) {
-      int carry = 0;
-      for (int base = 0; base < K; base += 32) {
-        const int e = base + (int)threadIdx.x;
-        const int v = e < K ? s_hist[e] : 0;
-        int inc = v;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const int t = __shfl_up_sync(0xffffffffu, inc, o);
-          if ((int)threadIdx.x >= o) inc += t;
-        }
-        if (e < K) s_hist[e] = carry + inc - v;
-        carry += __shfl_sync(0xffffffffu, inc, 31);
-      }
-    }
-    __syncthreads();
-    for (int k = threadIdx.x; k < cnt; k += blockDim.x) s_order[atomicAdd(&s_hist[s_key[k]], 1)] = k;
-    __syncthreads();
-  } else {
-    for (int k = threadIdx.x; k < cnt; k += blockDim.x) s_order[k] = k;
-    __syncthreads();
-  }
-}
-
 // Bounding box (and largest payload) of every 32 consecutive tile-sorted records.
 template <int N>
 __global__ void __launch_bounds__(256) k_block_bbox(const float4* __restrict__ rec, int n, float4* __restrict__ blk) {
@@ -274,6 +206,171 @@ __global__ void __launch_bounds__(256) k_block_bbox(const float4* __restrict__ r
       for (int k = 0; k < BW; ++k)
         if (k == lane) v = make_float4(out[4 * k], out[4 * k + 1], out[4 * k + 2], out[4 * k + 3]);
       blk[(size_t)b * BW + lane] = v;
+    }
+  }
+}
+
+// Bounding boxes of super-blocks (32 consecutive blocks = 1024 records) from the block boxes.
+template <int N>
+__global__ void __launch_bounds__(256) k_superblock_bbox(const float4* __restrict__ blk, int n,
+                                                         float4* __restrict__ sblk) {
+  constexpr int BW = Blk<N>::kWords;
+  const int lane = threadIdx.x & 31;
+  const int nblk = (n + 31) >> 5;
+  const int nsb = (nblk + 31) >> 5;
+  const int wstride = (gridDim.x * blockDim.x) >> 5;
+  for (int sb = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; sb < nsb; sb += wstride) {
+    const int b = min((sb << 5) + lane, nblk - 1);
+    float v[4 * BW];
+#pragma unroll
+    for (int k = 0; k < BW; ++k) {
+      const float4 t4 = __ldg(blk + (size_t)b * BW + k);
+      v[4 * k] = t4.x;
+      v[4 * k + 1] = t4.y;
+      v[4 * k + 2] = t4.z;
+      v[4 * k + 3] = t4.w;
+    }
+#pragma unroll
+    for (int d = 0; d < N; ++d) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        v[d] = fminf(v[d], __shfl_xor_sync(0xffffffffu, v[d], o));
+        v[N + d] = fmaxf(v[N + d], __shfl_xor_sync(0xffffffffu, v[N + d], o));
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[2 * N] = fmaxf(v[2 * N], __shfl_xor_sync(0xffffffffu, v[2 * N], o));
+    if (lane < BW) {
+      float4 out;
+#pragma unroll
+      for (int k = 0; k < BW; ++k)
+        if (k == lane) out = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+      sblk[(size_t)sb * BW + lane] = out;
+    }
+  }
+}
+
+template <int N>
+__device__ __forceinline__ void load_box(const float4* __restrict__ a, int i, float* bb) {
+  constexpr int BW = Blk<N>::kWords;
+#pragma unroll
+  for (int k = 0; k < BW; ++k) {
+    const float4 t4 = __ldg(a + (size_t)i * BW + k);
+    bb[4 * k] = t4.x;
+    bb[4 * k + 1] = t4.y;
+    bb[4 * k + 2] = t4.z;
+    bb[4 * k + 3] = t4.w;
+  }
+}
+
+// A block of up to 32 consecutive records loaded cooperatively: lane k holds record p0 + k;
+// bcast_rec() hands record j to every lane through register shuffles.
+template <int N>
+__device__ __forceinline__ void warp_load_block(const float4* __restrict__ rec, int p0, int cnt, float* mine) {
+  constexpr int W = Rec<N>::kWords;
+  const int lane = threadIdx.x & 31;
+  const int p = p0 + (lane < cnt ? lane : 0);
+#pragma unroll
+  for (int k = 0; k < W; ++k) {
+    const float4 v = __ldg(rec + (size_t)p * W + k);
+    mine[4 * k] = v.x;
+    mine[4 * k + 1] = v.y;
+    mine[4 * k + 2] = v.z;
+    mine[4 * k + 3] = v.w;
+  }
+}
+template <int N>
+__device__ __forceinline__ void bcast_rec(const float* mine, int j, float* c, float& payload) {
+#pragma unroll
+  for (int d = 0; d < N; ++d) c[d] = __shfl_sync(0xffffffffu, mine[d], j);
+  payload = __shfl_sync(0xffffffffu, mine[Rec<N>::kPayload], j);
+}
+
+// Spatial sweep of one warp over the Morton-ordered records of its search-box tiles (any
+// order: the own tile first, then the union of the warp's boxes lexicographically).  Super-blocks
+// and blocks whose bounding box lies beyond bound() for every lane, or whose largest payload is
+// below pmin for every lane, are skipped; vis(p0, p1, inbox, lexpos) gets the rest.  lexpos is
+// the tile's position in this lane's reference iteration order (lexicographic over its box).
+template <int N, class M, class Bound, class Visit>
+__device__ __forceinline__ void spatial_sweep(const KParams& kp, const EvGrid* __restrict__ g,
+                                              const int32_t* __restrict__ off, const int* hb, const int* lo,
+                                              const int* hi, bool valid, const float* x,
+                                              const float4* __restrict__ blk, const float4* __restrict__ sblk,
+                                              float pmin, Bound&& bound, Visit&& vis) {
+  constexpr int BW = Blk<N>::kWords;
+  int wl[N], wh[N];
+#pragma unroll
+  for (int d = 0; d < N; ++d) {
+    wl[d] = warp_min_i(valid ? lo[d] : INT_MAX);
+    wh[d] = warp_max_i(valid ? hi[d] : INT_MIN);
+  }
+  int64_t ext[N];
+  {
+    int64_t m = 1;
+#pragma unroll
+    for (int d = N - 1; d >= 0; --d) {
+      ext[d] = m;
+      m *= (int64_t)(hi[d] - lo[d] + 1);
+    }
+  }
+  int v[N];
+  int phase = 0;  // 0: own tile, 1: first union tile pending, 2: iterating the union
+  while (true) {
+    if (phase == 0) {
+#pragma unroll
+      for (int d = 0; d < N; ++d) v[d] = hb[d];
+      phase = 1;
+    } else {
+      if (phase == 1) {
+#pragma unroll
+        for (int d = 0; d < N; ++d) v[d] = wl[d];
+        phase = 2;
+      } else {
+        int d = N - 1;
+        for (; d >= 0; --d) {
+          if (v[d] < wh[d]) {
+            ++v[d];
+            break;
+          }
+          v[d] = wl[d];
+        }
+        if (d < 0) break;
+      }
+      bool is_home = true;
+#pragma unroll
+      for (int d = 0; d < N; ++d) is_home = is_home && v[d] == hb[d];
+      if (is_home) continue;
+    }
+    bool inbox = valid;
+    int u = g->tile_base;
+    int64_t lexpos = 0;
+#pragma unroll
+    for (int d = 0; d < N; ++d) {
+      inbox = inbox && v[d] >= lo[d] && v[d] <= hi[d];
+      u += g->stride[d] * wrap_bin(v[d], g->nperdim);
+      lexpos += (int64_t)(v[d] - lo[d]) * ext[d];
+    }
+    if (!__any_sync(0xffffffffu, inbox)) continue;
+    const int pb = off[u], pe = off[u + 1];
+    if (pb >= pe) continue;
+    for (int sbk = pb >> 10; sbk <= (pe - 1) >> 10; ++sbk) {
+      if (kp.lb_ok) {
+        float bb[4 * BW];
+        load_box<N>(sblk, sbk, bb);
+        const bool need = inbox && M::lower(x, bb, bb + N, kp.mpar) <= bound() && bb[2 * N] >= pmin;
+        if (!__any_sync(0xffffffffu, need)) continue;
+      }
+      const int sp0 = max(pb, sbk << 10), sp1 = min(pe, (sbk + 1) << 10);
+      for (int b = sp0 >> 5; b <= (sp1 - 1) >> 5; ++b) {
+        bool need = inbox;
+        if (kp.lb_ok) {
+          float bb[4 * BW];
+          load_box<N>(blk, b, bb);
+          need = need && M::lower(x, bb, bb + N, kp.mpar) <= bound() && bb[2 * N] >= pmin;
+        }
+        if (!__any_sync(0xffffffffu, need)) continue;
+        vis(max(sp0, b << 5), min(sp1, (b + 1) << 5), need, lexpos);
+      }
     }
   }
 }
@@ -477,19 +574,87 @@ __global__ void __launch_bounds__(256) k_gather(InPtrs in, int n, const int32_t*
   }
 }
 
+// Morton bits per dimension of the fine order inside a tile (16 bits per key in total, so the
+// order -- and the spatial-order sums -- depend only on the tile's own points).
+template <int N>
+struct MortonBits {
+  static constexpr int kPerDim = N == 1 ? 16 : (16 / N > 0 ? 16 / N : 1);
+  static constexpr int kBits = kPerDim * N;
+};
+
+// Morton key of every tile-sorted record inside its tile (tile keys are read from tile_keys).
+template <int N>
+__global__ void __launch_bounds__(256) k_morton_keys(const KParams kp, Events ev, const float4* __restrict__ rec,
+                                                     const uint32_t* __restrict__ tile_keys,
+                                                     uint32_t* __restrict__ keys) {
+  constexpr int bpd = MortonBits<N>::kPerDim;
+  const float scale = (float)(1u << bpd);
+  const int stride = gridDim.x * blockDim.x;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < kp.n; q += stride) {
+    const uint32_t t = tile_keys[q];
+    const EvGrid* g = ev.eg + find_event(ev.tile, kp.n_events, (int)t);
+    int hb[N];
+    home_bins<N>(g, (int)t, hb);
+    float x[N], pl;
+    load_rec<N>(rec, q, x, pl);
+    uint32_t m = 0;
+#pragma unroll
+    for (int d = 0; d < N; ++d) {
+      const float t0 = g->mn[d] + (float)hb[d] * g->size[d];
+      int c = g->size[d] > 0.0f ? (int)((x[d] - t0) / g->size[d] * scale) : 0;
+      c = c < 0 ? 0 : (c > (1 << bpd) - 1 ? (1 << bpd) - 1 : c);
+      for (int bit = 0; bit < bpd; ++bit) m |= (uint32_t)((c >> bit) & 1) << (bit * N + d);
+    }
+    keys[q] = m;
+  }
+}
+
+// Tile key of every record in the Morton-sorted order (second, stable sort by tile).
+__global__ void __launch_bounds__(256) k_tile_of(const uint32_t* __restrict__ tile_keys,
+                                                 const int32_t* __restrict__ mq, int n, uint32_t* __restrict__ out) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) out[p] = tile_keys[mq[p]];
+}
+
+// Inverse permutation: minv[mq[p]] = p.
+__global__ void __launch_bounds__(256) k_invert(const int32_t* __restrict__ mq, int n, int32_t* __restrict__ minv) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) minv[mq[p]] = p;
+}
+
+template <int N>
+__global__ void __launch_bounds__(256) k_gather_morton(const float4* __restrict__ rec_r, int n,
+                                                       const int32_t* __restrict__ mq, float4* __restrict__ rec_m) {
+  constexpr int W = Rec<N>::kWords;
+  const int stride = gridDim.x * blockDim.x;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
+    const int q = mq[p];
+#pragma unroll
+    for (int k = 0; k < W; ++k) rec_m[(size_t)p * W + k] = __ldg(rec_r + (size_t)q * W + k);
+  }
+}
+
 // ---- work orders and chunks --------------------------------------------------
-// Every tile's points are ordered twice by search-box signature (radius dc for the
-// density, dm for the nearest higher) and cut into chunks of kChunk home points; one CTA
-// processes one chunk, so a heavy tile is spread over many CTAs.
+// Home points of every tile are taken in the fine Morton order of the tile (so 32 consecutive
+// points are close together at the data's own density scale) and stably partitioned by
+// search-box signature -- which neighbour tiles the box of radius dc (density) or dm (nearest
+// higher) reaches, 2 bits per dimension -- so the 32 lanes of a warp share one box.  The orders
+// are cut into chunks of kChunk home points; one CTA processes one chunk, so a heavy tile is
+// spread over many CTAs.  One CTA per tile; warp w partitions the w-th quarter of the tile and
+// the quarters are concatenated per key, which keeps the partition stable.
 template <int N>
 __global__ void __launch_bounds__(kTileThreads) k_order(const KParams kp, Events ev,
                                                         const int32_t* __restrict__ off,
                                                         const float4* __restrict__ rec_w,
+                                                        const int32_t* __restrict__ mq,
                                                         int32_t* __restrict__ ord_rho, int32_t* __restrict__ ord_nh,
                                                         uint32_t* __restrict__ chunk_count) {
-  __shared__ int32_t s_order[kCap];
-  __shared__ uint16_t s_key[kCap];
-  __shared__ int32_t s_hist[N <= 4 ? HomeKey<N>::kKeys : 1];
+  constexpr int K = N <= 4 ? (1 << (2 * N)) : 1;
+  __shared__ uint32_t s_cnt[kChunkWarps][2][K];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t lt = (1u << lane) - 1u;
+  int32_t* ord[2] = {ord_rho, ord_nh};
+  const float rad[2] = {kp.dc, kp.dm};
   for (int t = blockIdx.x; t < kp.ntiles; t += gridDim.x) {
     const int beg = off[t], end = off[t + 1];
     if (threadIdx.x == 0) chunk_count[t] = (uint32_t)((end - beg + kChunk - 1) / kChunk);
@@ -497,15 +662,55 @@ __global__ void __launch_bounds__(kTileThreads) k_order(const KParams kp, Events
     const EvGrid* g = ev.eg + find_event(ev.tile, kp.n_events, t);
     int hb[N];
     home_bins<N>(g, t, hb);
-    for (int cb = beg; cb < end; cb += kCap) {
-      const int cnt = min(kCap, end - cb);
-      home_sort<N>(kp, g, rec_w, cb, cnt, kp.dc, hb, s_order, s_key, s_hist);
-      for (int k = threadIdx.x; k < cnt; k += blockDim.x) ord_rho[cb + k] = cb + s_order[k];
-      __syncthreads();
-      home_sort<N>(kp, g, rec_w, cb, cnt, kp.dm, hb, s_order, s_key, s_hist);
-      for (int k = threadIdx.x; k < cnt; k += blockDim.x) ord_nh[cb + k] = cb + s_order[k];
-      __syncthreads();
+    const int quarter = ((end - beg + kChunkWarps - 1) / kChunkWarps + 31) & ~31;
+    const int wb = min(end, beg + warp * quarter), we = min(end, wb + quarter);
+    for (int e = threadIdx.x; e < kChunkWarps * 2 * K; e += blockDim.x) (&s_cnt[0][0][0])[e] = 0;
+    __syncthreads();
+    for (int pass = 0; pass < 2; ++pass) {
+      for (int base = wb; base < we; base += 32) {
+        const int p = base + lane;
+        const bool valid = p < we;
+        const int q = valid ? mq[p] : mq[beg];
+        float x[N], pl;
+        load_rec<N>(rec_w, q, x, pl);
+        int key[2];
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+          key[r] = 0;
+          if (K > 1) {
+            int lo[N], hi[N];
+            lane_box<N>(kp, g, x, rad[r], hb, lo, hi);
+#pragma unroll
+            for (int d = 0; d < N; ++d) key[r] |= ((lo[d] < hb[d] ? 1 : 0) | (hi[d] > hb[d] ? 2 : 0)) << (2 * d);
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+          const uint32_t peers = __match_any_sync(0xffffffffu, valid ? key[r] : -1);
+          const bool leader = valid && (peers & lt) == 0;
+          if (pass == 1 && valid) ord[r][beg + s_cnt[warp][r][key[r]] + __popc(peers & lt)] = q;
+          __syncwarp();
+          if (leader) s_cnt[warp][r][key[r]] += __popc(peers);
+          __syncwarp();
+        }
+      }
+      if (pass == 0) {
+        __syncthreads();
+        // first slot of (warp, key): keys in order, warps in order inside a key
+        if (threadIdx.x < 2) {
+          const int r = threadIdx.x;
+          uint32_t run = 0;
+          for (int k = 0; k < K; ++k)
+            for (int w = 0; w < kChunkWarps; ++w) {
+              const uint32_t c = s_cnt[w][r][k];
+              s_cnt[w][r][k] = run;
+              run += c;
+            }
+        }
+        __syncthreads();
+      }
     }
+    __syncthreads();
   }
 }
 
@@ -785,19 +990,24 @@ __global__ void __launch_bounds__(kTileThreads) k_density(const KParams kp, Even
 }
 
 // ---- stage 3: nearest higher -------------------------------------------------
-// j is higher than i iff rho_j > rho_i or (rho_j == rho_i, rho_j > 0, j > i) with
-// original indices; the nearest higher is the first candidate, in the reference's
-// order, with the strictly smallest distance <= dm (TIE == CLUE_TIE_REFERENCE), or the
-// candidate with the smallest (distance, -rho, index) (TIE == CLUE_TIE_RHO_INDEX).
+// j is higher than i iff rho_j > rho_i or (rho_j == rho_i, rho_j > 0, j > i) with original
+// indices.  The reference keeps the first candidate of its iteration order (search-box tiles
+// lexicographically, ascending index inside a tile) with the strictly smallest distance <= dm,
+// i.e. the minimum of (distance, iteration rank); that minimum does not depend on the order in
+// which candidates are visited, so the search here is spatial: every tile's records are also
+// kept in Morton order of a fine grid inside the tile, the own tile is searched first, and a
+// 32-record block is skipped when its bounding box is farther than every lane's current best
+// (or than dm) or holds no density reaching the lane's.  TIE == CLUE_TIE_RHO_INDEX resolves equal
+// distances by higher rho, then lower index.
+
 template <int N, int MT, int TIE>
 __global__ void __launch_bounds__(kTileThreads) k_nearest_higher(
     const KParams kp, Events ev, const int32_t* __restrict__ off, const int32_t* __restrict__ ord,
     const int32_t* __restrict__ chunk_tile, const uint32_t* __restrict__ chunk_off,
-    const uint32_t* __restrict__ chunk_total, const float4* __restrict__ rec_r, const float4* __restrict__ blk,
+    const uint32_t* __restrict__ chunk_total, const float4* __restrict__ rec_r, const float4* __restrict__ rec_m,
+    const int32_t* __restrict__ mq, const float4* __restrict__ blk, const float4* __restrict__ sblk,
     const int32_t* __restrict__ perm, int32_t* __restrict__ nh_s, float* __restrict__ delta_s, DevStatus* st) {
   using M = Metric<N, MT>;
-  constexpr int W = Rec<N>::kWords;
-  __shared__ StageSmem<N> sm;
   ChunkHome h;
   if (!chunk_home(kp, ev, off, ord, chunk_tile, chunk_off, chunk_total, h)) return;
   const int pos = h.pos;
@@ -808,23 +1018,25 @@ __global__ void __launch_bounds__(kTileThreads) k_nearest_higher(
   int hb[N], lo[N], hi[N];
   home_bins<N>(h.g, h.t, hb);
   lane_box<N>(kp, h.g, x, kp.dm, hb, lo, hi);
+  if (!__any_sync(0xffffffffu, valid)) return;
   const float tdm = kp.t_dm;
+  const float slack = M::kRoot ? 1.0f + 1.0f / 524288.0f : 1.0f;  // s range of one rounded distance
   float delta = FLT_MAX, s_best = INFINITY, rho_best = 0.0f;
   int nh = -1, orig_best = INT_MAX;
-  const bool ok = staged_sweep<N>(h.g, off, rec_r, sm, lo, hi, valid, [&](bool inbox, const float4* sb, int qb, int n_) {
-    if (!__any_sync(0xffffffffu, inbox)) return;
-    const bool strict = TIE == CLUE_TIE_REFERENCE;
-    scan_blocks<N, M>(kp, blk, x, inbox, fminf(tdm, s_best), strict && s_best <= tdm, rho_i, qb, n_,
-                      [&](int j0, int j1) {
-#pragma unroll 4
-    for (int j = j0; j < j1; ++j) {
+  uint64_t rank_best = ~0ull;
+  spatial_sweep<N, M>(kp, h.g, off, hb, lo, hi, valid, x, blk, sblk, rho_i,
+                      [&]() { return s_best < INFINITY ? fminf(tdm, s_best * slack) : tdm; },
+                      [&](int p0, int p1, bool need, int64_t lexpos) {
+    const float bound = s_best < INFINITY ? fminf(tdm, s_best * slack) : tdm;
+    float mine[4 * Rec<N>::kWords];
+    warp_load_block<N>(rec_m, p0, p1 - p0, mine);
+    for (int j = 0; j < p1 - p0; ++j) {
+      const int p = p0 + j;
       float c[N], rho_j;
-      unpack_rec<N>(sb + j * W, c, rho_j);
+      bcast_rec<N>(mine, j, c, rho_j);
       const float s = M::partial(x, c, kp.mpar);
-      bool cand = inbox && s <= tdm && rho_j >= rho_i;
-      if (TIE == CLUE_TIE_REFERENCE) cand = cand && s < s_best;
-      if (cand) {
-        const int q = qb + j;
+      if (need && s <= tdm && s <= bound && rho_j >= rho_i) {
+        const int q = __ldg(mq + p);
         int orig_j = -1;
         bool higher = rho_j > rho_i;
         if (!higher && rho_j > 0.0f) {
@@ -833,30 +1045,29 @@ __global__ void __launch_bounds__(kTileThreads) k_nearest_higher(
         }
         if (higher) {
           const float dist = M::finish(s);
-          if (dist < delta) {
+          const uint64_t rank = ((uint64_t)lexpos << 32) | (uint32_t)q;
+          bool better;
+          if (TIE == CLUE_TIE_REFERENCE) {
+            better = dist < delta || (dist == delta && rank < rank_best);
+          } else if (dist == delta && nh >= 0) {
+            if (orig_j < 0) orig_j = __ldg(perm + q);
+            if (orig_best < 0) orig_best = __ldg(perm + nh);
+            better = rho_j > rho_best || (rho_j == rho_best && orig_j < orig_best);
+          } else {
+            better = dist < delta;
+          }
+          if (better) {
             delta = dist;
             s_best = s;
             nh = q;
+            rank_best = rank;
             rho_best = rho_j;
             orig_best = orig_j;
-          } else if (TIE == CLUE_TIE_RHO_INDEX && dist == delta) {
-            if (orig_j < 0) orig_j = __ldg(perm + q);
-            if (orig_best < 0) orig_best = __ldg(perm + nh);
-            if (rho_j > rho_best || (rho_j == rho_best && orig_j < orig_best)) {
-              nh = q;
-              rho_best = rho_j;
-              orig_best = orig_j;
-            }
           }
         }
       }
     }
-    });
   });
-  if (!ok) {
-    if (threadIdx.x == 0) atomicOr(&st->stage_timeout, 1u);
-    return;
-  }
   if (valid) {
     nh_s[pos] = nh;
     delta_s[pos] = delta;
@@ -866,6 +1077,48 @@ __global__ void __launch_bounds__(kTileThreads) k_nearest_higher(
     atomicAdd(&st->seed_candidates, (uint32_t)__popc(none));
     atomicAdd(const_cast<uint32_t*>(&h.g->seed_candidates), (uint32_t)__popc(none));
   }
+}
+
+// Local density over the Morton-ordered records (any order, kernels other than flat): the
+// same candidate set as the reference (search-box tiles, d <= dc, self term 1), summed in
+// spatial order.  Blocks farther than dc from every lane are skipped.
+template <int N, int MT>
+__global__ void __launch_bounds__(kTileThreads) k_density_spatial(
+    const KParams kp, Events ev, const int32_t* __restrict__ off, const int32_t* __restrict__ ord,
+    const int32_t* __restrict__ chunk_tile, const uint32_t* __restrict__ chunk_off,
+    const uint32_t* __restrict__ chunk_total, const float4* __restrict__ rec_w, const float4* __restrict__ rec_m,
+    const int32_t* __restrict__ mq, const float4* __restrict__ blk, const float4* __restrict__ sblk,
+    float4* __restrict__ rec_r, const int32_t* __restrict__ minv) {
+  using M = Metric<N, MT>;
+  ChunkHome h;
+  if (!chunk_home(kp, ev, off, ord, chunk_tile, chunk_off, chunk_total, h)) return;
+  const int pos = h.pos;
+  const bool valid = h.valid;
+  float x[N], wi;
+  load_rec<N>(rec_w, pos, x, wi);
+  const int p_home = minv[pos];
+  int hb[N], lo[N], hi[N];
+  home_bins<N>(h.g, h.t, hb);
+  lane_box<N>(kp, h.g, x, kp.dc, hb, lo, hi);
+  if (!__any_sync(0xffffffffu, valid)) return;
+  const float tdc = kp.t_dc;
+  float rho = 0.0f;
+  spatial_sweep<N, M>(kp, h.g, off, hb, lo, hi, valid, x, blk, sblk, -INFINITY, [&]() { return tdc; },
+                      [&](int p0, int p1, bool need, int64_t) {
+    float mine[4 * Rec<N>::kWords];
+    warp_load_block<N>(rec_m, p0, p1 - p0, mine);
+    for (int j = 0; j < p1 - p0; ++j) {
+      float c[N], wj;
+      bcast_rec<N>(mine, j, c, wj);
+      const float s = M::partial(x, c, kp.mpar);
+      if (need && s <= tdc) {
+        const float dist = M::kRoot ? sqrt_approx(s) : s;
+        const float kv = (p0 + j == p_home) ? 1.0f : kernel_value_fast(kp.kernel_type, kp.kpar, kp.ginv, dist);
+        rho = fadd(rho, fmul(kv, wj));
+      }
+    }
+  });
+  if (valid) store_rec<N>(rec_r, pos, x, rho);
 }
 
 // ---- stage 4: seeds (KernelFindClusters) ---------------------------------------
@@ -1004,11 +1257,17 @@ void launch_nh(const KParams& kp, Workspace& ws, cudaStream_t s) {
   if (kp.tiebreak == CLUE_TIE_RHO_INDEX)
     k_nearest_higher<N, MT, CLUE_TIE_RHO_INDEX><<<chunk_grid(kp), kTileThreads, 0, s>>>(
         kp, events_of(ws), ws.offsets, ws.ord_nh, ws.chunk_tile, ws.chunk_count, ws.chunk_total, ws.rec_r,
-        ws.blk, ws.perm, ws.nh_s, ws.delta_s, ws.status);
+        ws.rec_m, ws.mq, ws.blk, ws.sblk, ws.perm, ws.nh_s, ws.delta_s, ws.status);
   else
     k_nearest_higher<N, MT, CLUE_TIE_REFERENCE><<<chunk_grid(kp), kTileThreads, 0, s>>>(
         kp, events_of(ws), ws.offsets, ws.ord_nh, ws.chunk_tile, ws.chunk_count, ws.chunk_total, ws.rec_r,
-        ws.blk, ws.perm, ws.nh_s, ws.delta_s, ws.status);
+        ws.rec_m, ws.mq, ws.blk, ws.sblk, ws.perm, ws.nh_s, ws.delta_s, ws.status);
+}
+template <int N, int MT>
+void launch_density_spatial(const KParams& kp, Workspace& ws, cudaStream_t s) {
+  k_density_spatial<N, MT><<<chunk_grid(kp), kTileThreads, 0, s>>>(
+      kp, events_of(ws), ws.offsets, ws.ord_rho, ws.chunk_tile, ws.chunk_count, ws.chunk_total, ws.rec_w,
+      ws.rec_m, ws.mq, ws.blk, ws.sblk, ws.rec_r, ws.minv);
 }
 template <int N, int MT>
 void launch_seeds(const KParams& kp, Workspace& ws, cudaStream_t s) {
@@ -1060,17 +1319,55 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
   ws.sorted_keys = ws.keys[cur];
   offsets_from_sorted(ws.sorted_keys, n, kp.ntiles, ws.offsets, s);
   k_gather<N><<<grid_for(n, 256), 256, 0, s>>>(in, n, ws.perm, ws.rec_w);
-  k_order<N><<<kp.ntiles, kTileThreads, 0, s>>>(kp, ev, ws.offsets, ws.rec_w, ws.ord_rho, ws.ord_nh,
+  {
+    // fine Morton order inside every tile: a stable sort by Morton key, then a stable sort by
+    // tile; mq[p] = tile-sorted position of the p-th record in (tile, Morton) order
+    uint32_t* mkeys[2] = {ws.keys[cur ^ 1], ws.mkeys_alt};
+    int32_t* mvals[2] = {ws.vals[cur ^ 1], ws.mq_alt};
+    k_morton_keys<N><<<grid_for(n, 256), 256, 0, s>>>(kp, ev, ws.rec_w, ws.sorted_keys, mkeys[0]);
+    int mc = radix_sort_pairs(mkeys, mvals, true, n, MortonBits<N>::kBits, ws.hist, ws.scan_scratch, s);
+    if (mc != 0) {
+      std::swap(mkeys[0], mkeys[1]);
+      std::swap(mvals[0], mvals[1]);
+    }
+    k_tile_of<<<grid_for(n, 256), 256, 0, s>>>(ws.sorted_keys, mvals[0], n, mkeys[0]);
+    mc = radix_sort_pairs(mkeys, mvals, false, n, bits, ws.hist, ws.scan_scratch, s);
+    ws.mq = mvals[mc];
+    ws.minv = mvals[mc ^ 1];
+    k_invert<<<grid_for(n, 256), 256, 0, s>>>(ws.mq, n, ws.minv);
+  }
+  k_order<N><<<kp.ntiles, kTileThreads, 0, s>>>(kp, ev, ws.offsets, ws.rec_w, ws.mq, ws.ord_rho, ws.ord_nh,
                                                 ws.chunk_count);
   exclusive_scan(ws.chunk_count, ws.chunk_count, (size_t)kp.ntiles, ws.scan_scratch, ws.chunk_total, s);
   k_chunk_map<<<grid_for(kp.ntiles, 256), 256, 0, s>>>(kp.ntiles, ws.offsets, ws.chunk_count, ws.chunk_tile);
 
-  k_block_bbox<N><<<grid_for(((n + 31) >> 5) * 32, 256), 256, 0, s>>>(ws.rec_w, n, ws.blk);
+  // density order: the reference's candidate order for the flat kernel (bit-exact sums), spatial
+  // order for the exponential and Gaussian kernels (whose device expf already differs from the
+  // host's by an ulp) unless the caller asks for the reference order
+  const bool spatial_density = (kp.flags & CLUE_FLAG_REFERENCE_ORDER) == 0 &&
+                               (kp.kernel_type != CLUE_KERNEL_FLAT || (kp.flags & CLUE_FLAG_SPATIAL_DENSITY) != 0);
+  const int nblk_threads = ((n + 31) >> 5) * 32;
+  const int nsb_threads = ((((n + 31) >> 5) + 31) >> 5) * 32;
+  if (spatial_density) {
+    k_gather_morton<N><<<grid_for(n, 256), 256, 0, s>>>(ws.rec_w, n, ws.mq, ws.rec_m);
+    k_block_bbox<N><<<grid_for(nblk_threads, 256), 256, 0, s>>>(ws.rec_m, n, ws.blk);
+    k_superblock_bbox<N><<<grid_for(nsb_threads, 256), 256, 0, s>>>(ws.blk, n, ws.sblk);
+  } else {
+    k_block_bbox<N><<<grid_for(nblk_threads, 256), 256, 0, s>>>(ws.rec_w, n, ws.blk);
+  }
 
   stage_mark(ws, 1, s);
-  CLUE_METRIC_SWITCH(a.metric, launch_density, kp, ws, s);
+  if (spatial_density) {
+    CLUE_METRIC_SWITCH(a.metric, launch_density_spatial, kp, ws, s);
+  } else {
+    CLUE_METRIC_SWITCH(a.metric, launch_density, kp, ws, s);
+  }
   stage_mark(ws, 2, s);
-  k_block_bbox<N><<<grid_for(((n + 31) >> 5) * 32, 256), 256, 0, s>>>(ws.rec_r, n, ws.blk);
+  // Morton-ordered copy of the records with their densities and its block / super-block boxes
+  // with the largest rho, for the nearest-higher search
+  k_gather_morton<N><<<grid_for(n, 256), 256, 0, s>>>(ws.rec_r, n, ws.mq, ws.rec_m);
+  k_block_bbox<N><<<grid_for(nblk_threads, 256), 256, 0, s>>>(ws.rec_m, n, ws.blk);
+  k_superblock_bbox<N><<<grid_for(nsb_threads, 256), 256, 0, s>>>(ws.blk, n, ws.sblk);
   CLUE_METRIC_SWITCH(a.metric, launch_nh, kp, ws, s);
   stage_mark(ws, 3, s);
   CLUE_METRIC_SWITCH(a.metric, launch_seeds, kp, ws, s);
@@ -1082,10 +1379,12 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
   k_event_info<<<grid_for(kp.n_events, 256), 256, 0, s>>>(kp, ws.ev, ws.ev_pt, ws.seed_flag, ws.seed_total,
                                                          a.ev_n_seeds, a.ev_n_clusters, ws.status);
   stage_mark(ws, 4, s);
-  // init, bbox, grid, bin, sort, offsets, gather, order, scan, chunk map, 2 block boxes, density, nh,
-  // seeds, scan, jumps, finalize, event info
-  ws.launches += 4 + radix_sort_launches(bits) + 2 + 1 + kScanLaunches + 1 + 2 + 3 + kScanLaunches +
-                 kJumpLaunches + 1 + 1;
+  // init, bbox, grid, bin, sort, offsets, gather, Morton keys + 2 sorts + tile keys + inverse, order,
+  // scan, chunk map, density boxes, density, Morton gather + boxes, nh, seeds, scan, jumps,
+  // finalize, event info
+  ws.launches += 4 + radix_sort_launches(bits) + 2 + 1 + radix_sort_launches(MortonBits<N>::kBits) + 1 +
+                 radix_sort_launches(bits) + 1 + 1 + kScanLaunches + 1 +
+                 (spatial_density ? 3 : 1) + 1 + 3 + 1 + 2 + kScanLaunches + kJumpLaunches + 1 + 1;
   CLUE_CUDA_TRY(cudaGetLastError());
   return CLUE_OK;
 }

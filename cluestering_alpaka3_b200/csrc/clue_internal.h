@@ -111,6 +111,12 @@ struct Workspace {
   uint32_t* seed_flag = nullptr;  // original order, then exclusive-scanned to ranks
   uint32_t* seed_total = nullptr;
   float4* blk = nullptr;          // bounding boxes of 32-record blocks of the sorted records
+  int32_t* mq_alt = nullptr;      // second value buffer of the Morton sort
+  uint32_t* mkeys_alt = nullptr;  // second key buffer of the Morton sort
+  int32_t* minv = nullptr;        // tile-sorted position -> Morton position (alias after the sort)
+  float4* rec_m = nullptr;        // records in Morton order inside every tile
+  float4* sblk = nullptr;         // bounding boxes of 1024-record super-blocks
+  int32_t* mq = nullptr;          // Morton position -> tile-sorted position (alias after the sort)
   int32_t* ord_rho = nullptr;     // per-tile home order for the density sweep
   int32_t* ord_nh = nullptr;      // per-tile home order for the nearest-higher sweep
   uint32_t* chunk_count = nullptr;  // [ntiles] chunks per tile, then exclusive-scanned

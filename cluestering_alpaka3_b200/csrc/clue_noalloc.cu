@@ -92,6 +92,10 @@ bool carve(Workspace& ws, void* base, int ndim, size_t n, size_t ntiles) {
       {(void**)&ws.seed_flag, n * 4},
       {(void**)&ws.seed_total, 16},
       {(void**)&ws.blk, (n / 32 + 1) * 6 * 16},
+      {(void**)&ws.mq_alt, n * 4},
+      {(void**)&ws.mkeys_alt, n * 4},
+      {(void**)&ws.rec_m, n * w * 16},
+      {(void**)&ws.sblk, (n / 1024 + 1) * 6 * 16},
       {(void**)&ws.ord_rho, n * 4},
       {(void**)&ws.ord_nh, n * 4},
       {(void**)&ws.chunk_count, (ntiles + 1) * 4},
@@ -188,6 +192,8 @@ extern "C" clue_status clue_make_clusters_noalloc(const clue_params* params, con
   kp.t_dc = threshold_for(params->dc, root);
   kp.t_dm = threshold_for(params->dm, root);
   kp.lb_ok = lower_bounds_ok(metric, ndim);
+  kp.flags = params->flags;
+  kp.ginv = kernel->type == CLUE_KERNEL_GAUSSIAN ? 1.0f / (2.0f * kernel->par[1] * kernel->par[1]) : 0.0f;
   kp.kernel_type = kernel->type;
   for (int k = 0; k < 3; ++k) kp.kpar[k] = kernel->par[k];
   for (int d = 0; d < ndim; ++d) kp.mpar[d] = metric->par[d];

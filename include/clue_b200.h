@@ -96,8 +96,16 @@ typedef struct clue_params {
    * label -1, as in include/CLUEstering/data_structures/internal/SeedArray.hpp:33-41. */
   int64_t seed_capacity;
   int32_t tiebreak;               /* clue_tiebreak */
-  int32_t reserved;
+  int32_t flags;                  /* CLUE_FLAG_* */
 } clue_params;
+
+/* Local-density summation order.  By default the flat kernel sums every point's terms in the
+ * reference's candidate order (search-box tiles lexicographically, ascending index inside a
+ * tile), which makes rho bit-identical to the reference's serial backend; the exponential and
+ * Gaussian kernels, whose device expf can differ from the host's by an ulp anyway, sum in a
+ * spatial order that skips far candidate blocks (rho within 1e-5 relative of FP64). */
+#define CLUE_FLAG_REFERENCE_ORDER 1 /* reference order for every kernel */
+#define CLUE_FLAG_SPATIAL_DENSITY 2 /* spatial order for the flat kernel too */
 
 /* Output arrays, caller-owned, n elements each, all in the memory space given by
  * `memory` in clue_make_clusters.  Only cluster_index is required. */

@@ -17,18 +17,19 @@ def oracle_cfg(dc, rhoc, dm=None, seed_dc=None, ppbin=128, kernel=("flat", (0.5,
 
 
 def gpu_args(dc, rhoc, dm=None, seed_dc=None, ppbin=128, kernel=("flat", (0.5,)),
-             metric=("euclidean", ()), wrapped=(), seed_capacity=0, tiebreak="reference"):
+             metric=("euclidean", ()), wrapped=(), seed_capacity=0, tiebreak="reference", flags=0):
     from cluestering_alpaka3_b200 import capi
     params = capi.Params(dc=dc, rhoc=rhoc, dm=dm, seed_dc=seed_dc, points_per_tile=ppbin,
                          wrapped=tuple(wrapped), seed_capacity=seed_capacity,
-                         tiebreak=capi.TIE_REFERENCE if tiebreak == "reference" else capi.TIE_RHO_INDEX)
+                         tiebreak=capi.TIE_REFERENCE if tiebreak == "reference" else capi.TIE_RHO_INDEX,
+                         flags=flags)
     k = capi.Kernel(KERNEL_NAMES[kernel[0]], tuple(kernel[1]))
     m = capi.Metric(METRIC_NAMES.index(metric[0]), tuple(metric[1]))
     return params, k, m
 
 
 def run_both(ctx, coords, weight, **kw):
-    cfg = oracle_cfg(**kw)
+    cfg = oracle_cfg(**{k: v for k, v in kw.items() if k != "flags"})
     ref = O.run(coords, weight, cfg)
     params, k, m = gpu_args(**kw)
     got = ctx.make_clusters_host(coords, weight, params, k, m)

@@ -85,13 +85,25 @@ def _assert_tolerant(ref, got, coords, weight, kw):
     assert rep["label_mismatch"] <= max(2, rep["n"] // 1000), rep
 
 
+@pytest.mark.parametrize("flags", [0, 1])
 @pytest.mark.parametrize("kernel", [("exp", (1.0, 1.0)), ("gaus", (0.0, 0.5, 1.0)), ("gaus", (1.0, 2.0, 1.5))])
-def test_exp_gauss_kernels(gpu_context, kernel):
+def test_exp_gauss_kernels(gpu_context, kernel, flags):
+    # flags 0: spatial summation order (default for these kernels); 1: reference order
     rng = np.random.default_rng(11)
     c, w = random_blobs(rng, 8000, 2, nblobs=12, extent=80.0, sigma=1.2)
     kw = dict(dc=2.0, rhoc=4.0, dm=3.0, kernel=kernel)
-    ref, got = run_both(gpu_context, c, w, **kw)
+    ref, got = run_both(gpu_context, c, w, flags=flags, **kw)
     np.testing.assert_array_equal(got.delta > 0, ref.delta > 0)
+    _assert_tolerant(ref, got, c, w, kw)
+
+
+@pytest.mark.parametrize("ndim", [2, 3, 4])
+def test_flat_spatial_order_tolerance(gpu_context, ndim):
+    from cluestering_alpaka3_b200 import capi
+    rng = np.random.default_rng(40 + ndim)
+    c, w = random_blobs(rng, 6000, ndim, nblobs=8, extent=40.0)
+    kw = dict(dc=1.5 + 0.3 * ndim, rhoc=3.0, dm=2.0 + 0.3 * ndim, kernel=("flat", (0.5,)))
+    ref, got = run_both(gpu_context, c, w, flags=capi.FLAG_SPATIAL_DENSITY, **kw)
     _assert_tolerant(ref, got, c, w, kw)
 
 
