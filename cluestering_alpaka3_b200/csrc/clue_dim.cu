@@ -291,13 +291,21 @@ __device__ __forceinline__ void bcast_rec(const float* mine, int j, float* c, fl
 // and blocks whose bounding box lies beyond bound() for every lane, or whose largest payload is
 // below pmin for every lane, are skipped; vis(p0, p1, inbox, lexpos) gets the rest.  lexpos is
 // the tile's position in this lane's reference iteration order (lexicographic over its box).
-template <int N, class M, class Bound, class Visit>
+// With PREVISIT, p_home is the lane's own Morton position: the blocks around the warp's own
+// positions in the home tile are visited first (the nearest candidates are there, which tightens
+// bound() for the rest of the sweep) and skipped later.  Without it every tile's blocks are
+// visited in Morton order, so order-sensitive sums do not depend on how records are aligned to
+// blocks (a batch and a single event give identical results).
+template <int N, class M, bool PREVISIT, class Bound, class Visit>
 __device__ __forceinline__ void spatial_sweep(const KParams& kp, const EvGrid* __restrict__ g,
                                               const int32_t* __restrict__ off, const int* hb, const int* lo,
                                               const int* hi, bool valid, const float* x,
                                               const float4* __restrict__ blk, const float4* __restrict__ sblk,
-                                              float pmin, Bound&& bound, Visit&& vis) {
+                                              float pmin, int p_home, Bound&& bound, Visit&& vis) {
   constexpr int BW = Blk<N>::kWords;
+  const int ph_lo = warp_min_i(valid ? p_home : INT_MAX);
+  const int ph_hi = warp_max_i(valid ? p_home : INT_MIN);
+  int skip_lo = 1, skip_hi = 0;  // home-tile blocks already visited
   int wl[N], wh[N];
 #pragma unroll
   for (int d = 0; d < N; ++d) {
@@ -353,6 +361,21 @@ __device__ __forceinline__ void spatial_sweep(const KParams& kp, const EvGrid* _
     if (!__any_sync(0xffffffffu, inbox)) continue;
     const int pb = off[u], pe = off[u + 1];
     if (pb >= pe) continue;
+    const bool home_tile = PREVISIT && phase == 1;
+    if (home_tile && ph_lo <= ph_hi) {
+      skip_lo = max(pb >> 5, (ph_lo >> 5) - 1);
+      skip_hi = min((pe - 1) >> 5, (ph_hi >> 5) + 1);
+      for (int b = skip_lo; b <= skip_hi; ++b) {
+        const int q0 = max(pb, b << 5), q1 = min(pe, (b + 1) << 5);
+        bool need = inbox;
+        if (kp.lb_ok) {
+          float bb[4 * BW];
+          load_box<N>(blk, b, bb);
+          need = need && M::lower(x, bb, bb + N, kp.mpar) <= bound() && bb[2 * N] >= pmin;
+        }
+        if (__any_sync(0xffffffffu, need)) vis(q0, q1, need, lexpos);
+      }
+    }
     for (int sbk = pb >> 10; sbk <= (pe - 1) >> 10; ++sbk) {
       if (kp.lb_ok) {
         float bb[4 * BW];
@@ -362,6 +385,7 @@ __device__ __forceinline__ void spatial_sweep(const KParams& kp, const EvGrid* _
       }
       const int sp0 = max(pb, sbk << 10), sp1 = min(pe, (sbk + 1) << 10);
       for (int b = sp0 >> 5; b <= (sp1 - 1) >> 5; ++b) {
+        if (home_tile && b >= skip_lo && b <= skip_hi) continue;
         bool need = inbox;
         if (kp.lb_ok) {
           float bb[4 * BW];
@@ -1006,7 +1030,8 @@ __global__ void __launch_bounds__(kTileThreads) k_nearest_higher(
     const int32_t* __restrict__ chunk_tile, const uint32_t* __restrict__ chunk_off,
     const uint32_t* __restrict__ chunk_total, const float4* __restrict__ rec_r, const float4* __restrict__ rec_m,
     const int32_t* __restrict__ mq, const float4* __restrict__ blk, const float4* __restrict__ sblk,
-    const int32_t* __restrict__ perm, int32_t* __restrict__ nh_s, float* __restrict__ delta_s, DevStatus* st) {
+    const int32_t* __restrict__ minv, const int32_t* __restrict__ perm, int32_t* __restrict__ nh_s,
+    float* __restrict__ delta_s, DevStatus* st) {
   using M = Metric<N, MT>;
   ChunkHome h;
   if (!chunk_home(kp, ev, off, ord, chunk_tile, chunk_off, chunk_total, h)) return;
@@ -1024,7 +1049,7 @@ __global__ void __launch_bounds__(kTileThreads) k_nearest_higher(
   float delta = FLT_MAX, s_best = INFINITY, rho_best = 0.0f;
   int nh = -1, orig_best = INT_MAX;
   uint64_t rank_best = ~0ull;
-  spatial_sweep<N, M>(kp, h.g, off, hb, lo, hi, valid, x, blk, sblk, rho_i,
+  spatial_sweep<N, M, true>(kp, h.g, off, hb, lo, hi, valid, x, blk, sblk, rho_i, minv[pos],
                       [&]() { return s_best < INFINITY ? fminf(tdm, s_best * slack) : tdm; },
                       [&](int p0, int p1, bool need, int64_t lexpos) {
     const float bound = s_best < INFINITY ? fminf(tdm, s_best * slack) : tdm;
@@ -1103,7 +1128,7 @@ __global__ void __launch_bounds__(kTileThreads) k_density_spatial(
   if (!__any_sync(0xffffffffu, valid)) return;
   const float tdc = kp.t_dc;
   float rho = 0.0f;
-  spatial_sweep<N, M>(kp, h.g, off, hb, lo, hi, valid, x, blk, sblk, -INFINITY, [&]() { return tdc; },
+  spatial_sweep<N, M, false>(kp, h.g, off, hb, lo, hi, valid, x, blk, sblk, -INFINITY, p_home, [&]() { return tdc; },
                       [&](int p0, int p1, bool need, int64_t) {
     float mine[4 * Rec<N>::kWords];
     warp_load_block<N>(rec_m, p0, p1 - p0, mine);
@@ -1257,11 +1282,11 @@ void launch_nh(const KParams& kp, Workspace& ws, cudaStream_t s) {
   if (kp.tiebreak == CLUE_TIE_RHO_INDEX)
     k_nearest_higher<N, MT, CLUE_TIE_RHO_INDEX><<<chunk_grid(kp), kTileThreads, 0, s>>>(
         kp, events_of(ws), ws.offsets, ws.ord_nh, ws.chunk_tile, ws.chunk_count, ws.chunk_total, ws.rec_r,
-        ws.rec_m, ws.mq, ws.blk, ws.sblk, ws.perm, ws.nh_s, ws.delta_s, ws.status);
+        ws.rec_m, ws.mq, ws.blk, ws.sblk, ws.minv, ws.perm, ws.nh_s, ws.delta_s, ws.status);
   else
     k_nearest_higher<N, MT, CLUE_TIE_REFERENCE><<<chunk_grid(kp), kTileThreads, 0, s>>>(
         kp, events_of(ws), ws.offsets, ws.ord_nh, ws.chunk_tile, ws.chunk_count, ws.chunk_total, ws.rec_r,
-        ws.rec_m, ws.mq, ws.blk, ws.sblk, ws.perm, ws.nh_s, ws.delta_s, ws.status);
+        ws.rec_m, ws.mq, ws.blk, ws.sblk, ws.minv, ws.perm, ws.nh_s, ws.delta_s, ws.status);
 }
 template <int N, int MT>
 void launch_density_spatial(const KParams& kp, Workspace& ws, cudaStream_t s) {
