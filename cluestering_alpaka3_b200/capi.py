@@ -458,6 +458,16 @@ class Context:
                                    ms.ctypes.data if ms is not None else None))
         return ms
 
+    def get_clusters(self, labels_ptr: int, n: int, offsets_ptr: int, points_ptr: int,
+                     stream: int = 0) -> tuple[int, int]:
+        """Cluster -> points CSR of n device labels (clue_get_clusters).  offsets_ptr must hold
+        n + 1 int32 and points_ptr n int32 (device).  Returns (n_clusters, n_clustered)."""
+        nc, ncl = ctypes.c_int32(0), ctypes.c_int32(0)
+        check(lib.clue_get_clusters(self.handle, n, ctypes.c_void_p(labels_ptr), ctypes.c_void_p(offsets_ptr),
+                                    ctypes.c_void_p(points_ptr), ctypes.byref(nc), ctypes.byref(ncl),
+                                    ctypes.c_void_p(stream)))
+        return nc.value, ncl.value
+
     def read_info(self, stream: int = 0) -> RunInfo:
         info = _RunInfo()
         check(lib.clue_context_read_info(self.handle, ctypes.c_void_p(stream), ctypes.byref(info)))

@@ -273,6 +273,33 @@ float metric_eval_n(int32_t type, const float* a, const float* b, const float* p
 
 }  // namespace clue_b200
 
+namespace clue_b200 {
+
+// keys[i] = cluster_index[i] + 1 (0 for outliers); labels outside [-1, n) raise *bad and count
+// as outliers so that every key stays inside the offsets table.
+__global__ void k_label_keys(const int32_t* __restrict__ label, int n, uint32_t* __restrict__ keys,
+                             int32_t* __restrict__ bad) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int l = label[i];
+    const bool ok = l >= -1 && l < n;
+    if (!ok) atomicOr(bad, 1);
+    keys[i] = ok ? (uint32_t)(l + 1) : 0u;
+  }
+}
+
+// off[k] = first sorted position of key k (k = 0..n+1); key 0 holds the outliers, so cluster c
+// owns sorted positions [off[c + 1], off[c + 2]).  Writes offsets[0..n] and the clustered points.
+__global__ void k_cluster_csr(const int32_t* __restrict__ off, const int32_t* __restrict__ vals, int n,
+                              int32_t* __restrict__ offsets, int32_t* __restrict__ points) {
+  const int first = off[1];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= n; i += gridDim.x * blockDim.x) {
+    offsets[i] = off[i + 1] - first;
+    if (i < n - first) points[i] = vals[first + i];
+  }
+}
+
+}  // namespace clue_b200
+
 using namespace clue_b200;
 
 struct clue_context_s {
@@ -739,10 +766,44 @@ clue_status clue_context_stage_times(clue_context ctx, float* ms, int32_t n_stag
 
 uint64_t clue_context_kernel_launches(clue_context ctx) { return ctx ? ctx->ws.launches : 0; }
 
-clue_status clue_get_clusters(clue_context, int32_t, const int32_t*, int32_t*, int32_t*, int32_t*, int32_t*,
-                              void*) {
-  set_error("clue_get_clusters: not built yet");
-  return CLUE_ERR_NOT_SUPPORTED;
+clue_status clue_get_clusters(clue_context ctx, int32_t n, const int32_t* cluster_index, int32_t* offsets,
+                              int32_t* points, int32_t* n_clusters_out, int32_t* n_clustered_out, void* stream) {
+  if (!ctx || n <= 0 || !cluster_index || !offsets || !points) {
+    set_error("clue_get_clusters: null argument or n <= 0");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  Workspace& ws = ctx->ws;
+  // keys = label + 1 in [0, n]; offsets_from_sorted needs n + 2 entries, one more word holds
+  // the invalid-label flag.
+  clue_status st = workspace_reserve(ws, 1, (size_t)n, (size_t)n + 2, 1);
+  if (st != CLUE_OK) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  cudaSetDevice(ws.device);
+  int32_t* bad = ws.offsets + (n + 2);
+  CLUE_CUDA_TRY(cudaMemsetAsync(bad, 0, sizeof(int32_t), s));
+  const int threads = 256;
+  const int blocks = std::min((n + threads - 1) / threads, 148 * 16);
+  k_label_keys<<<blocks, threads, 0, s>>>(cluster_index, n, ws.keys[0], bad);
+  const int cur = radix_sort_pairs(ws.keys, ws.vals, true, n, bits_for((uint32_t)n), ws.hist, ws.scan_scratch, s);
+  offsets_from_sorted(ws.keys[cur], n, n + 1, ws.offsets, s);
+  k_cluster_csr<<<blocks, threads, 0, s>>>(ws.offsets, ws.vals[cur], n, offsets, points);
+  ws.launches += 3 + radix_sort_launches(bits_for((uint32_t)n));
+  int32_t h[2] = {0, 0};
+  uint32_t last = 0;
+  CLUE_CUDA_TRY(cudaMemcpyAsync(h, ws.offsets + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  CLUE_CUDA_TRY(cudaMemcpyAsync(h + 1, bad, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  CLUE_CUDA_TRY(cudaMemcpyAsync(&last, ws.keys[cur] + (n - 1), sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  CLUE_CUDA_TRY(cudaStreamSynchronize(s));
+  cudaSetDevice(prev);
+  if (h[1]) {
+    set_error("clue_get_clusters: cluster index outside [-1, n)");
+    return CLUE_ERR_OUT_OF_RANGE;
+  }
+  if (n_clusters_out) *n_clusters_out = (int32_t)last;  // max label + 1 (0 when all are -1)
+  if (n_clustered_out) *n_clustered_out = n - h[0];
+  return CLUE_OK;
 }
 
 }  // extern "C"

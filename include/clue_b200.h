@@ -276,10 +276,14 @@ clue_status clue_make_clusters_noalloc(const clue_params* params, const clue_ker
                                        const clue_outputs* out, void* stream, clue_run_info* info);
 
 /*
- * Cluster -> points association map (CSR) from device labels: offsets[n_clusters + 1],
- * points[n_clustered] (point indexes ascending inside each cluster).  All device
- * pointers; `offsets` must hold max_label + 2 entries and `points` n entries.
- * n_clusters_out / n_clustered_out are written on the host (synchronises).
+ * Cluster -> points association map (CSR) from device labels, the device side of
+ * clue::get_clusters (include/CLUEstering/utils/get_clusters.hpp:34-36 and
+ * data_structures/internal/MakeAssociator.hpp:11-34 in the reference): keys 0..max_label,
+ * offsets[c]..offsets[c + 1] are the points of cluster c, point indexes ascending inside a
+ * cluster (the order of the reference's host fill); labels -1 are left out.  All device
+ * pointers: `offsets` must hold n + 1 entries (entries past n_clusters repeat the total) and
+ * `points` n entries.  n_clusters_out (= max label + 1) and n_clustered_out are written on the
+ * host; the call synchronises `stream`.  A label outside [-1, n) gives CLUE_ERR_OUT_OF_RANGE.
  */
 clue_status clue_get_clusters(clue_context ctx, int32_t n, const int32_t* cluster_index,
                               int32_t* offsets, int32_t* points, int32_t* n_clusters_out,
