@@ -39,7 +39,9 @@ EXPORTED = [
     "clue_context_read_info", "clue_get_clusters", "clue_context_set_timing",
     "clue_context_stage_times", "clue_context_kernel_launches", "clue_make_clusters_noalloc",
     "clue_batch_make_clusters", "clue_batch_make_clusters_async", "clue_graph_capture_batch",
-    "clue_graph_launch", "clue_graph_destroy", "clue_events_loop",
+    "clue_graph_launch", "clue_graph_destroy", "clue_events_loop", "clue_context_reserve_batch",
+    "clue_server_create", "clue_server_destroy", "clue_server_submit", "clue_server_wait",
+    "clue_server_stats_read", "clue_server_replay",
 ]
 
 
@@ -83,6 +85,25 @@ class _RunInfo(ctypes.Structure):
                 ("dropped_seeds", ctypes.c_int64), ("seed_capacity_used", ctypes.c_int64),
                 ("n_tiles", ctypes.c_int64), ("n_per_dim", ctypes.c_int64),
                 ("label_rounds", ctypes.c_int64)]
+
+
+class _ServerConfig(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("ndim", ctypes.c_int32), ("n_slots", ctypes.c_int32),
+                ("max_batch_events", ctypes.c_int32), ("max_event_points", ctypes.c_int32),
+                ("max_pending", ctypes.c_int32), ("device_budget_bytes", ctypes.c_int64)]
+
+
+class _RequestInfo(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int32), ("n_clusters", ctypes.c_int32), ("batch_events", ctypes.c_int32),
+                ("slot", ctypes.c_int32), ("submit_s", ctypes.c_double), ("start_s", ctypes.c_double),
+                ("done_s", ctypes.c_double)]
+
+
+class _ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("rejected", ctypes.c_int64),
+                ("failed", ctypes.c_int64), ("batches", ctypes.c_int64), ("batched_points", ctypes.c_int64),
+                ("slot_points", ctypes.c_int64), ("slot_events", ctypes.c_int64), ("device_bytes", ctypes.c_int64),
+                ("max_batch_seen", ctypes.c_int32), ("max_in_flight", ctypes.c_int32)]
 
 
 def _load() -> ctypes.CDLL:
@@ -140,11 +161,19 @@ def _load() -> ctypes.CDLL:
     sig["clue_graph_launch"] = ([vp, vp], ctypes.c_int)
     sig["clue_events_loop"] = (batch_args[:-1] + [vp, vp], ctypes.c_int)
     sig["clue_graph_destroy"] = ([vp], ctypes.c_int)
+    sig["clue_context_reserve_batch"] = ([vp, i32, i64, i64, i32], ctypes.c_int)
+    sig["clue_server_create"] = ([ctypes.POINTER(_ServerConfig), ctypes.POINTER(_Params), ctypes.POINTER(_Kernel),
+                                  ctypes.POINTER(_Metric), ctypes.POINTER(vp)], ctypes.c_int)
+    sig["clue_server_destroy"] = ([vp], ctypes.c_int)
+    sig["clue_server_submit"] = ([vp, i32, vp, i64, vp, ctypes.POINTER(_Outputs), ctypes.POINTER(i64)], ctypes.c_int)
+    sig["clue_server_wait"] = ([vp, i64, i32, ctypes.POINTER(_RequestInfo)], ctypes.c_int)
+    sig["clue_server_stats_read"] = ([vp, ctypes.POINTER(_ServerStats)], ctypes.c_int)
+    sig["clue_server_replay"] = ([vp, i32, vp, vp, vp, vp, vp, ctypes.POINTER(_Outputs), vp, ctypes.POINTER(i32)],
+                                 ctypes.c_int)
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
         f.argtypes = args
         f.restype = res
-    _ = i64
     return lib
 
 
@@ -486,6 +515,116 @@ class Graph:
     def close(self):
         if self.handle:
             lib.clue_graph_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class ServerConfig:
+    ndim: int
+    device: int = 0
+    n_slots: int = 3
+    max_batch_events: int = 1024
+    max_event_points: int = 200000
+    max_pending: int = 1 << 16
+    device_budget_bytes: int = 8 << 30
+
+    def struct(self) -> _ServerConfig:
+        c = _ServerConfig()
+        for f, _ in _ServerConfig._fields_:
+            setattr(c, f, getattr(self, f))
+        return c
+
+
+@dataclass
+class EventResult:
+    cluster_index: np.ndarray
+    is_seed: np.ndarray
+    rho: np.ndarray
+    nearest_higher: np.ndarray
+    delta: np.ndarray
+    info: dict
+
+
+class Server:
+    """Continuous-batching request loop on one GPU (clue_server_*): submit events from host
+    memory, wait for their results; or replay a whole arrival trace natively."""
+
+    def __init__(self, config: ServerConfig, params: Params, kernel: Kernel, metric: Metric | None = None):
+        metric = metric or Metric()
+        self.ndim = config.ndim
+        h = ctypes.c_void_p()
+        cfg = config.struct()
+        check(lib.clue_server_create(ctypes.byref(cfg), ctypes.byref(params.struct()), ctypes.byref(kernel.struct()),
+                                     ctypes.byref(metric.struct(config.ndim)), ctypes.byref(h)))
+        self.handle = h
+        self._live = {}  # ticket -> arrays the server reads / writes until the request is waited
+
+    def submit(self, coords: np.ndarray, weight: np.ndarray) -> int:
+        coords = np.ascontiguousarray(coords, dtype=np.float32)
+        weight = np.ascontiguousarray(weight, dtype=np.float32)
+        n = weight.shape[0]
+        res = EventResult(np.empty(n, np.int32), np.empty(n, np.int32), np.empty(n, np.float32),
+                          np.empty(n, np.int32), np.empty(n, np.float32), {})
+        out = _Outputs(res.cluster_index.ctypes.data, res.is_seed.ctypes.data, res.rho.ctypes.data,
+                       res.nearest_higher.ctypes.data, res.delta.ctypes.data)
+        t = ctypes.c_int64()
+        check(lib.clue_server_submit(self.handle, n, coords.ctypes.data, coords.shape[1], weight.ctypes.data,
+                                     ctypes.byref(out), ctypes.byref(t)))
+        self._live[t.value] = (coords, weight, res)
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = -1) -> EventResult:
+        info = _RequestInfo()
+        st = lib.clue_server_wait(self.handle, ticket, timeout_ms, ctypes.byref(info))
+        if st == ERR_TIMEOUT:
+            check(st)
+        _, _, res = self._live.pop(ticket)
+        check(st)
+        res.info = {f: getattr(info, f) for f, _ in _RequestInfo._fields_}
+        return res
+
+    def stats(self) -> dict:
+        s = _ServerStats()
+        check(lib.clue_server_stats_read(self.handle, ctypes.byref(s)))
+        return {f: getattr(s, f) for f, _ in _ServerStats._fields_}
+
+    def replay(self, coords: np.ndarray, weight: np.ndarray, event_offsets, arrival_s, event_ids=None,
+               outputs: bool = True):
+        """Submits trace event e (pool event event_ids[e], or e) at arrival_s[e] seconds, open loop,
+        from a native thread.  Returns (outputs dict of concatenated arrays or None,
+        latency_s per event (-1 = refused), n_refused)."""
+        coords = np.ascontiguousarray(coords, dtype=np.float32)
+        weight = np.ascontiguousarray(weight, dtype=np.float32)
+        off = np.ascontiguousarray(event_offsets, dtype=np.int32)
+        arr = np.ascontiguousarray(arrival_s, dtype=np.float64)
+        ids = None if event_ids is None else np.ascontiguousarray(event_ids, dtype=np.int32)
+        E = arr.shape[0]
+        res, outp = None, None
+        if outputs:
+            if ids is not None:
+                raise ValueError("outputs need one trace event per pool event (event_ids=None)")
+            n = weight.shape[0]
+            res = {"cluster_index": np.empty(n, np.int32), "is_seed": np.empty(n, np.int32),
+                   "rho": np.empty(n, np.float32), "nearest_higher": np.empty(n, np.int32),
+                   "delta": np.empty(n, np.float32)}
+            outp = ctypes.byref(_Outputs(*(res[k].ctypes.data for k in
+                                           ("cluster_index", "is_seed", "rho", "nearest_higher", "delta"))))
+        lat = np.empty(E, np.float64)
+        rej = ctypes.c_int32()
+        check(lib.clue_server_replay(self.handle, E, None if ids is None else ids.ctypes.data, off.ctypes.data,
+                                     arr.ctypes.data, coords.ctypes.data, weight.ctypes.data, outp, lat.ctypes.data,
+                                     ctypes.byref(rej)))
+        return res, lat, rej.value
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib.clue_server_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

@@ -104,25 +104,21 @@ int lower_bounds_ok(const clue_metric* m, int ndim) {
   return 1;
 }
 
-clue_status workspace_reserve(Workspace& ws, int ndim, size_t n, size_t ntiles, size_t n_events) {
-  const size_t words = (size_t)((ndim + 1 + 3) / 4);
-  if (n <= ws.cap_n && ntiles <= ws.cap_tiles && words <= ws.cap_words && n_events <= ws.cap_events && ws.arena)
-    return CLUE_OK;
-  n = std::max(n, ws.cap_n);
-  ntiles = std::max(ntiles, ws.cap_tiles);
-  n_events = std::max(n_events, ws.cap_events);
-  const size_t w = std::max(words, ws.cap_words);
+namespace {
+
+struct ArenaItem {
+  void** ptr;
+  size_t bytes;
+};
+
+// The buffers of the workspace arena for n points, ntiles tiles, n_events events and w record
+// words; `nw` receives the carved pointers once an arena is placed (arena_place).
+std::vector<ArenaItem> arena_items(Workspace& nw, void** evtab, size_t n, size_t ntiles, size_t n_events, size_t w) {
   const size_t nb = (size_t)sort_blocks((int)n);
   const size_t hist_len = (size_t)kRadix * nb;
   const size_t scan_words = scan_scratch_words(std::max(std::max(hist_len, n), ntiles)) + 1;
-  struct Item {
-    void** ptr;
-    size_t bytes;
-  };
-  Workspace nw = ws;
-  void* evtab = nullptr;
-  Item items[] = {
-      {&evtab, event_table_bytes(n_events)},
+  return {
+      {evtab, event_table_bytes(n_events)},
       {(void**)&nw.status, sizeof(DevStatus)},
       {(void**)&nw.keys[0], n * 4},
       {(void**)&nw.keys[1], n * 4},
@@ -150,8 +146,34 @@ clue_status workspace_reserve(Workspace& ws, int ndim, size_t n, size_t ntiles, 
       {(void**)&nw.chunk_tile, (n / kChunkPoints + ntiles + 1) * 4},
       {(void**)&nw.chunk_total, 16},
   };
+}
+
+size_t arena_total(const std::vector<ArenaItem>& items) {
   size_t total = 0;
   for (auto& it : items) total = align_up(total, 256) + align_up(it.bytes, 256);
+  return total;
+}
+
+}  // namespace
+
+size_t workspace_bytes_for(int ndim, size_t n, size_t ntiles, size_t n_events) {
+  Workspace nw;
+  void* evtab = nullptr;
+  return arena_total(arena_items(nw, &evtab, n, ntiles, n_events, (size_t)((ndim + 1 + 3) / 4)));
+}
+
+clue_status workspace_reserve(Workspace& ws, int ndim, size_t n, size_t ntiles, size_t n_events) {
+  const size_t words = (size_t)((ndim + 1 + 3) / 4);
+  if (n <= ws.cap_n && ntiles <= ws.cap_tiles && words <= ws.cap_words && n_events <= ws.cap_events && ws.arena)
+    return CLUE_OK;
+  n = std::max(n, ws.cap_n);
+  ntiles = std::max(ntiles, ws.cap_tiles);
+  n_events = std::max(n_events, ws.cap_events);
+  const size_t w = std::max(words, ws.cap_words);
+  Workspace nw = ws;
+  void* evtab = nullptr;
+  const std::vector<ArenaItem> items = arena_items(nw, &evtab, n, ntiles, n_events, w);
+  const size_t total = arena_total(items);
   int prev = 0;
   cudaGetDevice(&prev);
   cudaSetDevice(ws.device);
@@ -542,6 +564,16 @@ clue_status clue_context_reserve(clue_context ctx, int32_t ndim, int32_t n, int3
   int32_t npd, nt;
   grid_shape(n, ppbin, ndim, &npd, &nt);
   return workspace_reserve(ctx->ws, ndim, (size_t)n, (size_t)nt);
+}
+
+clue_status clue_context_reserve_batch(clue_context ctx, int32_t ndim, int64_t n_points, int64_t n_tiles,
+                                       int32_t n_events) {
+  if (!ctx || n_points <= 0 || n_tiles <= 0 || n_events <= 0 || ndim < 1 || ndim > CLUE_MAX_DIM ||
+      n_points > 2147483000ll || n_tiles > 2147483000ll) {
+    set_error("invalid batch reserve request");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  return workspace_reserve(ctx->ws, ndim, (size_t)n_points, (size_t)n_tiles, (size_t)n_events);
 }
 
 size_t clue_context_workspace_bytes(clue_context ctx) { return ctx ? ctx->ws.arena_bytes + ctx->ws.dstage_bytes : 0; }

@@ -158,6 +158,8 @@ inline void event_table_carve(void* base, size_t cap, EvGrid** eg, int32_t** pt,
   *tile = *pt + cap + 1;
 }
 void workspace_release(Workspace& ws);
+// Arena bytes workspace_reserve would allocate for these capacities (nothing is allocated).
+size_t workspace_bytes_for(int ndim, size_t n, size_t ntiles, size_t n_events);
 
 // Host helpers (clue_capi.cu)
 float threshold_for(float r, bool root);

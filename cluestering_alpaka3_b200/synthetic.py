@@ -110,6 +110,24 @@ def blobs_4d_event(rng: np.random.Generator, n: int) -> tuple[np.ndarray, np.nda
     return np.ascontiguousarray(c), w
 
 
+def serving_events(n_events: int, seed: int = 5000, lo: int = 100, hi: int = 200000):
+    """4-D serving events: sizes lognormal(median 2000, sigma 1) clipped to [lo, hi]; returns
+    the events concatenated (coords (4, n_total), weight, event offsets) and the parameters."""
+    rng = np.random.default_rng(seed)
+    sizes = np.clip(np.round(rng.lognormal(np.log(2000), 1.0, size=n_events)), lo, hi).astype(np.int64)
+    evs = [blobs_4d_event(rng, int(s)) for s in sizes]
+    off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int32)
+    coords = np.ascontiguousarray(np.concatenate([e[0] for e in evs], axis=1))
+    weight = np.ascontiguousarray(np.concatenate([e[1] for e in evs]))
+    return coords, weight, off, dict(dc=2.5, rhoc=6.0, dm=2.5, kernel=("flat", (0.5,)))
+
+
+def poisson_arrivals(rate: float, n: int, seed: int = 0) -> np.ndarray:
+    """Arrival times (seconds) of a Poisson stream of `rate` events/s."""
+    rng = np.random.default_rng(seed)
+    return np.cumsum(rng.exponential(1.0 / rate, size=n))
+
+
 CONFIGS = {
     "blobs2d_16k": blobs_2d_16k,
     "blobs2d_1m": blobs_2d_1m,

@@ -173,6 +173,10 @@ clue_status clue_context_destroy(clue_context ctx);
 /* Pre-size the workspace for up to n points of ndim dimensions (optional). */
 clue_status clue_context_reserve(clue_context ctx, int32_t ndim, int32_t n, int32_t points_per_tile);
 /* Bytes of device workspace the context currently holds. */
+/* Pre-sizes the workspace for batched calls of up to n_points points, n_tiles tiles (the sum of
+ * the events' reference grids) and n_events events, so that such calls allocate nothing. */
+clue_status clue_context_reserve_batch(clue_context ctx, int32_t ndim, int64_t n_points, int64_t n_tiles,
+                                       int32_t n_events);
 size_t clue_context_workspace_bytes(clue_context ctx);
 
 /*
@@ -288,6 +292,75 @@ clue_status clue_make_clusters_noalloc(const clue_params* params, const clue_ker
 clue_status clue_get_clusters(clue_context ctx, int32_t n, const int32_t* cluster_index,
                               int32_t* offsets, int32_t* points, int32_t* n_clusters_out,
                               int32_t* n_clustered_out, void* stream);
+
+/* ---- serving (no reference counterpart) -------------------------------------------------
+ * A request loop with continuous batching on one GPU.  Callers submit single events (host
+ * memory) from any thread; a dispatcher thread owned by the server packs every pending event
+ * that fits into the next free slot and runs them as one batched pipeline, while the other
+ * slots' batches are still on the GPU.  Each slot is a preallocated device pool (workspace,
+ * input and output buffers) plus pinned staging and a stream; together the slots stay inside
+ * device_budget_bytes, and an event is admitted to a slot only while the slot's points,
+ * tiles and events stay within what was reserved for it.  Results are identical to clustering
+ * the event alone (same per-event grids and label numbering; nearest_higher is event-local).
+ */
+typedef struct clue_server_s* clue_server;
+
+typedef struct clue_server_config {
+  int32_t device;
+  int32_t ndim;                 /* 1..10 */
+  int32_t n_slots;              /* batches that may be on the GPU at once, 1..16 */
+  int32_t max_batch_events;     /* events per batch, >= 1 */
+  int32_t max_event_points;     /* larger events are refused (CLUE_ERR_CAPACITY) */
+  int32_t max_pending;          /* queued events before submit refuses (CLUE_ERR_CAPACITY) */
+  int64_t device_budget_bytes;  /* device memory for all slots; each slot holds >= max_event_points */
+} clue_server_config;
+
+typedef struct clue_request_info {
+  int32_t status;          /* clue_status of the request */
+  int32_t n_clusters;      /* clusters of the event */
+  int32_t batch_events;    /* events in the batch that carried it */
+  int32_t slot;            /* slot that ran it */
+  double submit_s;         /* server clock (seconds since creation): accepted */
+  double start_s;          /* its batch was enqueued on the GPU */
+  double done_s;           /* results were in the caller's buffers */
+} clue_request_info;
+
+typedef struct clue_server_stats {
+  int64_t submitted, completed, rejected, failed;
+  int64_t batches, batched_points;
+  int64_t slot_points;     /* points one slot holds */
+  int64_t slot_events;
+  int64_t device_bytes;    /* device memory held by all slots */
+  int32_t max_batch_seen;  /* largest batch (events) so far */
+  int32_t max_in_flight;   /* most slots on the GPU at once so far */
+} clue_server_stats;
+
+clue_status clue_server_create(const clue_server_config* config, const clue_params* params,
+                               const clue_kernel* kernel, const clue_metric* metric, clue_server* server);
+/* Waits for the batches on the GPU, then frees everything; pending requests fail. */
+clue_status clue_server_destroy(clue_server server);
+/* Queues one event: coords[d * coord_stride + i] (host), weight[i], i < n.  Inputs and the
+ * host output arrays in `out` (cluster_index required) must stay valid until the request is
+ * waited for.  Writes the request's ticket. */
+clue_status clue_server_submit(clue_server server, int32_t n, const float* coords, int64_t coord_stride,
+                               const float* weight, const clue_outputs* out, int64_t* ticket);
+/* Waits up to timeout_ms (< 0: no limit) for a request, then releases it and fills `info`
+ * (may be NULL).  CLUE_ERR_TIMEOUT leaves the request pending; the returned status is the
+ * request's own otherwise. */
+clue_status clue_server_wait(clue_server server, int64_t ticket, int32_t timeout_ms, clue_request_info* info);
+clue_status clue_server_stats_read(clue_server server, clue_server_stats* stats);
+/* Open-loop load replay from the calling thread.  Trace event e is pool event
+ * id = event_ids ? event_ids[e] : e, i.e. points [event_offsets[id], event_offsets[id + 1]) of
+ * the concatenated SoA host arrays (coords[d * n_pool_points + i], n_pool_points =
+ * event_offsets[max id + 1]); it is submitted arrival_s[e] seconds after the call.  With `out`
+ * given (only without event_ids) results land at the event's offsets; with out == NULL they
+ * stay in the server (throughput / latency runs).  latency_s[e] = completion - scheduled
+ * arrival, or -1 for an event the server refused (counted in *n_rejected).  Returns when every
+ * admitted event is done. */
+clue_status clue_server_replay(clue_server server, int32_t n_events, const int32_t* event_ids,
+                               const int32_t* event_offsets, const double* arrival_s, const float* coords,
+                               const float* weight, const clue_outputs* out, double* latency_s,
+                               int32_t* n_rejected);
 
 #ifdef __cplusplus
 }
