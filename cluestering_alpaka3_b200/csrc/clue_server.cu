@@ -482,7 +482,7 @@ clue_status clue_server_replay(clue_server S, int32_t n_events, const int32_t* e
     set_error("clue_server_replay: null argument, n_events <= 0, or outputs requested with event_ids");
     return CLUE_ERR_INVALID_ARG;
   }
-  int32_t n_pool = n_events;
+  int32_t n_pool = event_ids ? 0 : n_events;  // events in the pool: event_offsets holds n_pool + 1 entries
   if (event_ids)
     for (int32_t e = 0; e < n_events; ++e) n_pool = std::max(n_pool, event_ids[e] + 1);
   const int64_t n_total = off[n_pool];
