@@ -174,6 +174,7 @@ def main():
     ap.add_argument("--workload", default="calo4096",
                     choices=["calo4096", "blobs2d_16k", "blobs2d_1m", "blobs3d_4m"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -324,6 +325,19 @@ def main():
         if not batched:
             cpu["labels_equal_to_gpu"] = bool(np.array_equal(ref.cluster_index, res.cluster_index))
 
+    # ---- serving: Poisson stream of 4-D events through the continuous-batching server ----
+    serving = None
+    if rank == 0 and world == 1 and not args.no_serving:
+        from cluestering_alpaka3_b200 import serve_bench
+        pc, pw, po, _ = serve_bench.make_pool(512)
+        srv = serve_bench.make_server(slots=3, budget_gb=6.0)
+        try:
+            serve_bench.run_rate(srv, pc, pw, po, 2000.0, 0.3, seed=99)  # warm-up
+            serving = [serve_bench.run_rate(srv, pc, pw, po, r, 2.0, seed=1000 + i)
+                       for i, r in enumerate((5000.0, 20000.0, 50000.0))]
+        finally:
+            srv.close()
+
     if rank == 0:
         step_ms = total_ms / args.steps
         config = {"workload": wl.name, "n_points": n, "ndim": ndim, "dc": wl.dc, "rhoc": wl.rhoc, "dm": wl.dm,
@@ -350,6 +364,12 @@ def main():
             "b_alg_total": B["total"],
             "pipeline_hbm_frac": B["total"] / (step_ms / 1e3) / 1e9 / peak,
             "cpu_baseline": cpu, "clocks": clk, "gpu_launches": int(launches),
+            "serving": None if serving is None else {
+                "workload": "Poisson stream of 4-D events (lognormal sizes, median 2000, clipped [100, 200000]), "
+                            "dc=2.5 rhoc=6 dm=2.5 FlatKernel(0.5), 3 slots, 6 GiB device budget",
+                "rates": [{k: r[k] for k in ("offered_events_per_s", "p50_ms", "p99_ms", "points_per_s",
+                                             "achieved_events_per_s", "events_per_batch", "refused")}
+                          for r in serving]},
         }
         print(json.dumps(line), flush=True)
     graph.close()
