@@ -170,10 +170,12 @@ struct Metric;
 template <int N>
 struct Metric<N, CLUE_METRIC_EUCLIDEAN> {
   static constexpr bool kRoot = true;
+  // Right fold t_0 + (t_1 + (... + (t_{N-1} + 0))).  A square is never -0, so t_{N-1} + 0 is
+  // t_{N-1} itself and the fold starts there.
   CLUE_HD static float partial(const float* a, const float* b, const float*) {
-    float acc = 0.0f;
+    float acc = fmul(fsub(a[N - 1], b[N - 1]), fsub(a[N - 1], b[N - 1]));
 #pragma unroll
-    for (int d = N - 1; d >= 0; --d) {
+    for (int d = N - 2; d >= 0; --d) {
       const float t = fmul(fsub(a[d], b[d]), fsub(a[d], b[d]));
       acc = fadd(t, acc);
     }
@@ -220,15 +222,18 @@ struct Metric<N, CLUE_METRIC_WEIGHTED_EUCLIDEAN> {
 template <int N>
 struct Metric<N, CLUE_METRIC_PERIODIC_EUCLIDEAN> {
   static constexpr bool kRoot = true;
+  CLUE_HD static float term(float a, float b, float period) {
+    const float diff = fabsf(fsub(a, b));
+    const float alt = fsub(period, diff);
+    const float pd = alt < diff ? alt : diff;
+    return fmul(pd, pd);
+  }
+  // Right fold as for the Euclidean metric; a square is never -0, so the fold starts at the
+  // last term.
   CLUE_HD static float partial(const float* a, const float* b, const float* period) {
-    float acc = 0.0f;
+    float acc = term(a[N - 1], b[N - 1], period[N - 1]);
 #pragma unroll
-    for (int d = N - 1; d >= 0; --d) {
-      const float diff = fabsf(fsub(a[d], b[d]));
-      const float alt = fsub(period[d], diff);
-      const float pd = alt < diff ? alt : diff;
-      acc = fadd(fmul(pd, pd), acc);
-    }
+    for (int d = N - 2; d >= 0; --d) acc = fadd(term(a[d], b[d], period[d]), acc);
     return acc;
   }
   // Periodic dimensions contribute no bound; the others bound like the Euclidean metric.
@@ -247,10 +252,11 @@ struct Metric<N, CLUE_METRIC_PERIODIC_EUCLIDEAN> {
 template <int N>
 struct Metric<N, CLUE_METRIC_MANHATTAN> {
   static constexpr bool kRoot = false;
+  // Right fold of |a_d - b_d|; an absolute value is never -0, so the fold starts at the last term.
   CLUE_HD static float partial(const float* a, const float* b, const float*) {
-    float acc = 0.0f;
+    float acc = fabsf(fsub(a[N - 1], b[N - 1]));
 #pragma unroll
-    for (int d = N - 1; d >= 0; --d) acc = fadd(fabsf(fsub(a[d], b[d])), acc);
+    for (int d = N - 2; d >= 0; --d) acc = fadd(fabsf(fsub(a[d], b[d])), acc);
     return acc;
   }
   CLUE_HD static float lower(const float* x, const float* lo, const float* hi, const float*) {
@@ -322,6 +328,11 @@ struct Metric<N, CLUE_METRIC_WEIGHTED_CHEBYSHEV> {
 __device__ __forceinline__ float sqrt_approx(float x) {
   float y;
   asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float ex2_approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
 }
 __device__ __forceinline__ float exp_approx(float x) {

@@ -286,6 +286,37 @@ __device__ __forceinline__ void bcast_rec(const float* mine, int j, float* c, fl
   payload = __shfl_sync(0xffffffffu, mine[Rec<N>::kPayload], j);
 }
 
+// A block of up to 32 consecutive records staged in the warp's shared-memory slot: lane k
+// copies record p0 + k; smem_rec() then reads record j with broadcast loads (every lane reads
+// the same address), one 16-byte load per record word.
+template <int N>
+__device__ __forceinline__ void stage_block(float4* sm, const float4* __restrict__ rec, int p0, int cnt) {
+  constexpr int W = Rec<N>::kWords;
+  const int lane = threadIdx.x & 31;
+  __syncwarp();  // the previous block's readers are done
+  if (lane < cnt) {
+#pragma unroll
+    for (int k = 0; k < W; ++k) sm[lane * W + k] = __ldg(rec + (size_t)(p0 + lane) * W + k);
+  }
+  __syncwarp();
+}
+template <int N>
+__device__ __forceinline__ void smem_rec(const float4* sm, int j, float* c, float& payload) {
+  constexpr int W = Rec<N>::kWords;
+  float r[4 * W];
+#pragma unroll
+  for (int k = 0; k < W; ++k) {
+    const float4 v = sm[j * W + k];
+    r[4 * k] = v.x;
+    r[4 * k + 1] = v.y;
+    r[4 * k + 2] = v.z;
+    r[4 * k + 3] = v.w;
+  }
+#pragma unroll
+  for (int d = 0; d < N; ++d) c[d] = r[d];
+  payload = r[Rec<N>::kPayload];
+}
+
 // Spatial sweep of one warp over the Morton-ordered records of its search-box tiles (any
 // order: the own tile first, then the union of the warp's boxes lexicographically).  Super-blocks
 // and blocks whose bounding box lies beyond bound() for every lane, or whose largest payload is
@@ -1025,7 +1056,7 @@ __global__ void __launch_bounds__(kTileThreads) k_density(const KParams kp, Even
 // distances by higher rho, then lower index.
 
 template <int N, int MT, int TIE>
-__global__ void __launch_bounds__(kTileThreads) k_nearest_higher(
+__global__ void __launch_bounds__(kTileThreads, N <= 2 ? 8 : (N <= 4 ? 6 : 4)) k_nearest_higher(
     const KParams kp, Events ev, const int32_t* __restrict__ off, const int32_t* __restrict__ ord,
     const int32_t* __restrict__ chunk_tile, const uint32_t* __restrict__ chunk_off,
     const uint32_t* __restrict__ chunk_total, const float4* __restrict__ rec_r, const float4* __restrict__ rec_m,
@@ -1045,6 +1076,8 @@ __global__ void __launch_bounds__(kTileThreads) k_nearest_higher(
   lane_box<N>(kp, h.g, x, kp.dm, hb, lo, hi);
   if (!__any_sync(0xffffffffu, valid)) return;
   const float tdm = kp.t_dm;
+  __shared__ float4 s_rec[kTileThreads / 32][32 * Rec<N>::kWords];
+  float4* sm = s_rec[threadIdx.x >> 5];
   const float slack = M::kRoot ? 1.0f + 1.0f / 524288.0f : 1.0f;  // s range of one rounded distance
   float delta = FLT_MAX, s_best = INFINITY, rho_best = 0.0f;
   int nh = -1, orig_best = INT_MAX;
@@ -1053,14 +1086,17 @@ __global__ void __launch_bounds__(kTileThreads) k_nearest_higher(
                       [&]() { return s_best < INFINITY ? fminf(tdm, s_best * slack) : tdm; },
                       [&](int p0, int p1, bool need, int64_t lexpos) {
     const float bound = s_best < INFINITY ? fminf(tdm, s_best * slack) : tdm;
-    float mine[4 * Rec<N>::kWords];
-    warp_load_block<N>(rec_m, p0, p1 - p0, mine);
-    for (int j = 0; j < p1 - p0; ++j) {
+    const int cnt = p1 - p0;
+    stage_block<N>(sm, rec_m, p0, cnt);
+    for (int j0 = 0; j0 < cnt; j0 += 4) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int j = j0 + u;
       const int p = p0 + j;
       float c[N], rho_j;
-      bcast_rec<N>(mine, j, c, rho_j);
+      smem_rec<N>(sm, j, c, rho_j);
       const float s = M::partial(x, c, kp.mpar);
-      if (need && s <= tdm && s <= bound && rho_j >= rho_i) {
+      if (need && j < cnt && s <= tdm && s <= bound && rho_j >= rho_i) {
         const int q = __ldg(mq + p);
         int orig_j = -1;
         bool higher = rho_j > rho_i;
@@ -1092,6 +1128,7 @@ __global__ void __launch_bounds__(kTileThreads) k_nearest_higher(
         }
       }
     }
+    }
   });
   if (valid) {
     nh_s[pos] = nh;
@@ -1104,17 +1141,25 @@ __global__ void __launch_bounds__(kTileThreads) k_nearest_higher(
   }
 }
 
+// Forms of the spatial-order density.  With unit amplitude the exponential kernel is
+// exp2(kexp * d) and the zero-mean Gaussian exp2(kexp * d^2), kexp folding -avg or -1/(2 std^2)
+// with log2(e); their value at d = 0 is exp2(0) = 1, the reference's self term, so no per-pair
+// self test is needed.  Every other kernel takes the generic form.
+enum { kDensGeneric = 0, kDensExpUnit = 1, kDensGauss0Unit = 2 };
+
 // Local density over the Morton-ordered records (any order, kernels other than flat): the
 // same candidate set as the reference (search-box tiles, d <= dc, self term 1), summed in
-// spatial order.  Blocks farther than dc from every lane are skipped.
-template <int N, int MT>
-__global__ void __launch_bounds__(kTileThreads) k_density_spatial(
+// spatial order.  Blocks farther than dc from every lane are skipped; inside a block, candidates
+// that no lane of the warp holds within dc skip the kernel evaluation.
+template <int N, int MT, int FORM>
+__global__ void __launch_bounds__(kTileThreads, N <= 4 ? 8 : 4) k_density_spatial(
     const KParams kp, Events ev, const int32_t* __restrict__ off, const int32_t* __restrict__ ord,
     const int32_t* __restrict__ chunk_tile, const uint32_t* __restrict__ chunk_off,
     const uint32_t* __restrict__ chunk_total, const float4* __restrict__ rec_w, const float4* __restrict__ rec_m,
     const int32_t* __restrict__ mq, const float4* __restrict__ blk, const float4* __restrict__ sblk,
-    float4* __restrict__ rec_r, const int32_t* __restrict__ minv) {
+    float4* __restrict__ rec_r, const int32_t* __restrict__ minv, float kexp) {
   using M = Metric<N, MT>;
+  __shared__ float4 s_rec[kTileThreads / 32][32 * Rec<N>::kWords];
   ChunkHome h;
   if (!chunk_home(kp, ev, off, ord, chunk_tile, chunk_off, chunk_total, h)) return;
   const int pos = h.pos;
@@ -1127,19 +1172,34 @@ __global__ void __launch_bounds__(kTileThreads) k_density_spatial(
   lane_box<N>(kp, h.g, x, kp.dc, hb, lo, hi);
   if (!__any_sync(0xffffffffu, valid)) return;
   const float tdc = kp.t_dc;
+  float4* sm = s_rec[threadIdx.x >> 5];
   float rho = 0.0f;
   spatial_sweep<N, M, false>(kp, h.g, off, hb, lo, hi, valid, x, blk, sblk, -INFINITY, p_home, [&]() { return tdc; },
                       [&](int p0, int p1, bool need, int64_t) {
-    float mine[4 * Rec<N>::kWords];
-    warp_load_block<N>(rec_m, p0, p1 - p0, mine);
-    for (int j = 0; j < p1 - p0; ++j) {
-      float c[N], wj;
-      bcast_rec<N>(mine, j, c, wj);
-      const float s = M::partial(x, c, kp.mpar);
-      if (need && s <= tdc) {
-        const float dist = M::kRoot ? sqrt_approx(s) : s;
-        const float kv = (p0 + j == p_home) ? 1.0f : kernel_value_fast(kp.kernel_type, kp.kpar, kp.ginv, dist);
-        rho = fadd(rho, fmul(kv, wj));
+    const int cnt = p1 - p0;
+    stage_block<N>(sm, rec_m, p0, cnt);
+    const int jself = p_home - p0;
+    for (int j0 = 0; j0 < cnt; j0 += 8) {
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int j = j0 + u;
+        float c[N], wj;
+        smem_rec<N>(sm, j, c, wj);
+        const float s = M::partial(x, c, kp.mpar);
+        const bool in = need && j < cnt && s <= tdc;
+        if (__any_sync(0xffffffffu, in)) {
+          float kv;
+          if (FORM == kDensExpUnit) {
+            kv = ex2_approx(kexp * (M::kRoot ? sqrt_approx(s) : s));
+          } else if (FORM == kDensGauss0Unit) {
+            kv = ex2_approx(kexp * (M::kRoot ? s : s * s));
+          } else {
+            const float dist = M::kRoot ? sqrt_approx(s) : s;
+            kv = (j == jself) ? 1.0f : kernel_value_fast(kp.kernel_type, kp.kpar, kp.ginv, dist);
+          }
+          const float t = kv * wj;
+          rho = fadd(rho, in ? t : 0.0f);
+        }
       }
     }
   });
@@ -1288,11 +1348,21 @@ void launch_nh(const KParams& kp, Workspace& ws, cudaStream_t s) {
         kp, events_of(ws), ws.offsets, ws.ord_nh, ws.chunk_tile, ws.chunk_count, ws.chunk_total, ws.rec_r,
         ws.rec_m, ws.mq, ws.blk, ws.sblk, ws.minv, ws.perm, ws.nh_s, ws.delta_s, ws.status);
 }
+template <int N, int MT, int FORM>
+void launch_density_spatial_form(const KParams& kp, Workspace& ws, cudaStream_t s, float kexp) {
+  k_density_spatial<N, MT, FORM><<<chunk_grid(kp), kTileThreads, 0, s>>>(
+      kp, events_of(ws), ws.offsets, ws.ord_rho, ws.chunk_tile, ws.chunk_count, ws.chunk_total, ws.rec_w,
+      ws.rec_m, ws.mq, ws.blk, ws.sblk, ws.rec_r, ws.minv, kexp);
+}
 template <int N, int MT>
 void launch_density_spatial(const KParams& kp, Workspace& ws, cudaStream_t s) {
-  k_density_spatial<N, MT><<<chunk_grid(kp), kTileThreads, 0, s>>>(
-      kp, events_of(ws), ws.offsets, ws.ord_rho, ws.chunk_tile, ws.chunk_count, ws.chunk_total, ws.rec_w,
-      ws.rec_m, ws.mq, ws.blk, ws.sblk, ws.rec_r, ws.minv);
+  const float log2e = 1.4426950408889634f;
+  if (kp.kernel_type == CLUE_KERNEL_EXPONENTIAL && kp.kpar[1] == 1.0f)
+    launch_density_spatial_form<N, MT, kDensExpUnit>(kp, ws, s, -kp.kpar[0] * log2e);
+  else if (kp.kernel_type == CLUE_KERNEL_GAUSSIAN && kp.kpar[0] == 0.0f && kp.kpar[2] == 1.0f)
+    launch_density_spatial_form<N, MT, kDensGauss0Unit>(kp, ws, s, -kp.ginv * log2e);
+  else
+    launch_density_spatial_form<N, MT, kDensGeneric>(kp, ws, s, 0.0f);
 }
 template <int N, int MT>
 void launch_seeds(const KParams& kp, Workspace& ws, cudaStream_t s) {
