@@ -289,15 +289,19 @@ def main():
                                       "p99": float(np.percentile(ev_ms, 99))}}
 
     # ---- end to end through the C ABI with pinned host buffers ----------------
+    # inputs and the step's result (labels and seed flags, as the reference's make_clusters
+    # returns them) live in pinned host memory; densities and nearest highers stay on the device
     hc = torch.from_numpy(wl.coords).pin_memory().numpy()
     hw = torch.from_numpy(wl.weight).pin_memory().numpy()
+    hout = {k: torch.empty(n, dtype=torch.int32).pin_memory().numpy() for k in ("cluster_index", "is_seed")}
+    hncl_buf = torch.empty(E, dtype=torch.int32).pin_memory().numpy()
     for _ in range(2):
-        res, hncl = ctx.batch_host(hc, hw, offsets, params, kernel, metric, stream=sp)
+        res, hncl = ctx.batch_host(hc, hw, offsets, params, kernel, metric, stream=sp, out=hout, ncl=hncl_buf)
     e2e_ms = []
     for _ in range(args.steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        res, hncl = ctx.batch_host(hc, hw, offsets, params, kernel, metric, stream=sp)
+        res, hncl = ctx.batch_host(hc, hw, offsets, params, kernel, metric, stream=sp, out=hout, ncl=hncl_buf)
         e2e_ms.append(1e3 * (time.perf_counter() - t0))
     e2e_total = float(sum(e2e_ms))
     if world > 1:
@@ -355,7 +359,7 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config,
             "e2e": {"value": world * n * args.steps / (e2e_total / 1e3), "unit": "points/s",
                     "h2d_bytes_per_step": int(n * (ndim + 1) * 4 + 12 * E + 264 * E),
-                    "d2h_bytes_per_step": int(n * 5 * 4 + 4 * E)},
+                    "d2h_bytes_per_step": int(n * 2 * 4 + 4 * E)},
             "roofline": {"bound": "hbm", "kernel": "k_density", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": traffic, "algorithmic_bytes": B["density_kernel"], "launch_ms": dens_ms},

@@ -409,8 +409,11 @@ class Context:
         return (params.struct(), (kernel or FlatKernel(0.5)).struct(), (metric or Metric()).struct(ndim), off)
 
     def batch_host(self, coords: np.ndarray, weight: np.ndarray, event_offsets, params: Params,
-                   kernel: Kernel | None = None, metric: Metric | None = None, stream: int = 0):
-        """Cluster concatenated events (host arrays); returns (Result, n_clusters per event)."""
+                   kernel: Kernel | None = None, metric: Metric | None = None, stream: int = 0,
+                   out: dict | None = None, ncl: np.ndarray | None = None):
+        """Cluster concatenated events (host arrays); returns (Result, n_clusters per event).
+        `out` may hold preallocated host arrays (e.g. pinned) for some of cluster_index, is_seed,
+        rho, nearest_higher, delta: then only those are copied back (the others are None)."""
         c = np.ascontiguousarray(coords, dtype=np.float32)
         if c.ndim == 1:
             c = c[None, :]
@@ -418,12 +421,18 @@ class Context:
         w = np.ascontiguousarray(weight, dtype=np.float32)
         p, k, m, off = self._batch_structs(ndim, params, kernel, metric, event_offsets)
         E = len(off) - 1
-        res = Result(np.empty(n, np.int32), np.empty(n, np.int32), np.empty(n, np.float32),
-                     np.empty(n, np.int32), np.empty(n, np.float32))
+        names = ("cluster_index", "is_seed", "rho", "nearest_higher", "delta")
+        if out is None:
+            res = Result(np.empty(n, np.int32), np.empty(n, np.int32), np.empty(n, np.float32),
+                         np.empty(n, np.int32), np.empty(n, np.float32))
+        else:
+            res = Result(*(out.get(name) for name in names))
         out = _Outputs()
-        for name in ("cluster_index", "is_seed", "rho", "nearest_higher", "delta"):
-            setattr(out, name, getattr(res, name).ctypes.data)
-        ncl = np.empty(E, np.int32)
+        for name in names:
+            a = getattr(res, name)
+            setattr(out, name, a.ctypes.data if a is not None else None)
+        if ncl is None:
+            ncl = np.empty(E, np.int32)
         info = _RunInfo()
         check(lib.clue_batch_make_clusters(self.handle, ctypes.byref(p), ctypes.byref(k), ctypes.byref(m), ndim,
                                            E, off.ctypes.data, c.ctypes.data, w.ctypes.data, ctypes.byref(out),

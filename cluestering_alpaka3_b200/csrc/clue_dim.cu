@@ -289,14 +289,17 @@ __device__ __forceinline__ void bcast_rec(const float* mine, int j, float* c, fl
 // A block of up to 32 consecutive records staged in the warp's shared-memory slot: lane k
 // copies record p0 + k; smem_rec() then reads record j with broadcast loads (every lane reads
 // the same address), one 16-byte load per record word.
+// With sq / mq given, the records' tile-sorted positions mq[p0 + k] are staged in sq as well.
 template <int N>
-__device__ __forceinline__ void stage_block(float4* sm, const float4* __restrict__ rec, int p0, int cnt) {
+__device__ __forceinline__ void stage_block(float4* sm, const float4* __restrict__ rec, int p0, int cnt,
+                                            int32_t* sq = nullptr, const int32_t* __restrict__ mq = nullptr) {
   constexpr int W = Rec<N>::kWords;
   const int lane = threadIdx.x & 31;
   __syncwarp();  // the previous block's readers are done
   if (lane < cnt) {
 #pragma unroll
     for (int k = 0; k < W; ++k) sm[lane * W + k] = __ldg(rec + (size_t)(p0 + lane) * W + k);
+    if (sq) sq[lane] = __ldg(mq + p0 + lane);
   }
   __syncwarp();
 }
@@ -1077,27 +1080,30 @@ __global__ void __launch_bounds__(kTileThreads, N <= 2 ? 8 : (N <= 4 ? 6 : 4)) k
   if (!__any_sync(0xffffffffu, valid)) return;
   const float tdm = kp.t_dm;
   __shared__ float4 s_rec[kTileThreads / 32][32 * Rec<N>::kWords];
+  __shared__ int32_t s_q[kTileThreads / 32][32];
   float4* sm = s_rec[threadIdx.x >> 5];
+  int32_t* sq = s_q[threadIdx.x >> 5];
   const float slack = M::kRoot ? 1.0f + 1.0f / 524288.0f : 1.0f;  // s range of one rounded distance
-  float delta = FLT_MAX, s_best = INFINITY, rho_best = 0.0f;
+  float delta = FLT_MAX, rho_best = 0.0f;
+  // Candidates beyond bnd cannot be nearer than the best so far (nor within dm): its distance
+  // would round above delta.
+  float bnd = tdm;
   int nh = -1, orig_best = INT_MAX;
   uint64_t rank_best = ~0ull;
   spatial_sweep<N, M, true>(kp, h.g, off, hb, lo, hi, valid, x, blk, sblk, rho_i, minv[pos],
-                      [&]() { return s_best < INFINITY ? fminf(tdm, s_best * slack) : tdm; },
+                      [&]() { return bnd; },
                       [&](int p0, int p1, bool need, int64_t lexpos) {
-    const float bound = s_best < INFINITY ? fminf(tdm, s_best * slack) : tdm;
     const int cnt = p1 - p0;
-    stage_block<N>(sm, rec_m, p0, cnt);
+    stage_block<N>(sm, rec_m, p0, cnt, sq, mq);
     for (int j0 = 0; j0 < cnt; j0 += 4) {
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       const int j = j0 + u;
-      const int p = p0 + j;
       float c[N], rho_j;
       smem_rec<N>(sm, j, c, rho_j);
       const float s = M::partial(x, c, kp.mpar);
-      if (need && j < cnt && s <= tdm && s <= bound && rho_j >= rho_i) {
-        const int q = __ldg(mq + p);
+      if (need && j < cnt && s <= bnd && rho_j >= rho_i) {
+        const int q = sq[j];
         int orig_j = -1;
         bool higher = rho_j > rho_i;
         if (!higher && rho_j > 0.0f) {
@@ -1119,7 +1125,7 @@ __global__ void __launch_bounds__(kTileThreads, N <= 2 ? 8 : (N <= 4 ? 6 : 4)) k
           }
           if (better) {
             delta = dist;
-            s_best = s;
+            bnd = fminf(tdm, s * slack);
             nh = q;
             rank_best = rank;
             rho_best = rho_j;
