@@ -1095,14 +1095,11 @@ __global__ void __launch_bounds__(kTileThreads, N <= 2 ? 8 : (N <= 4 ? 6 : 4)) k
                       [&](int p0, int p1, bool need, int64_t lexpos) {
     const int cnt = p1 - p0;
     stage_block<N>(sm, rec_m, p0, cnt, sq, mq);
-    for (int j0 = 0; j0 < cnt; j0 += 4) {
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int j = j0 + u;
+    auto pair = [&](int j, bool in_block) {
       float c[N], rho_j;
       smem_rec<N>(sm, j, c, rho_j);
       const float s = M::partial(x, c, kp.mpar);
-      if (need && j < cnt && s <= bnd && rho_j >= rho_i) {
+      if (need && in_block && s <= bnd && rho_j >= rho_i) {
         const int q = sq[j];
         int orig_j = -1;
         bool higher = rho_j > rho_i;
@@ -1133,7 +1130,10 @@ __global__ void __launch_bounds__(kTileThreads, N <= 2 ? 8 : (N <= 4 ? 6 : 4)) k
           }
         }
       }
-    }
+    };
+    for (int j0 = 0; j0 < cnt; j0 += 4) {
+#pragma unroll
+      for (int u = 0; u < 4; ++u) pair(j0 + u, j0 + u < cnt);
     }
   });
   if (valid) {
@@ -1185,28 +1185,33 @@ __global__ void __launch_bounds__(kTileThreads, N <= 4 ? 8 : 4) k_density_spatia
     const int cnt = p1 - p0;
     stage_block<N>(sm, rec_m, p0, cnt);
     const int jself = p_home - p0;
-    for (int j0 = 0; j0 < cnt; j0 += 8) {
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const int j = j0 + u;
-        float c[N], wj;
-        smem_rec<N>(sm, j, c, wj);
-        const float s = M::partial(x, c, kp.mpar);
-        const bool in = need && j < cnt && s <= tdc;
-        if (__any_sync(0xffffffffu, in)) {
-          float kv;
-          if (FORM == kDensExpUnit) {
-            kv = ex2_approx(kexp * (M::kRoot ? sqrt_approx(s) : s));
-          } else if (FORM == kDensGauss0Unit) {
-            kv = ex2_approx(kexp * (M::kRoot ? s : s * s));
-          } else {
-            const float dist = M::kRoot ? sqrt_approx(s) : s;
-            kv = (j == jself) ? 1.0f : kernel_value_fast(kp.kernel_type, kp.kpar, kp.ginv, dist);
-          }
-          const float t = kv * wj;
-          rho = fadd(rho, in ? t : 0.0f);
+    auto pair = [&](int j, bool in_block) {
+      float c[N], wj;
+      smem_rec<N>(sm, j, c, wj);
+      const float s = M::partial(x, c, kp.mpar);
+      const bool in = need && in_block && s <= tdc;
+      if (__any_sync(0xffffffffu, in)) {
+        float kv;
+        if (FORM == kDensExpUnit) {
+          kv = ex2_approx(kexp * (M::kRoot ? sqrt_approx(s) : s));
+        } else if (FORM == kDensGauss0Unit) {
+          kv = ex2_approx(kexp * (M::kRoot ? s : s * s));
+        } else {
+          const float dist = M::kRoot ? sqrt_approx(s) : s;
+          kv = (j == jself) ? 1.0f : kernel_value_fast(kp.kernel_type, kp.kpar, kp.ginv, dist);
         }
+        const float t = kv * wj;
+        if (in) rho = fadd(rho, t);
       }
+    };
+    int j0 = 0;
+    for (; j0 + 8 <= cnt; j0 += 8) {
+#pragma unroll
+      for (int u = 0; u < 8; ++u) pair(j0 + u, true);
+    }
+    if (j0 < cnt) {
+#pragma unroll
+      for (int u = 0; u < 8; ++u) pair(j0 + u, j0 + u < cnt);
     }
   });
   if (valid) store_rec<N>(rec_r, pos, x, rho);

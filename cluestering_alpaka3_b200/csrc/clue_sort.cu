@@ -38,50 +38,6 @@ __global__ void __launch_bounds__(kSortThreads) k_radix_hist(const uint32_t* __r
   for (int d = threadIdx.x; d < kRadix; d += blockDim.x) hist[(size_t)d * nblocks + blockIdx.x] = h[d];
 }
 
-// Stable scatter: items are visited in index order (round-major, then warp, then lane),
-// each gets its global slot = scanned[d][block] + items of digit d before it in the block.
-__global__ void __launch_bounds__(kSortThreads) k_radix_scatter(
-    const uint32_t* __restrict__ kin, const int32_t* __restrict__ vin, uint32_t* __restrict__ kout,
-    int32_t* __restrict__ vout, int n, int shift, const uint32_t* __restrict__ scanned, int nblocks) {
-  constexpr int kWarps = kSortThreads / 32;
-  __shared__ uint32_t run[kRadix];
-  __shared__ uint32_t wcnt[kWarps][kRadix];
-  const int warp = threadIdx.x >> 5;
-  for (int d = threadIdx.x; d < kRadix; d += blockDim.x) run[d] = scanned[(size_t)d * nblocks + blockIdx.x];
-  const int base = blockIdx.x * kSortTile;
-  for (int r = 0; r < kSortItems; ++r) {
-    if (base + r * kSortThreads >= n) break;  // uniform across the block
-    for (int e = threadIdx.x; e < kWarps * kRadix; e += blockDim.x) (&wcnt[0][0])[e] = 0;
-    __syncthreads();
-    const int i = base + r * kSortThreads + threadIdx.x;
-    const bool valid = i < n;
-    const uint32_t key = valid ? kin[i] : 0u;
-    const int32_t val = valid ? (vin ? vin[i] : i) : 0;
-    const uint32_t d = valid ? (key >> shift) & (kRadix - 1) : (uint32_t)kRadix;
-    const uint32_t peers = __match_any_sync(0xffffffffu, d);
-    const uint32_t rank = __popc(peers & lanemask_lt());
-    if (valid && rank == 0) wcnt[warp][d] = __popc(peers);
-    __syncthreads();
-    for (int dd = threadIdx.x; dd < kRadix; dd += blockDim.x) {
-      uint32_t acc = run[dd];
-#pragma unroll
-      for (int w = 0; w < kWarps; ++w) {
-        const uint32_t c = wcnt[w][dd];
-        wcnt[w][dd] = acc;
-        acc += c;
-      }
-      run[dd] = acc;
-    }
-    __syncthreads();
-    if (valid) {
-      const uint32_t pos = wcnt[warp][d] + rank;
-      kout[pos] = key;
-      vout[pos] = val;
-    }
-    __syncthreads();
-  }
-}
-
 __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v) {
   const int lane = threadIdx.x & 31;
 #pragma unroll
@@ -110,6 +66,83 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* tot) {
   if (tot) *tot = ws[32];
   __syncthreads();
   return r;
+}
+
+// Stable scatter of one tile of kSortTile items.  Warp w ranks the w-th slice of the tile
+// (kSortItems steps of 32 consecutive items) against warp-private digit counters, so inside a
+// warp items keep index order without block barriers; one block-wide pass then turns the
+// per-warp counts into slice bases (digits in order, warps in order inside a digit).  Items are
+// placed digit-sorted in shared memory and written out in that order, so consecutive threads
+// write consecutive slots of a digit's run.  The tile's count of digit d is the difference of
+// consecutive entries of the digit-major scanned histogram.
+__global__ void __launch_bounds__(kSortThreads) k_radix_scatter(
+    const uint32_t* __restrict__ kin, const int32_t* __restrict__ vin, uint32_t* __restrict__ kout,
+    int32_t* __restrict__ vout, int n, int shift, const uint32_t* __restrict__ scanned, int nblocks) {
+  static_assert(kSortThreads == kRadix, "one thread per digit");
+  constexpr int kWarps = kSortThreads / 32;
+  constexpr int kSlice = kSortItems * 32;  // items per warp
+  __shared__ uint32_t s_key[kSortTile];
+  __shared__ int32_t s_val[kSortTile];
+  __shared__ uint32_t gbase[kRadix];
+  __shared__ uint32_t wcnt[kWarps][kRadix];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int base = blockIdx.x * kSortTile;
+  const int tile_n = min(kSortTile, n - base);
+  for (int e = threadIdx.x; e < kWarps * kRadix; e += blockDim.x) (&wcnt[0][0])[e] = 0;
+  uint32_t dstart;
+  {
+    const int d = threadIdx.x;
+    const size_t idx = (size_t)d * nblocks + blockIdx.x;
+    const uint32_t first = scanned[idx];
+    const uint32_t next = idx + 1 < (size_t)kRadix * nblocks ? scanned[idx + 1] : (uint32_t)n;
+    dstart = block_excl_scan(next - first, nullptr);  // ends with a block barrier
+    gbase[d] = first - dstart;
+  }
+  uint32_t key[kSortItems], off[kSortItems];
+  int32_t val[kSortItems];
+  const uint32_t lt = lanemask_lt();
+#pragma unroll
+  for (int r = 0; r < kSortItems; ++r) {
+    const int k = warp * kSlice + r * 32 + lane;
+    const bool valid = k < tile_n;
+    key[r] = valid ? kin[base + k] : 0u;
+    val[r] = valid ? (vin ? vin[base + k] : base + k) : 0;
+    const uint32_t d = valid ? (key[r] >> shift) & (kRadix - 1) : (uint32_t)kRadix;
+    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    const uint32_t rank = __popc(peers & lt);
+    off[r] = valid ? wcnt[warp][d] + rank : 0u;
+    __syncwarp();
+    if (valid && rank == 0) wcnt[warp][d] += __popc(peers);
+    __syncwarp();
+  }
+  __syncthreads();
+  {
+    const int d = threadIdx.x;
+    uint32_t acc = dstart;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+      const uint32_t c = wcnt[w][d];
+      wcnt[w][d] = acc;
+      acc += c;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < kSortItems; ++r) {
+    const int k = warp * kSlice + r * 32 + lane;
+    if (k < tile_n) {
+      const uint32_t pos = wcnt[warp][(key[r] >> shift) & (kRadix - 1)] + off[r];
+      s_key[pos] = key[r];
+      s_val[pos] = val[r];
+    }
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < tile_n; k += kSortThreads) {
+    const uint32_t kk = s_key[k];
+    const uint32_t g = gbase[(kk >> shift) & (kRadix - 1)] + (uint32_t)k;
+    kout[g] = kk;
+    vout[g] = s_val[k];
+  }
 }
 
 __global__ void __launch_bounds__(kScanThreads) k_scan_reduce(const uint32_t* __restrict__ in, size_t len,

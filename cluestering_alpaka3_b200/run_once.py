@@ -32,6 +32,8 @@ def main():
     ap.add_argument("--workload", default="calo4096",
                     choices=["calo4096", "blobs2d_16k", "blobs2d_1m", "blobs3d_4m"])
     ap.add_argument("--passes", type=int, default=2)
+    ap.add_argument("--stages", action="store_true",
+                    help="time the four stages with CUDA events and print their medians")
     args = ap.parse_args()
 
     import torch
@@ -49,6 +51,9 @@ def main():
              ("nearest_higher", torch.int32), ("delta", torch.float32))}
     optr = {k: v.data_ptr() for k, v in outs.items()}
     stream = torch.cuda.Stream()
+    if args.stages:
+        ctx.set_timing(True)
+    stage_ms = []
     for p in range(args.passes):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -57,6 +62,12 @@ def main():
         stream.synchronize()
         print(f"pass {p}: {1e3 * (time.perf_counter() - t0):.3f} ms wall, {n} points, "
               f"{len(off) - 1} events", flush=True)
+        if args.stages:
+            stage_ms.append(ctx.stage_times())
+    if args.stages and stage_ms:
+        med = np.median(np.array(stage_ms), axis=0)
+        print("stage ms (median): tiles %.3f density %.3f nearest_higher %.3f seeds_labels %.3f total %.3f"
+              % (med[0], med[1], med[2], med[3], med.sum()), flush=True)
     info = ctx.read_info(stream.cuda_stream)
     print(f"clusters {info.n_clusters}, seeds {info.n_seeds}")
     ctx.close()
