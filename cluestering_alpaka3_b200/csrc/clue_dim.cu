@@ -1084,7 +1084,7 @@ __global__ void __launch_bounds__(kTileThreads, N <= 2 ? 8 : (N <= 4 ? 6 : 4)) k
   float4* sm = s_rec[threadIdx.x >> 5];
   int32_t* sq = s_q[threadIdx.x >> 5];
   const float slack = M::kRoot ? 1.0f + 1.0f / 524288.0f : 1.0f;  // s range of one rounded distance
-  float delta = FLT_MAX, rho_best = 0.0f;
+  float s_best = INFINITY, rho_best = 0.0f;  // metric value of the nearest higher so far
   // Candidates beyond bnd cannot be nearer than the best so far (nor within dm): its distance
   // would round above delta.
   float bnd = tdm;
@@ -1108,20 +1108,25 @@ __global__ void __launch_bounds__(kTileThreads, N <= 2 ? 8 : (N <= 4 ? 6 : 4)) k
           higher = orig_j > orig_i;
         }
         if (higher) {
-          const float dist = M::finish(s);
           const uint64_t rank = ((uint64_t)lexpos << 32) | (uint32_t)q;
           bool better;
-          if (TIE == CLUE_TIE_REFERENCE) {
-            better = dist < delta || (dist == delta && rank < rank_best);
-          } else if (dist == delta && nh >= 0) {
-            if (orig_j < 0) orig_j = __ldg(perm + q);
-            if (orig_best < 0) orig_best = __ldg(perm + nh);
-            better = rho_j > rho_best || (rho_j == rho_best && orig_j < orig_best);
+          if (s * slack < s_best) {
+            better = true;  // its distance rounds strictly below the best one's
           } else {
-            better = dist < delta;
+            // the two distances may round to the same value: decide on the rounded distances
+            const float dist = M::finish(s), dbest = M::finish(s_best);
+            if (TIE == CLUE_TIE_REFERENCE) {
+              better = dist < dbest || (dist == dbest && rank < rank_best);
+            } else if (dist == dbest && nh >= 0) {
+              if (orig_j < 0) orig_j = __ldg(perm + q);
+              if (orig_best < 0) orig_best = __ldg(perm + nh);
+              better = rho_j > rho_best || (rho_j == rho_best && orig_j < orig_best);
+            } else {
+              better = dist < dbest;
+            }
           }
           if (better) {
-            delta = dist;
+            s_best = s;
             bnd = fminf(tdm, s * slack);
             nh = q;
             rank_best = rank;
@@ -1138,7 +1143,7 @@ __global__ void __launch_bounds__(kTileThreads, N <= 2 ? 8 : (N <= 4 ? 6 : 4)) k
   });
   if (valid) {
     nh_s[pos] = nh;
-    delta_s[pos] = delta;
+    delta_s[pos] = nh >= 0 ? M::finish(s_best) : FLT_MAX;
   }
   const uint32_t none = __ballot_sync(0xffffffffu, valid && nh < 0);
   if ((threadIdx.x & 31) == 0 && none) {
