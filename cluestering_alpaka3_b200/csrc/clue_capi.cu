@@ -145,6 +145,9 @@ std::vector<ArenaItem> arena_items(Workspace& nw, void** evtab, size_t n, size_t
       {(void**)&nw.chunk_count, (ntiles + 1) * 4},
       {(void**)&nw.chunk_tile, (n / kChunkPoints + ntiles + 1) * 4},
       {(void**)&nw.chunk_total, 16},
+      {(void**)&nw.tblk, std::min(n, n / 32 + ntiles + 1) * 2 * w * 16},
+      {(void**)&nw.tblk_off, (ntiles + 1) * 4},
+      {(void**)&nw.rho_fix, n * 8},
   };
 }
 

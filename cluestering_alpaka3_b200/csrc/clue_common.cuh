@@ -75,6 +75,7 @@ struct EvGrid {
   int32_t pt_base;          // first point of the event
   int32_t pt_count;
   uint32_t seed_candidates; // points of the event without nearest higher
+  uint32_t wmax_bits;       // largest |weight| of the event (float bits; non-negative floats order as integers)
 };
 
 // Device-side status block (counters and flags), read back once per call.

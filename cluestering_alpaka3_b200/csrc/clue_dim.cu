@@ -482,6 +482,7 @@ __global__ void k_init(const KParams kp, Events ev, int32_t* ev_pt, int32_t* ev_
       g.enc_max[d] = 0u;
     }
     g.seed_candidates = 0;
+    g.wmax_bits = 0u;
     if (kp.n_events == 1) {
       g.nperdim = kp.nperdim0;
       g.ntiles = kp.ntiles;
@@ -507,6 +508,7 @@ __global__ void __launch_bounds__(256) k_bbox_single(InPtrs in, int n, EvGrid* g
     emx[d] = 0u;
   }
   bool bad = false;
+  uint32_t wmax = 0u;
   const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
 #pragma unroll
@@ -517,19 +519,23 @@ __global__ void __launch_bounds__(256) k_bbox_single(InPtrs in, int n, EvGrid* g
       emn[d] = min(emn[d], e);
       emx[d] = max(emx[d], e);
     }
-    bad |= !isfinite(in.w[i]);
+    const float w = in.w[i];
+    bad |= !isfinite(w);
+    wmax = max(wmax, __float_as_uint(fabsf(w)));
   }
 #pragma unroll
   for (int d = 0; d < N; ++d) {
     emn[d] = warp_min_u(emn[d]);
     emx[d] = warp_max_u(emx[d]);
   }
+  wmax = warp_max_u(wmax);
   if ((threadIdx.x & 31) == 0) {
 #pragma unroll
     for (int d = 0; d < N; ++d) {
       atomicMin(&g->enc_min[d], emn[d]);
       atomicMax(&g->enc_max[d], emx[d]);
     }
+    atomicMax(&g->wmax_bits, wmax);
   }
   if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&st->nonfinite, 1u);
 }
@@ -537,7 +543,7 @@ __global__ void __launch_bounds__(256) k_bbox_single(InPtrs in, int n, EvGrid* g
 // Bounding box of many events: one CTA per event (grid-stride over events).
 template <int N>
 __global__ void __launch_bounds__(256) k_bbox_events(InPtrs in, int E, EvGrid* eg, DevStatus* st) {
-  __shared__ uint32_t s_mn[8][N], s_mx[8][N];
+  __shared__ uint32_t s_mn[8][N], s_mx[8][N], s_w[8];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int e = blockIdx.x; e < E; e += gridDim.x) {
     const int b = eg[e].pt_base, cnt = eg[e].pt_count;
@@ -548,6 +554,7 @@ __global__ void __launch_bounds__(256) k_bbox_events(InPtrs in, int E, EvGrid* e
       emx[d] = 0u;
     }
     bool bad = false;
+    uint32_t wmax = 0u;
     for (int i = b + threadIdx.x; i < b + cnt; i += blockDim.x) {
 #pragma unroll
       for (int d = 0; d < N; ++d) {
@@ -557,19 +564,23 @@ __global__ void __launch_bounds__(256) k_bbox_events(InPtrs in, int E, EvGrid* e
         emn[d] = min(emn[d], en);
         emx[d] = max(emx[d], en);
       }
-      bad |= !isfinite(in.w[i]);
+      const float w = in.w[i];
+      bad |= !isfinite(w);
+      wmax = max(wmax, __float_as_uint(fabsf(w)));
     }
 #pragma unroll
     for (int d = 0; d < N; ++d) {
       emn[d] = warp_min_u(emn[d]);
       emx[d] = warp_max_u(emx[d]);
     }
+    wmax = warp_max_u(wmax);
     if (lane == 0) {
 #pragma unroll
       for (int d = 0; d < N; ++d) {
         s_mn[warp][d] = emn[d];
         s_mx[warp][d] = emx[d];
       }
+      s_w[warp] = wmax;
     }
     if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(&st->nonfinite, 1u);
     __syncthreads();
@@ -582,6 +593,11 @@ __global__ void __launch_bounds__(256) k_bbox_events(InPtrs in, int E, EvGrid* e
       }
       eg[e].enc_min[d] = a;
       eg[e].enc_max[d] = z;
+    }
+    if (threadIdx.x == 0) {
+      uint32_t m = 0u;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = max(m, s_w[w]);
+      eg[e].wmax_bits = m;
     }
     __syncthreads();
   }
@@ -706,7 +722,8 @@ __global__ void __launch_bounds__(kTileThreads) k_order(const KParams kp, Events
                                                         const float4* __restrict__ rec_w,
                                                         const int32_t* __restrict__ mq,
                                                         int32_t* __restrict__ ord_rho, int32_t* __restrict__ ord_nh,
-                                                        uint32_t* __restrict__ chunk_count) {
+                                                        uint32_t* __restrict__ chunk_count,
+                                                        uint32_t* __restrict__ blk_count) {
   constexpr int K = N <= 4 ? (1 << (2 * N)) : 1;
   __shared__ uint32_t s_cnt[kChunkWarps][2][K];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -715,7 +732,10 @@ __global__ void __launch_bounds__(kTileThreads) k_order(const KParams kp, Events
   const float rad[2] = {kp.dc, kp.dm};
   for (int t = blockIdx.x; t < kp.ntiles; t += gridDim.x) {
     const int beg = off[t], end = off[t + 1];
-    if (threadIdx.x == 0) chunk_count[t] = (uint32_t)((end - beg + kChunk - 1) / kChunk);
+    if (threadIdx.x == 0) {
+      chunk_count[t] = (uint32_t)((end - beg + kChunk - 1) / kChunk);
+      if (blk_count) blk_count[t] = (uint32_t)((end - beg + 31) / 32);
+    }
     if (beg == end) continue;
     const EvGrid* g = ev.eg + find_event(ev.tile, kp.n_events, t);
     int hb[N];
@@ -1222,6 +1242,203 @@ __global__ void __launch_bounds__(kTileThreads, N <= 4 ? 8 : 4) k_density_spatia
   if (valid) store_rec<N>(rec_r, pos, x, rho);
 }
 
+// ---- symmetric spatial density -------------------------------------------------
+// For metrics whose value bounds every coordinate difference (Euclidean, Manhattan, Chebyshev)
+// and no wrapped coordinate, d(i, j) <= dc already places j's tile inside i's search box, so the
+// candidate set is {j : d(i, j) <= dc} and every pair can be evaluated once for both points.
+// Blocks are 32 consecutive Morton-ordered records counted from their tile's start (so the
+// result does not depend on where a tile lies in a batch): block slot 4 c + w is warp w of
+// chunk c.  The warp of block A evaluates A against itself one-sidedly and every block B of its
+// tile after A and of the later tiles of its search-box union both ways: the candidate records
+// rotate through the lanes, each lane adding K(d) w_j to its own sum and K(d) w_i to the
+// travelling candidate's sum, which is then added in fixed point (exact integer adds, so the
+// order of arrival does not matter) to the candidate's accumulator.
+
+// Block boxes in compact order: block b of tile u is entry bo[u] + b (bo = exclusive scan of
+// the tiles' block counts).  One thread per (chunk, warp) slot; slots past a tile's end write
+// nothing.
+template <int N>
+__global__ void __launch_bounds__(256) k_tblock_bbox(int max_slots, const uint32_t* __restrict__ chunk_total,
+                                                    const int32_t* __restrict__ off,
+                                                    const int32_t* __restrict__ chunk_tile,
+                                                    const uint32_t* __restrict__ chunk_off,
+                                                    const uint32_t* __restrict__ bo,
+                                                    const float4* __restrict__ rec_m, float4* __restrict__ tblk) {
+  constexpr int BW = Blk<N>::kWords;
+  const int nslots = min(max_slots, 4 * (int)*chunk_total);
+  const int stride = gridDim.x * blockDim.x;
+  for (int sl = blockIdx.x * blockDim.x + threadIdx.x; sl < nslots; sl += stride) {
+    const int c = sl >> 2;
+    const int t = chunk_tile[c];
+    const int b = ((c - (int)chunk_off[t]) << 2) + (sl & 3);
+    const int first = off[t] + (b << 5);
+    const int cnt = min(32, off[t + 1] - first);
+    if (cnt <= 0) continue;
+    float bb[4 * BW];
+#pragma unroll
+    for (int d = 0; d < N; ++d) {
+      bb[d] = INFINITY;
+      bb[N + d] = -INFINITY;
+    }
+#pragma unroll
+    for (int k = 2 * N; k < 4 * BW; ++k) bb[k] = 0.0f;
+    for (int r = 0; r < cnt; ++r) {
+      float x[N], pl;
+      load_rec<N>(rec_m, first + r, x, pl);
+#pragma unroll
+      for (int d = 0; d < N; ++d) {
+        bb[d] = fminf(bb[d], x[d]);
+        bb[N + d] = fmaxf(bb[N + d], x[d]);
+      }
+    }
+    const size_t id = (size_t)bo[t] + b;
+#pragma unroll
+    for (int k = 0; k < BW; ++k)
+      tblk[id * BW + k] = make_float4(bb[4 * k], bb[4 * k + 1], bb[4 * k + 2], bb[4 * k + 3]);
+  }
+}
+
+// Fixed-point exponent of an event: contributions times 2^F stay below 2^61 in total
+// (|sum| <= count * max|w| * max kernel value).
+__device__ __forceinline__ int fix_exponent(const EvGrid* g, float kmax) {
+  const float bound = __uint_as_float(g->wmax_bits) * (float)g->pt_count * kmax;
+  int e = 0;
+  frexpf(bound, &e);  // bound < 2^e
+  return max(-126, min(126, 61 - e));
+}
+
+template <int N, int MT, int FORM>
+__global__ void __launch_bounds__(kTileThreads, N <= 4 ? 8 : 4) k_density_sym(
+    const KParams kp, Events ev, const int32_t* __restrict__ off, const int32_t* __restrict__ chunk_tile,
+    const uint32_t* __restrict__ chunk_off, const uint32_t* __restrict__ chunk_total,
+    const float4* __restrict__ rec_m, const int32_t* __restrict__ mq, const uint32_t* __restrict__ bo,
+    const float4* __restrict__ tblk, float4* __restrict__ rec_r, int64_t* __restrict__ rho_fix, float kexp,
+    float kmax) {
+  using M = Metric<N, MT>;
+  constexpr int BW = Blk<N>::kWords;
+  __shared__ float4 s_rec[kTileThreads / 32][32 * Rec<N>::kWords];
+  const int c = blockIdx.x;
+  if (c >= (int)*chunk_total) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int t = chunk_tile[c];
+  const int a_loc = ((c - (int)chunk_off[t]) << 2) + warp;  // block of the tile
+  const int startA = off[t] + (a_loc << 5);
+  const int cntA = min(32, off[t + 1] - startA);
+  if (cntA <= 0) return;  // whole warp: this block of the chunk is past the tile's end
+  const EvGrid* g = ev.eg + find_event(ev.tile, kp.n_events, t);
+  const bool hv = lane < cntA;
+  const int pA = startA + (hv ? lane : 0);
+  float x[N], wi;
+  load_rec<N>(rec_m, pA, x, wi);
+  int hb[N], lo[N], hi[N];
+  home_bins<N>(g, t, hb);
+  lane_box<N>(kp, g, x, kp.dc, hb, lo, hi);
+  int wl[N], wh[N];
+#pragma unroll
+  for (int d = 0; d < N; ++d) {
+    wl[d] = warp_min_i(hv ? lo[d] : INT_MAX);
+    wh[d] = warp_max_i(hv ? hi[d] : INT_MIN);
+  }
+  const float tdc = kp.t_dc;
+  const float scale = ldexpf(1.0f, fix_exponent(g, kmax));
+  auto kval = [&](float s, bool self) -> float {
+    if (FORM == kDensExpUnit) return ex2_approx(kexp * (M::kRoot ? sqrt_approx(s) : s));
+    if (FORM == kDensGauss0Unit) return ex2_approx(kexp * (M::kRoot ? s : s * s));
+    const float dist = M::kRoot ? sqrt_approx(s) : s;
+    return self ? 1.0f : kernel_value_fast(kp.kernel_type, kp.kpar, kp.ginv, dist);
+  };
+  float acc = 0.0f;
+  // block A against itself, one-sided (the self pair gives the reference's self term)
+  {
+    float4* sm = s_rec[warp];
+    stage_block<N>(sm, rec_m, startA, cntA);
+    for (int j = 0; j < cntA; ++j) {
+      float cx[N], wj;
+      smem_rec<N>(sm, j, cx, wj);
+      const float sd = M::partial(x, cx, kp.mpar);
+      const bool in = hv && sd <= tdc;
+      if (__any_sync(0xffffffffu, in)) {
+        const float t2 = kval(sd, j == lane) * wj;
+        if (in) acc = fadd(acc, t2);
+      }
+    }
+  }
+  // later blocks of the own tile, then the later tiles of the union box, both ways
+  int v[N];
+#pragma unroll
+  for (int d = 0; d < N; ++d) v[d] = wl[d];
+  while (true) {
+    int u = g->tile_base;
+#pragma unroll
+    for (int d = 0; d < N; ++d) u += g->stride[d] * v[d];
+    if (u >= t) {
+      const int pb = off[u], pe = off[u + 1];
+      const int nb = (pe - pb + 31) >> 5;
+      for (int b = (u == t ? a_loc + 1 : 0); b < nb; ++b) {
+        float bb[4 * BW];
+        load_box<N>(tblk, (int)bo[u] + b, bb);
+        const bool need = hv && M::lower(x, bb, bb + N, kp.mpar) <= tdc;
+        if (!__any_sync(0xffffffffu, need)) continue;
+        const int first = pb + (b << 5);
+        const int cntB = min(32, pe - first);
+        const bool cv = lane < cntB;
+        float cx[N], cw;
+        load_rec<N>(rec_m, first + (cv ? lane : 0), cx, cw);
+        if (!cv) {
+#pragma unroll
+          for (int d = 0; d < N; ++d) cx[d] = INFINITY;  // never within dc
+          cw = 0.0f;
+        }
+        float cacc = 0.0f;
+        const int src = (lane + 1) & 31;
+        for (int k = 0; k < 32; ++k) {
+          const float sd = M::partial(x, cx, kp.mpar);
+          const bool in = hv && sd <= tdc;
+          if (__any_sync(0xffffffffu, in)) {
+            const float kv = kval(sd, false);
+            if (in) {
+              acc = fadd(acc, kv * cw);
+              cacc = fadd(cacc, kv * wi);
+            }
+          }
+#pragma unroll
+          for (int d = 0; d < N; ++d) cx[d] = __shfl_sync(0xffffffffu, cx[d], src);
+          cw = __shfl_sync(0xffffffffu, cw, src);
+          cacc = __shfl_sync(0xffffffffu, cacc, src);
+        }
+        if (cv && cacc != 0.0f)
+          atomicAdd(reinterpret_cast<unsigned long long*>(rho_fix + mq[first + lane]),
+                    (unsigned long long)__float2ll_rn(cacc * scale));
+      }
+    }
+    int d = N - 1;
+    for (; d >= 0; --d) {
+      if (v[d] < wh[d]) {
+        ++v[d];
+        break;
+      }
+      v[d] = wl[d];
+    }
+    if (d < 0) break;
+  }
+  if (hv) store_rec<N>(rec_r, mq[pA], x, acc);
+}
+
+// rho = own-side sum + the fixed-point sum of the contributions received as a candidate.
+template <int N>
+__global__ void __launch_bounds__(256) k_density_combine(const KParams kp, Events ev, int n,
+                                                         const int64_t* __restrict__ rho_fix,
+                                                         float4* __restrict__ rec_r, float kmax) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride) {
+    const EvGrid* g = ev.eg + find_event(ev.pt, kp.n_events, q);
+    float x[N], acc;
+    load_rec<N>(rec_r, q, x, acc);
+    const float recv = (float)((double)rho_fix[q] * ldexp(1.0, -fix_exponent(g, kmax)));
+    store_rec<N>(rec_r, q, x, fadd(acc, recv));
+  }
+}
+
 // ---- stage 4: seeds (KernelFindClusters) ---------------------------------------
 template <int N, int MT>
 __global__ void __launch_bounds__(256) k_seeds(const KParams kp, int n, const float4* __restrict__ rec_r,
@@ -1380,6 +1597,47 @@ void launch_density_spatial(const KParams& kp, Workspace& ws, cudaStream_t s) {
   else
     launch_density_spatial_form<N, MT, kDensGeneric>(kp, ws, s, 0.0f);
 }
+// Symmetric density: kernel form and largest kernel value (the self term is 1).
+template <int N, int MT, int FORM>
+void launch_density_sym_form(const KParams& kp, Workspace& ws, cudaStream_t s, float kexp, float kmax) {
+  k_density_sym<N, MT, FORM><<<chunk_grid(kp), kTileThreads, 0, s>>>(
+      kp, events_of(ws), ws.offsets, ws.chunk_tile, ws.chunk_count, ws.chunk_total, ws.rec_m, ws.mq, ws.tblk_off,
+      ws.tblk, ws.rec_r, ws.rho_fix, kexp, kmax);
+}
+template <int N, int MT>
+void launch_density_sym(const KParams& kp, Workspace& ws, cudaStream_t s) {
+  const float log2e = 1.4426950408889634f;
+  float kmax = 1.0f;
+  if (kp.kernel_type == CLUE_KERNEL_FLAT) kmax = fmaxf(1.0f, fabsf(kp.kpar[0]));
+  if (kp.kernel_type == CLUE_KERNEL_EXPONENTIAL) kmax = fmaxf(1.0f, fabsf(kp.kpar[1]));
+  if (kp.kernel_type == CLUE_KERNEL_GAUSSIAN) kmax = fmaxf(1.0f, fabsf(kp.kpar[2]));
+  cudaMemsetAsync(ws.rho_fix, 0, (size_t)kp.n * sizeof(int64_t), s);
+  if (kp.kernel_type == CLUE_KERNEL_EXPONENTIAL && kp.kpar[1] == 1.0f)
+    launch_density_sym_form<N, MT, kDensExpUnit>(kp, ws, s, -kp.kpar[0] * log2e, kmax);
+  else if (kp.kernel_type == CLUE_KERNEL_GAUSSIAN && kp.kpar[0] == 0.0f && kp.kpar[2] == 1.0f)
+    launch_density_sym_form<N, MT, kDensGauss0Unit>(kp, ws, s, -kp.ginv * log2e, kmax);
+  else
+    launch_density_sym_form<N, MT, kDensGeneric>(kp, ws, s, 0.0f, kmax);
+  k_density_combine<N><<<grid_for(kp.n, 256), 256, 0, s>>>(kp, events_of(ws), kp.n, ws.rho_fix, ws.rec_r, kmax);
+}
+// The symmetric sweep covers exactly the reference's candidates when the metric bounds every
+// coordinate difference and no coordinate wraps.
+inline bool symmetric_density_ok(const KParams& kp, int metric, int ndim) {
+  if (metric != CLUE_METRIC_EUCLIDEAN && metric != CLUE_METRIC_MANHATTAN && metric != CLUE_METRIC_CHEBYSHEV)
+    return false;
+  for (int d = 0; d < ndim; ++d)
+    if (kp.wrapped[d]) return false;
+  return true;
+}
+template <int N>
+void launch_density_sym_metric(int metric, const KParams& kp, Workspace& ws, cudaStream_t s) {
+  if (metric == CLUE_METRIC_MANHATTAN)
+    launch_density_sym<N, CLUE_METRIC_MANHATTAN>(kp, ws, s);
+  else if (metric == CLUE_METRIC_CHEBYSHEV)
+    launch_density_sym<N, CLUE_METRIC_CHEBYSHEV>(kp, ws, s);
+  else
+    launch_density_sym<N, CLUE_METRIC_EUCLIDEAN>(kp, ws, s);
+}
 template <int N, int MT>
 void launch_seeds(const KParams& kp, Workspace& ws, cudaStream_t s) {
   k_seeds<N, MT><<<grid_for(kp.n, 256), 256, 0, s>>>(kp, kp.n, ws.rec_r, ws.nh_s, ws.perm, ws.is_seed_s, ws.par,
@@ -1447,19 +1705,29 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
     ws.minv = mvals[mc ^ 1];
     k_invert<<<grid_for(n, 256), 256, 0, s>>>(ws.mq, n, ws.minv);
   }
-  k_order<N><<<kp.ntiles, kTileThreads, 0, s>>>(kp, ev, ws.offsets, ws.rec_w, ws.mq, ws.ord_rho, ws.ord_nh,
-                                                ws.chunk_count);
-  exclusive_scan(ws.chunk_count, ws.chunk_count, (size_t)kp.ntiles, ws.scan_scratch, ws.chunk_total, s);
-  k_chunk_map<<<grid_for(kp.ntiles, 256), 256, 0, s>>>(kp.ntiles, ws.offsets, ws.chunk_count, ws.chunk_tile);
-
   // density order: the reference's candidate order for the flat kernel (bit-exact sums), spatial
   // order for the exponential and Gaussian kernels (whose device expf already differs from the
   // host's by an ulp) unless the caller asks for the reference order
   const bool spatial_density = (kp.flags & CLUE_FLAG_REFERENCE_ORDER) == 0 &&
                                (kp.kernel_type != CLUE_KERNEL_FLAT || (kp.flags & CLUE_FLAG_SPATIAL_DENSITY) != 0);
+  // (a workspace without the symmetric sweep's buffers, such as the fixed scratch of the
+  // no-allocation entry point, keeps the one-sided sweep)
+  const bool symmetric =
+      spatial_density && symmetric_density_ok(kp, a.metric, N) && ws.tblk && ws.tblk_off && ws.rho_fix;
+  k_order<N><<<kp.ntiles, kTileThreads, 0, s>>>(kp, ev, ws.offsets, ws.rec_w, ws.mq, ws.ord_rho, ws.ord_nh,
+                                                ws.chunk_count, symmetric ? ws.tblk_off : nullptr);
+  exclusive_scan(ws.chunk_count, ws.chunk_count, (size_t)kp.ntiles, ws.scan_scratch, ws.chunk_total, s);
+  if (symmetric) exclusive_scan(ws.tblk_off, ws.tblk_off, (size_t)kp.ntiles, ws.scan_scratch, nullptr, s);
+  k_chunk_map<<<grid_for(kp.ntiles, 256), 256, 0, s>>>(kp.ntiles, ws.offsets, ws.chunk_count, ws.chunk_tile);
+
   const int nblk_threads = ((n + 31) >> 5) * 32;
   const int nsb_threads = ((((n + 31) >> 5) + 31) >> 5) * 32;
-  if (spatial_density) {
+  const int max_slots = 4 * (n / kChunk + kp.ntiles + 1);
+  if (symmetric) {
+    k_gather_morton<N><<<grid_for(n, 256), 256, 0, s>>>(ws.rec_w, n, ws.mq, ws.rec_m);
+    k_tblock_bbox<N><<<grid_for(max_slots, 256), 256, 0, s>>>(max_slots, ws.chunk_total, ws.offsets, ws.chunk_tile,
+                                                               ws.chunk_count, ws.tblk_off, ws.rec_m, ws.tblk);
+  } else if (spatial_density) {
     k_gather_morton<N><<<grid_for(n, 256), 256, 0, s>>>(ws.rec_w, n, ws.mq, ws.rec_m);
     k_block_bbox<N><<<grid_for(nblk_threads, 256), 256, 0, s>>>(ws.rec_m, n, ws.blk);
     k_superblock_bbox<N><<<grid_for(nsb_threads, 256), 256, 0, s>>>(ws.blk, n, ws.sblk);
@@ -1468,7 +1736,9 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
   }
 
   stage_mark(ws, 1, s);
-  if (spatial_density) {
+  if (symmetric) {
+    launch_density_sym_metric<N>(a.metric, kp, ws, s);
+  } else if (spatial_density) {
     CLUE_METRIC_SWITCH(a.metric, launch_density_spatial, kp, ws, s);
   } else {
     CLUE_METRIC_SWITCH(a.metric, launch_density, kp, ws, s);
@@ -1495,7 +1765,8 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
   // finalize, event info
   ws.launches += 4 + radix_sort_launches(bits) + 2 + 1 + radix_sort_launches(MortonBits<N>::kBits) + 1 +
                  radix_sort_launches(bits) + 1 + 1 + kScanLaunches + 1 +
-                 (spatial_density ? 3 : 1) + 1 + 3 + 1 + 2 + kScanLaunches + kJumpLaunches + 1 + 1;
+                 (symmetric ? 2 + kScanLaunches : (spatial_density ? 3 : 1)) + (symmetric ? 2 : 1) + 3 + 1 + 2 +
+                 kScanLaunches + kJumpLaunches + 1 + 1;
   CLUE_CUDA_TRY(cudaGetLastError());
   return CLUE_OK;
 }

@@ -122,6 +122,9 @@ struct Workspace {
   uint32_t* chunk_count = nullptr;  // [ntiles] chunks per tile, then exclusive-scanned
   int32_t* chunk_tile = nullptr;  // [max chunks] tile of every chunk
   uint32_t* chunk_total = nullptr;
+  float4* tblk = nullptr;         // boxes of 32-record blocks counted from every tile's start
+  uint32_t* tblk_off = nullptr;   // [ntiles] such blocks per tile, then exclusive-scanned
+  int64_t* rho_fix = nullptr;     // fixed-point density contributions of the symmetric sweep
 
   // pinned host copy of the event tables (same layout as the device block)
   void* pinned = nullptr;
