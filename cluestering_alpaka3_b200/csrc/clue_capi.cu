@@ -141,7 +141,6 @@ std::vector<ArenaItem> arena_items(Workspace& nw, void** evtab, size_t n, size_t
       {(void**)&nw.rec_m, n * w * 16},
       {(void**)&nw.sblk, (n / 1024 + 1) * 6 * 16},
       {(void**)&nw.ord_rho, n * 4},
-      {(void**)&nw.ord_nh, n * 4},
       {(void**)&nw.chunk_count, (ntiles + 1) * 4},
       {(void**)&nw.chunk_tile, (n / kChunkPoints + ntiles + 1) * 4},
       {(void**)&nw.chunk_total, 16},

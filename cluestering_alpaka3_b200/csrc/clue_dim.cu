@@ -710,78 +710,65 @@ __global__ void __launch_bounds__(256) k_gather_morton(const float4* __restrict_
 
 // ---- work orders and chunks --------------------------------------------------
 // Home points of every tile are taken in the fine Morton order of the tile (so 32 consecutive
-// points are close together at the data's own density scale) and stably partitioned by
-// search-box signature -- which neighbour tiles the box of radius dc (density) or dm (nearest
-// higher) reaches, 2 bits per dimension -- so the 32 lanes of a warp share one box.  The orders
-// are cut into chunks of kChunk home points; one CTA processes one chunk, so a heavy tile is
-// spread over many CTAs.  One CTA per tile; warp w partitions the w-th quarter of the tile and
-// the quarters are concatenated per key, which keeps the partition stable.
+// points are close together at the data's own density scale).  For the one-sided density
+// sweeps they are also stably partitioned by search-box signature -- which neighbour tiles the
+// box of radius dc reaches, 2 bits per dimension -- so the 32 lanes of a warp share one box.
+// (The nearest-higher sweep and the symmetric density sweep take the Morton order as it is.)
+// The orders are cut into chunks of kChunk home points; one CTA processes one chunk, so a heavy
+// tile is spread over many CTAs.  One CTA per tile; warp w partitions the w-th quarter of the
+// tile and the quarters are concatenated per key, which keeps the partition stable.
 template <int N>
 __global__ void __launch_bounds__(kTileThreads) k_order(const KParams kp, Events ev,
                                                         const int32_t* __restrict__ off,
                                                         const float4* __restrict__ rec_w,
                                                         const int32_t* __restrict__ mq,
-                                                        int32_t* __restrict__ ord_rho, int32_t* __restrict__ ord_nh,
-                                                        uint32_t* __restrict__ chunk_count,
-                                                        uint32_t* __restrict__ blk_count) {
+                                                        int32_t* __restrict__ ord_rho,
+                                                        uint32_t* __restrict__ chunk_count) {
   constexpr int K = N <= 4 ? (1 << (2 * N)) : 1;
-  __shared__ uint32_t s_cnt[kChunkWarps][2][K];
+  __shared__ uint32_t s_cnt[kChunkWarps][K];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const uint32_t lt = (1u << lane) - 1u;
-  int32_t* ord[2] = {ord_rho, ord_nh};
-  const float rad[2] = {kp.dc, kp.dm};
   for (int t = blockIdx.x; t < kp.ntiles; t += gridDim.x) {
     const int beg = off[t], end = off[t + 1];
-    if (threadIdx.x == 0) {
-      chunk_count[t] = (uint32_t)((end - beg + kChunk - 1) / kChunk);
-      if (blk_count) blk_count[t] = (uint32_t)((end - beg + 31) / 32);
-    }
+    if (threadIdx.x == 0) chunk_count[t] = (uint32_t)((end - beg + kChunk - 1) / kChunk);
     if (beg == end) continue;
     const EvGrid* g = ev.eg + find_event(ev.tile, kp.n_events, t);
     int hb[N];
     home_bins<N>(g, t, hb);
     const int quarter = ((end - beg + kChunkWarps - 1) / kChunkWarps + 31) & ~31;
     const int wb = min(end, beg + warp * quarter), we = min(end, wb + quarter);
-    for (int e = threadIdx.x; e < kChunkWarps * 2 * K; e += blockDim.x) (&s_cnt[0][0][0])[e] = 0;
+    for (int e = threadIdx.x; e < kChunkWarps * K; e += blockDim.x) (&s_cnt[0][0])[e] = 0;
     __syncthreads();
     for (int pass = 0; pass < 2; ++pass) {
       for (int base = wb; base < we; base += 32) {
         const int p = base + lane;
         const bool valid = p < we;
         const int q = valid ? mq[p] : mq[beg];
-        float x[N], pl;
-        load_rec<N>(rec_w, q, x, pl);
-        int key[2];
+        int key = 0;
+        if (K > 1) {
+          float x[N], pl;
+          load_rec<N>(rec_w, q, x, pl);
+          int lo[N], hi[N];
+          lane_box<N>(kp, g, x, kp.dc, hb, lo, hi);
 #pragma unroll
-        for (int r = 0; r < 2; ++r) {
-          key[r] = 0;
-          if (K > 1) {
-            int lo[N], hi[N];
-            lane_box<N>(kp, g, x, rad[r], hb, lo, hi);
-#pragma unroll
-            for (int d = 0; d < N; ++d) key[r] |= ((lo[d] < hb[d] ? 1 : 0) | (hi[d] > hb[d] ? 2 : 0)) << (2 * d);
-          }
+          for (int d = 0; d < N; ++d) key |= ((lo[d] < hb[d] ? 1 : 0) | (hi[d] > hb[d] ? 2 : 0)) << (2 * d);
         }
-#pragma unroll
-        for (int r = 0; r < 2; ++r) {
-          const uint32_t peers = __match_any_sync(0xffffffffu, valid ? key[r] : -1);
-          const bool leader = valid && (peers & lt) == 0;
-          if (pass == 1 && valid) ord[r][beg + s_cnt[warp][r][key[r]] + __popc(peers & lt)] = q;
-          __syncwarp();
-          if (leader) s_cnt[warp][r][key[r]] += __popc(peers);
-          __syncwarp();
-        }
+        const uint32_t peers = __match_any_sync(0xffffffffu, valid ? key : -1);
+        const bool leader = valid && (peers & lt) == 0;
+        if (pass == 1 && valid) ord_rho[beg + s_cnt[warp][key] + __popc(peers & lt)] = q;
+        __syncwarp();
+        if (leader) s_cnt[warp][key] += __popc(peers);
+        __syncwarp();
       }
       if (pass == 0) {
         __syncthreads();
         // first slot of (warp, key): keys in order, warps in order inside a key
-        if (threadIdx.x < 2) {
-          const int r = threadIdx.x;
+        if (threadIdx.x == 0) {
           uint32_t run = 0;
           for (int k = 0; k < K; ++k)
             for (int w = 0; w < kChunkWarps; ++w) {
-              const uint32_t c = s_cnt[w][r][k];
-              s_cnt[w][r][k] = run;
+              const uint32_t c = s_cnt[w][k];
+              s_cnt[w][k] = run;
               run += c;
             }
         }
@@ -789,6 +776,17 @@ __global__ void __launch_bounds__(kTileThreads) k_order(const KParams kp, Events
       }
     }
     __syncthreads();
+  }
+}
+
+// Chunks of kChunk and blocks of 32 points of every tile (when no density home order is built).
+__global__ void k_tile_counts(int ntiles, const int32_t* __restrict__ off, uint32_t* __restrict__ chunk_count,
+                              uint32_t* __restrict__ blk_count) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntiles; t += stride) {
+    const int cnt = off[t + 1] - off[t];
+    chunk_count[t] = (uint32_t)((cnt + kChunk - 1) / kChunk);
+    blk_count[t] = (uint32_t)((cnt + 31) / 32);
   }
 }
 
@@ -1574,11 +1572,11 @@ template <int N, int MT>
 void launch_nh(const KParams& kp, Workspace& ws, cudaStream_t s) {
   if (kp.tiebreak == CLUE_TIE_RHO_INDEX)
     k_nearest_higher<N, MT, CLUE_TIE_RHO_INDEX><<<chunk_grid(kp), kTileThreads, 0, s>>>(
-        kp, events_of(ws), ws.offsets, ws.ord_nh, ws.chunk_tile, ws.chunk_count, ws.chunk_total, ws.rec_r,
+        kp, events_of(ws), ws.offsets, ws.mq, ws.chunk_tile, ws.chunk_count, ws.chunk_total, ws.rec_r,
         ws.rec_m, ws.mq, ws.blk, ws.sblk, ws.minv, ws.perm, ws.nh_s, ws.delta_s, ws.status);
   else
     k_nearest_higher<N, MT, CLUE_TIE_REFERENCE><<<chunk_grid(kp), kTileThreads, 0, s>>>(
-        kp, events_of(ws), ws.offsets, ws.ord_nh, ws.chunk_tile, ws.chunk_count, ws.chunk_total, ws.rec_r,
+        kp, events_of(ws), ws.offsets, ws.mq, ws.chunk_tile, ws.chunk_count, ws.chunk_total, ws.rec_r,
         ws.rec_m, ws.mq, ws.blk, ws.sblk, ws.minv, ws.perm, ws.nh_s, ws.delta_s, ws.status);
 }
 template <int N, int MT, int FORM>
@@ -1714,8 +1712,10 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
   // no-allocation entry point, keeps the one-sided sweep)
   const bool symmetric =
       spatial_density && symmetric_density_ok(kp, a.metric, N) && ws.tblk && ws.tblk_off && ws.rho_fix;
-  k_order<N><<<kp.ntiles, kTileThreads, 0, s>>>(kp, ev, ws.offsets, ws.rec_w, ws.mq, ws.ord_rho, ws.ord_nh,
-                                                ws.chunk_count, symmetric ? ws.tblk_off : nullptr);
+  if (symmetric)
+    k_tile_counts<<<grid_for(kp.ntiles, 256), 256, 0, s>>>(kp.ntiles, ws.offsets, ws.chunk_count, ws.tblk_off);
+  else
+    k_order<N><<<kp.ntiles, kTileThreads, 0, s>>>(kp, ev, ws.offsets, ws.rec_w, ws.mq, ws.ord_rho, ws.chunk_count);
   exclusive_scan(ws.chunk_count, ws.chunk_count, (size_t)kp.ntiles, ws.scan_scratch, ws.chunk_total, s);
   if (symmetric) exclusive_scan(ws.tblk_off, ws.tblk_off, (size_t)kp.ntiles, ws.scan_scratch, nullptr, s);
   k_chunk_map<<<grid_for(kp.ntiles, 256), 256, 0, s>>>(kp.ntiles, ws.offsets, ws.chunk_count, ws.chunk_tile);

@@ -117,8 +117,7 @@ struct Workspace {
   float4* rec_m = nullptr;        // records in Morton order inside every tile
   float4* sblk = nullptr;         // bounding boxes of 1024-record super-blocks
   int32_t* mq = nullptr;          // Morton position -> tile-sorted position (alias after the sort)
-  int32_t* ord_rho = nullptr;     // per-tile home order for the density sweep
-  int32_t* ord_nh = nullptr;      // per-tile home order for the nearest-higher sweep
+  int32_t* ord_rho = nullptr;     // per-tile home order for the one-sided density sweeps
   uint32_t* chunk_count = nullptr;  // [ntiles] chunks per tile, then exclusive-scanned
   int32_t* chunk_tile = nullptr;  // [max chunks] tile of every chunk
   uint32_t* chunk_total = nullptr;

@@ -97,7 +97,6 @@ bool carve(Workspace& ws, void* base, int ndim, size_t n, size_t ntiles) {
       {(void**)&ws.rec_m, n * w * 16},
       {(void**)&ws.sblk, (n / 1024 + 1) * 6 * 16},
       {(void**)&ws.ord_rho, n * 4},
-      {(void**)&ws.ord_nh, n * 4},
       {(void**)&ws.chunk_count, (ntiles + 1) * 4},
       {(void**)&ws.chunk_tile, (n / kChunkPoints + ntiles + 1) * 4},
       {(void**)&ws.chunk_total, 16},
