@@ -1380,29 +1380,30 @@ __global__ void __launch_bounds__(kTileThreads, N <= 4 ? 8 : 4) k_density_sym(
         const int first = pb + (b << 5);
         const int cntB = min(32, pe - first);
         const bool cv = lane < cntB;
-        float cx[N], cw;
-        load_rec<N>(rec_m, first + (cv ? lane : 0), cx, cw);
+        // lane m owns candidate m of the block; at step k lane l meets candidate (l + k) mod 32
+        // and the candidate's owner collects the term from lane (m - k) mod 32, so no value is
+        // carried from one step to the next
+        float ox[N], ow;
+        load_rec<N>(rec_m, first + (cv ? lane : 0), ox, ow);
         if (!cv) {
 #pragma unroll
-          for (int d = 0; d < N; ++d) cx[d] = INFINITY;  // never within dc
-          cw = 0.0f;
+          for (int d = 0; d < N; ++d) ox[d] = INFINITY;  // never within dc
+          ow = 0.0f;
         }
         float cacc = 0.0f;
-        const int src = (lane + 1) & 31;
+#pragma unroll 4
         for (int k = 0; k < 32; ++k) {
+          const int src = (lane + k) & 31;
+          float cx[N];
+#pragma unroll
+          for (int d = 0; d < N; ++d) cx[d] = __shfl_sync(0xffffffffu, ox[d], src);
+          const float cw = __shfl_sync(0xffffffffu, ow, src);
           const float sd = M::partial(x, cx, kp.mpar);
           const bool in = hv && sd <= tdc;
-          if (__any_sync(0xffffffffu, in)) {
-            const float kv = kval(sd, false);
-            if (in) {
-              acc = fadd(acc, kv * cw);
-              cacc = fadd(cacc, kv * wi);
-            }
-          }
-#pragma unroll
-          for (int d = 0; d < N; ++d) cx[d] = __shfl_sync(0xffffffffu, cx[d], src);
-          cw = __shfl_sync(0xffffffffu, cw, src);
-          cacc = __shfl_sync(0xffffffffu, cacc, src);
+          const float kv = kval(sd, false);
+          if (in) acc = fadd(acc, kv * cw);
+          const float tc = in ? kv * wi : 0.0f;
+          cacc = fadd(cacc, __shfl_sync(0xffffffffu, tc, (lane - k) & 31));
         }
         if (cv && cacc != 0.0f)
           atomicAdd(reinterpret_cast<unsigned long long*>(rho_fix + mq[first + lane]),
