@@ -236,3 +236,59 @@ def test_blobs2d_medium_exact(gpu_context):
     wl = synthetic.blobs_2d_1m(n=1 << 17)
     ref, got = run_both(gpu_context, wl.coords, wl.weight, dc=wl.dc, rhoc=wl.rhoc, dm=wl.dm)
     assert_exact(ref, got)
+
+
+# ---- symmetric density sweep (Euclidean / Manhattan / Chebyshev, no wrapped coordinate) ----
+@pytest.mark.parametrize("metric", [("euclidean", ()), ("manhattan", ()), ("chebyshev", ())])
+@pytest.mark.parametrize("kernel", [("exp", (1.0, 1.0)), ("exp", (0.7, 2.0)), ("gaus", (0.0, 0.8, 1.0)),
+                                    ("gaus", (0.5, 1.0, 1.3))])
+def test_symmetric_density_metrics_kernels(gpu_context, metric, kernel):
+    rng = np.random.default_rng(71)
+    c, w = random_blobs(rng, 7000, 2, nblobs=10, extent=60.0, sigma=1.0)
+    kw = dict(dc=1.8, rhoc=3.0, dm=2.5, kernel=kernel, metric=metric)
+    ref, got = run_both(gpu_context, c, w, **kw)
+    np.testing.assert_array_equal(got.delta > 0, ref.delta > 0)
+    cfg = O.Config(dc=1.8, rhoc=3.0, dm=2.5, kernel=kernel[0], kernel_par=kernel[1], metric=metric[0])
+    from parity_util import tolerance_report
+    rep = tolerance_report(got.rho, ref.rho, c, w, cfg, got.cluster_index, ref.cluster_index, RTOL)
+    print("tolerance report", rep)
+    assert rep["max_rel_far"] <= RTOL, rep
+    assert rep["label_mismatch"] <= max(2, rep["n"] // 1000), rep
+
+
+@pytest.mark.parametrize("ndim", [1, 3, 4])
+def test_symmetric_density_dimensions(gpu_context, ndim):
+    rng = np.random.default_rng(80 + ndim)
+    c, w = random_blobs(rng, 8000, ndim, nblobs=8, extent=30.0, sigma=0.8)
+    kw = dict(dc=1.0 + 0.2 * ndim, rhoc=3.0, dm=1.5 + 0.2 * ndim, kernel=("exp", (1.0, 1.0)))
+    ref, got = run_both(gpu_context, c, w, **kw)
+    _assert_tolerant(ref, got, c, w, kw)
+
+
+def test_symmetric_density_negative_weights(gpu_context):
+    # the mirrored terms are accumulated in fixed point scaled by the event's largest |weight|
+    rng = np.random.default_rng(91)
+    c, w = random_blobs(rng, 5000, 2, nblobs=6, extent=40.0)
+    w = (w - 0.8).astype(np.float32)
+    kw = dict(dc=1.5, rhoc=0.5, dm=2.0, kernel=("exp", (1.0, 1.0)))
+    ref, got = run_both(gpu_context, c, w, **kw)
+    rho64 = O.rho_f64(c, w, O.Config(dc=1.5, rhoc=0.5, dm=2.0, kernel="exp", kernel_par=(1.0, 1.0)))
+    scale = np.abs(w).max() * 50
+    assert np.max(np.abs(got.rho.astype(np.float64) - rho64)) <= 1e-5 * scale
+
+
+def test_symmetric_density_deterministic_and_placement_free(gpu_context):
+    # an event alone and the same event inside a batch (other events before it) give the same bits
+    from parity_util import gpu_args
+    rng = np.random.default_rng(95)
+    c1, w1 = random_blobs(rng, 3000, 2, nblobs=5, extent=25.0)
+    c2, w2 = random_blobs(rng, 4321, 2, nblobs=7, extent=25.0)
+    p, k, m = gpu_args(dc=1.5, rhoc=3.0, dm=2.0, kernel=("exp", (1.0, 1.0)))
+    alone = gpu_context.make_clusters_host(c2, w2, p, k, m)
+    again = gpu_context.make_clusters_host(c2, w2, p, k, m)
+    np.testing.assert_array_equal(alone.rho.view(np.uint32), again.rho.view(np.uint32))
+    coords = np.ascontiguousarray(np.concatenate([c1, c2], axis=1))
+    weight = np.concatenate([w1, w2])
+    res, _ = gpu_context.batch_host(coords, weight, [0, c1.shape[1], coords.shape[1]], p, k, m)
+    np.testing.assert_array_equal(res.rho[c1.shape[1]:].view(np.uint32), alone.rho.view(np.uint32))
+    np.testing.assert_array_equal(res.cluster_index[c1.shape[1]:], alone.cluster_index)
