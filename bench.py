@@ -360,7 +360,8 @@ def main():
             "e2e": {"value": world * n * args.steps / (e2e_total / 1e3), "unit": "points/s",
                     "h2d_bytes_per_step": int(n * (ndim + 1) * 4 + 12 * E + 264 * E),
                     "d2h_bytes_per_step": int(n * 2 * 4 + 4 * E)},
-            "roofline": {"bound": "hbm", "kernel": "k_density", "achieved": achieved, "peak": peak,
+            "roofline": {"bound": "hbm", "kernel": "k_density" if kname == "flat" else "k_density_sym",
+                         "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": traffic, "algorithmic_bytes": B["density_kernel"], "launch_ms": dens_ms},
             "stage_ms": {"tiles": stage_avg[0], "density": stage_avg[1], "nearest_higher": stage_avg[2],
