@@ -18,24 +18,39 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
   return m;
 }
 
-// Per-block digit histogram; hist is digit-major: hist[d * nblocks + block].
+// Per-block digit histogram; hist is digit-major: hist[d * nblocks + block].  Every warp counts
+// into its own shared-memory histogram (plain shared atomics), the warps' counts are summed at
+// the end; keys are read four at a time where the tile is complete.
 __global__ void __launch_bounds__(kSortThreads) k_radix_hist(const uint32_t* __restrict__ keys, int n,
                                                              int shift, uint32_t* __restrict__ hist,
                                                              int nblocks) {
-  __shared__ uint32_t h[kRadix];
-  for (int d = threadIdx.x; d < kRadix; d += blockDim.x) h[d] = 0;
+  constexpr int kWarps = kSortThreads / 32;
+  __shared__ uint32_t h[kWarps][kRadix];
+  const int warp = threadIdx.x >> 5;
+  for (int e = threadIdx.x; e < kWarps * kRadix; e += blockDim.x) (&h[0][0])[e] = 0;
   __syncthreads();
   const int base = blockIdx.x * kSortTile;
-#pragma unroll 4
-  for (int r = 0; r < kSortItems; ++r) {
-    const int i = base + r * kSortThreads + threadIdx.x;
-    const bool valid = i < n;
-    const uint32_t d = valid ? (keys[i] >> shift) & (kRadix - 1) : (uint32_t)kRadix;
-    const uint32_t peers = __match_any_sync(0xffffffffu, d);
-    if (valid && (peers & lanemask_lt()) == 0) atomicAdd(&h[d], __popc(peers));
+  uint32_t* hw = h[warp];
+  if (base + kSortTile <= n) {
+    const uint4* k4 = reinterpret_cast<const uint4*>(keys + base);
+#pragma unroll
+    for (int r = 0; r < kSortItems / 4; ++r) {
+      const uint4 v = __ldg(k4 + r * kSortThreads + threadIdx.x);
+      atomicAdd(&hw[(v.x >> shift) & (kRadix - 1)], 1u);
+      atomicAdd(&hw[(v.y >> shift) & (kRadix - 1)], 1u);
+      atomicAdd(&hw[(v.z >> shift) & (kRadix - 1)], 1u);
+      atomicAdd(&hw[(v.w >> shift) & (kRadix - 1)], 1u);
+    }
+  } else {
+    for (int i = base + threadIdx.x; i < n; i += kSortThreads) atomicAdd(&hw[(keys[i] >> shift) & (kRadix - 1)], 1u);
   }
   __syncthreads();
-  for (int d = threadIdx.x; d < kRadix; d += blockDim.x) hist[(size_t)d * nblocks + blockIdx.x] = h[d];
+  for (int d = threadIdx.x; d < kRadix; d += blockDim.x) {
+    uint32_t c = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) c += h[w][d];
+    hist[(size_t)d * nblocks + blockIdx.x] = c;
+  }
 }
 
 __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v) {
