@@ -263,29 +263,6 @@ __device__ __forceinline__ void load_box(const float4* __restrict__ a, int i, fl
   }
 }
 
-// A block of up to 32 consecutive records loaded cooperatively: lane k holds record p0 + k;
-// bcast_rec() hands record j to every lane through register shuffles.
-template <int N>
-__device__ __forceinline__ void warp_load_block(const float4* __restrict__ rec, int p0, int cnt, float* mine) {
-  constexpr int W = Rec<N>::kWords;
-  const int lane = threadIdx.x & 31;
-  const int p = p0 + (lane < cnt ? lane : 0);
-#pragma unroll
-  for (int k = 0; k < W; ++k) {
-    const float4 v = __ldg(rec + (size_t)p * W + k);
-    mine[4 * k] = v.x;
-    mine[4 * k + 1] = v.y;
-    mine[4 * k + 2] = v.z;
-    mine[4 * k + 3] = v.w;
-  }
-}
-template <int N>
-__device__ __forceinline__ void bcast_rec(const float* mine, int j, float* c, float& payload) {
-#pragma unroll
-  for (int d = 0; d < N; ++d) c[d] = __shfl_sync(0xffffffffu, mine[d], j);
-  payload = __shfl_sync(0xffffffffu, mine[Rec<N>::kPayload], j);
-}
-
 // A block of up to 32 consecutive records staged in the warp's shared-memory slot: lane k
 // copies record p0 + k; smem_rec() then reads record j with broadcast loads (every lane reads
 // the same address), one 16-byte load per record word.
