@@ -517,67 +517,64 @@ __global__ void __launch_bounds__(256) k_bbox_single(InPtrs in, int n, EvGrid* g
   if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&st->nonfinite, 1u);
 }
 
-// Bounding box of many events: one CTA per event (grid-stride over events).
+// Event of point i, looked up once per warp when the warp's points share one event (the usual
+// case: events are contiguous ranges of points) and per lane otherwise.
+__device__ __forceinline__ int warp_event(const int32_t* __restrict__ ev_pt, int E, int i, bool active,
+                                          bool& uniform) {
+  const unsigned am = __activemask();
+  const int first = __shfl_sync(am, i, __ffs(am) - 1);
+  const int last = __shfl_sync(am, i, 31 - __clz(am));
+  const int e0 = find_event(ev_pt, E, first);
+  uniform = last < ev_pt[e0 + 1];
+  return uniform ? e0 : (active ? find_event(ev_pt, E, i) : e0);
+}
+
+// Bounding box and largest |weight| of many events: grid-stride over points; a warp whose points
+// share an event reduces them before its atomics.
 template <int N>
-__global__ void __launch_bounds__(256) k_bbox_events(InPtrs in, int E, EvGrid* eg, DevStatus* st) {
-  __shared__ uint32_t s_mn[8][N], s_mx[8][N], s_w[8];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  for (int e = blockIdx.x; e < E; e += gridDim.x) {
-    const int b = eg[e].pt_base, cnt = eg[e].pt_count;
+__global__ void __launch_bounds__(256) k_bbox_events(InPtrs in, int n, int E, const int32_t* __restrict__ ev_pt,
+                                                     EvGrid* eg, DevStatus* st) {
+  const int stride = gridDim.x * blockDim.x;
+  bool bad = false;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    bool uniform;
+    const int e = warp_event(ev_pt, E, i, true, uniform);
     uint32_t emn[N], emx[N];
 #pragma unroll
     for (int d = 0; d < N; ++d) {
-      emn[d] = 0xffffffffu;
-      emx[d] = 0u;
+      const float x = in.c[d][i];
+      bad |= !isfinite(x);
+      emn[d] = emx[d] = enc_float(x);
     }
-    bool bad = false;
-    uint32_t wmax = 0u;
-    for (int i = b + threadIdx.x; i < b + cnt; i += blockDim.x) {
+    const float w = in.w[i];
+    bad |= !isfinite(w);
+    uint32_t wm = __float_as_uint(fabsf(w));
+    const unsigned am = __activemask();
+    if (uniform && am == 0xffffffffu) {
 #pragma unroll
       for (int d = 0; d < N; ++d) {
-        const float x = in.c[d][i];
-        bad |= !isfinite(x);
-        const uint32_t en = enc_float(x);
-        emn[d] = min(emn[d], en);
-        emx[d] = max(emx[d], en);
+        emn[d] = warp_min_u(emn[d]);
+        emx[d] = warp_max_u(emx[d]);
       }
-      const float w = in.w[i];
-      bad |= !isfinite(w);
-      wmax = max(wmax, __float_as_uint(fabsf(w)));
-    }
+      wm = warp_max_u(wm);
+      if ((threadIdx.x & 31) == 0) {
 #pragma unroll
-    for (int d = 0; d < N; ++d) {
-      emn[d] = warp_min_u(emn[d]);
-      emx[d] = warp_max_u(emx[d]);
-    }
-    wmax = warp_max_u(wmax);
-    if (lane == 0) {
+        for (int d = 0; d < N; ++d) {
+          atomicMin(&eg[e].enc_min[d], emn[d]);
+          atomicMax(&eg[e].enc_max[d], emx[d]);
+        }
+        atomicMax(&eg[e].wmax_bits, wm);
+      }
+    } else {
 #pragma unroll
       for (int d = 0; d < N; ++d) {
-        s_mn[warp][d] = emn[d];
-        s_mx[warp][d] = emx[d];
+        atomicMin(&eg[e].enc_min[d], emn[d]);
+        atomicMax(&eg[e].enc_max[d], emx[d]);
       }
-      s_w[warp] = wmax;
+      atomicMax(&eg[e].wmax_bits, wm);
     }
-    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(&st->nonfinite, 1u);
-    __syncthreads();
-    if (threadIdx.x < N) {
-      const int d = threadIdx.x;
-      uint32_t a = 0xffffffffu, z = 0u;
-      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-        a = min(a, s_mn[w][d]);
-        z = max(z, s_mx[w][d]);
-      }
-      eg[e].enc_min[d] = a;
-      eg[e].enc_max[d] = z;
-    }
-    if (threadIdx.x == 0) {
-      uint32_t m = 0u;
-      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = max(m, s_w[w]);
-      eg[e].wmax_bits = m;
-    }
-    __syncthreads();
   }
+  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&st->nonfinite, 1u);
 }
 
 // Tile size (max - min) / nperdim in FP32 (ComputeTiles.hpp:20-23), per event.
@@ -603,7 +600,8 @@ __global__ void __launch_bounds__(256) k_bin(const KParams kp, InPtrs in, Events
                                              uint32_t* __restrict__ keys) {
   const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kp.n; i += stride) {
-    const EvGrid* g = ev.eg + find_event(ev.pt, kp.n_events, i);
+    bool uniform;
+    const EvGrid* g = ev.eg + warp_event(ev.pt, kp.n_events, i, true, uniform);
     int gb = g->tile_base;
 #pragma unroll
     for (int d = 0; d < N; ++d)
@@ -643,7 +641,8 @@ __global__ void __launch_bounds__(256) k_morton_keys(const KParams kp, Events ev
   const int stride = gridDim.x * blockDim.x;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < kp.n; q += stride) {
     const uint32_t t = tile_keys[q];
-    const EvGrid* g = ev.eg + find_event(ev.tile, kp.n_events, (int)t);
+    bool uniform;  // tile-sorted positions are event-major: event e holds [ev.pt[e], ev.pt[e + 1])
+    const EvGrid* g = ev.eg + warp_event(ev.pt, kp.n_events, q, true, uniform);
     int hb[N];
     home_bins<N>(g, (int)t, hb);
     float x[N], pl;
@@ -1407,7 +1406,8 @@ __global__ void __launch_bounds__(256) k_density_combine(const KParams kp, Event
                                                          float4* __restrict__ rec_r, float kmax) {
   const int stride = gridDim.x * blockDim.x;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride) {
-    const EvGrid* g = ev.eg + find_event(ev.pt, kp.n_events, q);
+    bool uniform;
+    const EvGrid* g = ev.eg + warp_event(ev.pt, kp.n_events, q, true, uniform);
     float x[N], acc;
     load_rec<N>(rec_r, q, x, acc);
     const float recv = (float)((double)rho_fix[q] * ldexp(1.0, -fix_exponent(g, kmax)));
@@ -1487,11 +1487,12 @@ __global__ void __launch_bounds__(256) k_finalize(const KParams kp, Events ev, c
                                                   const float* __restrict__ delta_s, clue_outputs out) {
   const int stride = gridDim.x * blockDim.x;
   for (int pos = blockIdx.x * blockDim.x + threadIdx.x; pos < kp.n; pos += stride) {
+    bool uniform;
+    const int e = warp_event(ev.pt, kp.n_events, pos, true, uniform);
     const int p = par[pos];
     const int root = p >= 0 ? p : pos;
     int lab = -1;
     if (is_seed_s[root]) {
-      const int e = find_event(ev.pt, kp.n_events, pos);
       const uint32_t rk = seed_rank[perm[root]] - seed_rank[ev.pt[e]];
       if ((int64_t)rk < seed_cap(kp, ev.eg + e)) lab = (int)rk;
     }
@@ -1654,8 +1655,7 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
   if (kp.n_events == 1)
     k_bbox_single<N><<<grid_for(n, 256), 256, 0, s>>>(in, n, ws.ev, ws.status);
   else
-    k_bbox_events<N><<<kp.n_events < 148 * 16 ? kp.n_events : 148 * 16, 256, 0, s>>>(in, kp.n_events, ws.ev,
-                                                                                    ws.status);
+    k_bbox_events<N><<<grid_for(n, 256), 256, 0, s>>>(in, n, kp.n_events, ws.ev_pt, ws.ev, ws.status);
   k_grid<N><<<grid_for(kp.n_events, 256), 256, 0, s>>>(kp.n_events, ws.ev);
   k_bin<N><<<grid_for(n, 256), 256, 0, s>>>(kp, in, ev, ws.keys[0]);
   const int bits = bits_for((uint32_t)(kp.ntiles - 1));
