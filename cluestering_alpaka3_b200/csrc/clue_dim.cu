@@ -666,6 +666,38 @@ __global__ void __launch_bounds__(256) k_tile_of(const uint32_t* __restrict__ ti
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) out[p] = tile_keys[mq[p]];
 }
 
+// Composite key (tile << mbits | Morton code of the point inside its tile, top mbits bits) of every
+// point, for the single sort that yields the (tile, Morton) order directly.
+template <int N>
+__global__ void __launch_bounds__(256) k_bin_composite(const KParams kp, InPtrs in, Events ev, int mbits,
+                                                       uint32_t* __restrict__ keys) {
+  constexpr int bpd = MortonBits<N>::kPerDim;
+  const float scale = (float)(1u << bpd);
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kp.n; i += stride) {
+    bool uniform;
+    const EvGrid* g = ev.eg + warp_event(ev.pt, kp.n_events, i, true, uniform);
+    int gb = g->tile_base;
+    uint32_t m = 0;
+#pragma unroll
+    for (int d = 0; d < N; ++d) {
+      const float x = in.c[d][i];
+      const int b = get_bin(x, g->mn[d], g->mx[d], g->size[d], kp.wrapped[d] != 0, g->nperdim);
+      gb += g->stride[d] * b;
+      const float t0 = g->mn[d] + (float)b * g->size[d];
+      int c = g->size[d] > 0.0f ? (int)((x - t0) / g->size[d] * scale) : 0;
+      c = c < 0 ? 0 : (c > (1 << bpd) - 1 ? (1 << bpd) - 1 : c);
+      for (int bit = 0; bit < bpd; ++bit) m |= (uint32_t)((c >> bit) & 1) << (bit * N + d);
+    }
+    keys[i] = ((uint32_t)gb << mbits) | (m >> (MortonBits<N>::kBits - mbits));
+  }
+}
+
+__global__ void __launch_bounds__(256) k_iota2(int32_t* __restrict__ a, int32_t* __restrict__ b, int n) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) a[p] = b[p] = p;
+}
+
 // Inverse permutation: minv[mq[p]] = p.
 __global__ void __launch_bounds__(256) k_invert(const int32_t* __restrict__ mq, int n, int32_t* __restrict__ minv) {
   const int stride = gridDim.x * blockDim.x;
@@ -1082,8 +1114,8 @@ __global__ void __launch_bounds__(kTileThreads, N <= 2 ? 8 : (N <= 4 ? 6 : 4)) k
   // Candidates beyond bnd cannot be nearer than the best so far (nor within dm): its distance
   // would round above delta.
   float bnd = tdm;
-  int nh = -1, orig_best = INT_MAX;
-  uint64_t rank_best = ~0ull;
+  int nh = -1, orig_best = -1;
+  int lex_best = 0;  // search-box position of the best one's tile (below the tile count)
   spatial_sweep<N, M, true>(kp, h.g, off, hb, lo, hi, valid, x, blk, sblk, rho_i, minv[pos],
                       [&]() { return bnd; },
                       [&](int p0, int p1, bool need, int64_t lexpos) {
@@ -1102,30 +1134,34 @@ __global__ void __launch_bounds__(kTileThreads, N <= 2 ? 8 : (N <= 4 ? 6 : 4)) k
           higher = orig_j > orig_i;
         }
         if (higher) {
-          const uint64_t rank = ((uint64_t)lexpos << 32) | (uint32_t)q;
           bool better;
           if (s * slack < s_best) {
             better = true;  // its distance rounds strictly below the best one's
           } else {
-            // the two distances may round to the same value: decide on the rounded distances
+            // the two distances may round to the same value: decide on the rounded distances,
+            // then on the iteration rank (search-box position of the tile, then the original
+            // index, which orders the points of one tile in the reference's iteration)
             const float dist = M::finish(s), dbest = M::finish(s_best);
-            if (TIE == CLUE_TIE_REFERENCE) {
-              better = dist < dbest || (dist == dbest && rank < rank_best);
-            } else if (dist == dbest && nh >= 0) {
-              if (orig_j < 0) orig_j = __ldg(perm + q);
-              if (orig_best < 0) orig_best = __ldg(perm + nh);
-              better = rho_j > rho_best || (rho_j == rho_best && orig_j < orig_best);
-            } else {
+            if (dist != dbest || nh < 0) {
               better = dist < dbest;
+            } else if (TIE == CLUE_TIE_REFERENCE && (int)lexpos != lex_best) {
+              better = (int)lexpos < lex_best;
+            } else {
+              if (orig_j < 0) orig_j = __ldg(perm + q);
+              const int ob = TIE == CLUE_TIE_REFERENCE || orig_best < 0 ? __ldg(perm + nh) : orig_best;
+              better = TIE == CLUE_TIE_REFERENCE ? orig_j < ob
+                                                 : rho_j > rho_best || (rho_j == rho_best && orig_j < ob);
             }
           }
           if (better) {
             s_best = s;
             bnd = fminf(tdm, s * slack);
             nh = q;
-            rank_best = rank;
-            rho_best = rho_j;
-            orig_best = orig_j;
+            lex_best = (int)lexpos;
+            if (TIE != CLUE_TIE_REFERENCE) {
+              rho_best = rho_j;
+              orig_best = orig_j;
+            }
           }
         }
       }
@@ -1552,17 +1588,17 @@ void launch_nh(const KParams& kp, Workspace& ws, cudaStream_t s) {
   if (kp.tiebreak == CLUE_TIE_RHO_INDEX)
     k_nearest_higher<N, MT, CLUE_TIE_RHO_INDEX><<<chunk_grid(kp), kTileThreads, 0, s>>>(
         kp, events_of(ws), ws.offsets, ws.mq, ws.chunk_tile, ws.chunk_count, ws.chunk_total, ws.rec_r,
-        ws.rec_m, ws.mq, ws.blk, ws.sblk, ws.minv, ws.perm, ws.nh_s, ws.delta_s, ws.status);
+        ws.rec_m_cur, ws.mq, ws.blk, ws.sblk, ws.minv, ws.perm, ws.nh_s, ws.delta_s, ws.status);
   else
     k_nearest_higher<N, MT, CLUE_TIE_REFERENCE><<<chunk_grid(kp), kTileThreads, 0, s>>>(
         kp, events_of(ws), ws.offsets, ws.mq, ws.chunk_tile, ws.chunk_count, ws.chunk_total, ws.rec_r,
-        ws.rec_m, ws.mq, ws.blk, ws.sblk, ws.minv, ws.perm, ws.nh_s, ws.delta_s, ws.status);
+        ws.rec_m_cur, ws.mq, ws.blk, ws.sblk, ws.minv, ws.perm, ws.nh_s, ws.delta_s, ws.status);
 }
 template <int N, int MT, int FORM>
 void launch_density_spatial_form(const KParams& kp, Workspace& ws, cudaStream_t s, float kexp) {
   k_density_spatial<N, MT, FORM><<<chunk_grid(kp), kTileThreads, 0, s>>>(
       kp, events_of(ws), ws.offsets, ws.ord_rho, ws.chunk_tile, ws.chunk_count, ws.chunk_total, ws.rec_w,
-      ws.rec_m, ws.mq, ws.blk, ws.sblk, ws.rec_r, ws.minv, kexp);
+      ws.rec_m_cur, ws.mq, ws.blk, ws.sblk, ws.rec_r, ws.minv, kexp);
 }
 template <int N, int MT>
 void launch_density_spatial(const KParams& kp, Workspace& ws, cudaStream_t s) {
@@ -1578,7 +1614,7 @@ void launch_density_spatial(const KParams& kp, Workspace& ws, cudaStream_t s) {
 template <int N, int MT, int FORM>
 void launch_density_sym_form(const KParams& kp, Workspace& ws, cudaStream_t s, float kexp, float kmax) {
   k_density_sym<N, MT, FORM><<<chunk_grid(kp), kTileThreads, 0, s>>>(
-      kp, events_of(ws), ws.offsets, ws.chunk_tile, ws.chunk_count, ws.chunk_total, ws.rec_m, ws.mq, ws.tblk_off,
+      kp, events_of(ws), ws.offsets, ws.chunk_tile, ws.chunk_count, ws.chunk_total, ws.rec_m_cur, ws.mq, ws.tblk_off,
       ws.tblk, ws.rec_r, ws.rho_fix, kexp, kmax);
 }
 template <int N, int MT>
@@ -1657,14 +1693,41 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
   else
     k_bbox_events<N><<<grid_for(n, 256), 256, 0, s>>>(in, n, kp.n_events, ws.ev_pt, ws.ev, ws.status);
   k_grid<N><<<grid_for(kp.n_events, 256), 256, 0, s>>>(kp.n_events, ws.ev);
-  k_bin<N><<<grid_for(n, 256), 256, 0, s>>>(kp, in, ev, ws.keys[0]);
+  int launches = 4;  // init, bbox, grid, bin
+  // density order: the reference's candidate order for the flat kernel (bit-exact sums), spatial
+  // order for the exponential and Gaussian kernels (whose device expf already differs from the
+  // host's by an ulp) unless the caller asks for the reference order
+  const bool spatial_density = (kp.flags & CLUE_FLAG_REFERENCE_ORDER) == 0 &&
+                               (kp.kernel_type != CLUE_KERNEL_FLAT || (kp.flags & CLUE_FLAG_SPATIAL_DENSITY) != 0);
+  // (a workspace without the symmetric sweep's buffers, such as the fixed scratch of the
+  // no-allocation entry point, keeps the one-sided sweep)
+  const bool symmetric =
+      spatial_density && symmetric_density_ok(kp, a.metric, N) && ws.tblk && ws.tblk_off && ws.rho_fix;
   const int bits = bits_for((uint32_t)(kp.ntiles - 1));
-  const int cur = radix_sort_pairs(ws.keys, ws.vals, true, n, bits, ws.hist, ws.scan_scratch, s);
-  ws.perm = ws.vals[cur];
-  ws.sorted_keys = ws.keys[cur];
-  offsets_from_sorted(ws.sorted_keys, n, kp.ntiles, ws.offsets, s);
-  k_gather<N><<<grid_for(n, 256), 256, 0, s>>>(in, n, ws.perm, ws.rec_w);
-  {
+  const int mbits = std::min(MortonBits<N>::kBits, 32 - bits);
+  // The symmetric sweep needs no tile order by point index: one sort by (tile, Morton) composite
+  // keys gives its record order, and positions inside a tile are only compared through the
+  // points' indices.  The other sweeps take the tile order by index and a Morton order beside it.
+  const bool composite = symmetric && mbits >= 8;
+  if (composite) {
+    k_bin_composite<N><<<grid_for(n, 256), 256, 0, s>>>(kp, in, ev, mbits, ws.keys[0]);
+    const int cur = radix_sort_pairs(ws.keys, ws.vals, true, n, bits + mbits, ws.hist, ws.scan_scratch, s);
+    ws.perm = ws.vals[cur];
+    ws.sorted_keys = ws.keys[cur];
+    offsets_from_sorted(ws.sorted_keys, n, kp.ntiles, ws.offsets, s, mbits);
+    k_gather<N><<<grid_for(n, 256), 256, 0, s>>>(in, n, ws.perm, ws.rec_w);
+    ws.mq = ws.vals[cur ^ 1];
+    ws.minv = ws.mq_alt;
+    k_iota2<<<grid_for(n, 256), 256, 0, s>>>(ws.mq, ws.minv, n);
+    ws.rec_m_cur = ws.rec_w;
+    launches += radix_sort_launches(bits + mbits) + 3;
+  } else {
+    k_bin<N><<<grid_for(n, 256), 256, 0, s>>>(kp, in, ev, ws.keys[0]);
+    const int cur = radix_sort_pairs(ws.keys, ws.vals, true, n, bits, ws.hist, ws.scan_scratch, s);
+    ws.perm = ws.vals[cur];
+    ws.sorted_keys = ws.keys[cur];
+    offsets_from_sorted(ws.sorted_keys, n, kp.ntiles, ws.offsets, s);
+    k_gather<N><<<grid_for(n, 256), 256, 0, s>>>(in, n, ws.perm, ws.rec_w);
     // fine Morton order inside every tile: a stable sort by Morton key, then a stable sort by
     // tile; mq[p] = tile-sorted position of the p-th record in (tile, Morton) order
     uint32_t* mkeys[2] = {ws.keys[cur ^ 1], ws.mkeys_alt};
@@ -1680,16 +1743,10 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
     ws.mq = mvals[mc];
     ws.minv = mvals[mc ^ 1];
     k_invert<<<grid_for(n, 256), 256, 0, s>>>(ws.mq, n, ws.minv);
+    ws.rec_m_cur = ws.rec_m;
+    launches += radix_sort_launches(bits) + 2 + 1 + radix_sort_launches(MortonBits<N>::kBits) + 1 +
+                radix_sort_launches(bits) + 1;
   }
-  // density order: the reference's candidate order for the flat kernel (bit-exact sums), spatial
-  // order for the exponential and Gaussian kernels (whose device expf already differs from the
-  // host's by an ulp) unless the caller asks for the reference order
-  const bool spatial_density = (kp.flags & CLUE_FLAG_REFERENCE_ORDER) == 0 &&
-                               (kp.kernel_type != CLUE_KERNEL_FLAT || (kp.flags & CLUE_FLAG_SPATIAL_DENSITY) != 0);
-  // (a workspace without the symmetric sweep's buffers, such as the fixed scratch of the
-  // no-allocation entry point, keeps the one-sided sweep)
-  const bool symmetric =
-      spatial_density && symmetric_density_ok(kp, a.metric, N) && ws.tblk && ws.tblk_off && ws.rho_fix;
   if (symmetric)
     k_tile_counts<<<grid_for(kp.ntiles, 256), 256, 0, s>>>(kp.ntiles, ws.offsets, ws.chunk_count, ws.tblk_off);
   else
@@ -1697,20 +1754,27 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
   exclusive_scan(ws.chunk_count, ws.chunk_count, (size_t)kp.ntiles, ws.scan_scratch, ws.chunk_total, s);
   if (symmetric) exclusive_scan(ws.tblk_off, ws.tblk_off, (size_t)kp.ntiles, ws.scan_scratch, nullptr, s);
   k_chunk_map<<<grid_for(kp.ntiles, 256), 256, 0, s>>>(kp.ntiles, ws.offsets, ws.chunk_count, ws.chunk_tile);
+  launches += 1 + kScanLaunches + (symmetric ? kScanLaunches : 0) + 1;
 
   const int nblk_threads = ((n + 31) >> 5) * 32;
   const int nsb_threads = ((((n + 31) >> 5) + 31) >> 5) * 32;
   const int max_slots = 4 * (n / kChunk + kp.ntiles + 1);
   if (symmetric) {
-    k_gather_morton<N><<<grid_for(n, 256), 256, 0, s>>>(ws.rec_w, n, ws.mq, ws.rec_m);
+    if (!composite) {
+      k_gather_morton<N><<<grid_for(n, 256), 256, 0, s>>>(ws.rec_w, n, ws.mq, ws.rec_m);
+      ++launches;
+    }
     k_tblock_bbox<N><<<grid_for(max_slots, 256), 256, 0, s>>>(max_slots, ws.chunk_total, ws.offsets, ws.chunk_tile,
-                                                               ws.chunk_count, ws.tblk_off, ws.rec_m, ws.tblk);
+                                                               ws.chunk_count, ws.tblk_off, ws.rec_m_cur, ws.tblk);
+    ++launches;
   } else if (spatial_density) {
     k_gather_morton<N><<<grid_for(n, 256), 256, 0, s>>>(ws.rec_w, n, ws.mq, ws.rec_m);
     k_block_bbox<N><<<grid_for(nblk_threads, 256), 256, 0, s>>>(ws.rec_m, n, ws.blk);
     k_superblock_bbox<N><<<grid_for(nsb_threads, 256), 256, 0, s>>>(ws.blk, n, ws.sblk);
+    launches += 3;
   } else {
     k_block_bbox<N><<<grid_for(nblk_threads, 256), 256, 0, s>>>(ws.rec_w, n, ws.blk);
+    ++launches;
   }
 
   stage_mark(ws, 1, s);
@@ -1721,11 +1785,19 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
   } else {
     CLUE_METRIC_SWITCH(a.metric, launch_density, kp, ws, s);
   }
+  launches += symmetric ? 2 : 1;
   stage_mark(ws, 2, s);
-  // Morton-ordered copy of the records with their densities and its block / super-block boxes
-  // with the largest rho, for the nearest-higher search
-  k_gather_morton<N><<<grid_for(n, 256), 256, 0, s>>>(ws.rec_r, n, ws.mq, ws.rec_m);
-  k_block_bbox<N><<<grid_for(nblk_threads, 256), 256, 0, s>>>(ws.rec_m, n, ws.blk);
+  // Morton-ordered copy of the records with their densities (the tile-ordered records themselves
+  // after a composite sort) and its block / super-block boxes with the largest rho, for the
+  // nearest-higher search
+  if (composite) {
+    ws.rec_m_cur = ws.rec_r;
+  } else {
+    k_gather_morton<N><<<grid_for(n, 256), 256, 0, s>>>(ws.rec_r, n, ws.mq, ws.rec_m);
+    ws.rec_m_cur = ws.rec_m;
+    ++launches;
+  }
+  k_block_bbox<N><<<grid_for(nblk_threads, 256), 256, 0, s>>>(ws.rec_m_cur, n, ws.blk);
   k_superblock_bbox<N><<<grid_for(nsb_threads, 256), 256, 0, s>>>(ws.blk, n, ws.sblk);
   CLUE_METRIC_SWITCH(a.metric, launch_nh, kp, ws, s);
   stage_mark(ws, 3, s);
@@ -1738,13 +1810,8 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
   k_event_info<<<grid_for(kp.n_events, 256), 256, 0, s>>>(kp, ws.ev, ws.ev_pt, ws.seed_flag, ws.seed_total,
                                                          a.ev_n_seeds, a.ev_n_clusters, ws.status);
   stage_mark(ws, 4, s);
-  // init, bbox, grid, bin, sort, offsets, gather, Morton keys + 2 sorts + tile keys + inverse, order,
-  // scan, chunk map, density boxes, density, Morton gather + boxes, nh, seeds, scan, jumps,
-  // finalize, event info
-  ws.launches += 4 + radix_sort_launches(bits) + 2 + 1 + radix_sort_launches(MortonBits<N>::kBits) + 1 +
-                 radix_sort_launches(bits) + 1 + 1 + kScanLaunches + 1 +
-                 (symmetric ? 2 + kScanLaunches : (spatial_density ? 3 : 1)) + (symmetric ? 2 : 1) + 3 + 1 + 2 +
-                 kScanLaunches + kJumpLaunches + 1 + 1;
+  // Morton boxes, nh, seeds, scan, jumps, finalize, event info
+  ws.launches += launches + 3 + 1 + kScanLaunches + kJumpLaunches + 1 + 1;
   CLUE_CUDA_TRY(cudaGetLastError());
   return CLUE_OK;
 }

@@ -57,9 +57,10 @@ constexpr int kScanLaunches = 3;
 void exclusive_scan(const uint32_t* in, uint32_t* out, size_t len, uint32_t* scratch,
                     uint32_t* total, cudaStream_t s);
 
-// offsets[b] = first position of key b in sorted keys (b = 0..nkeys), n at the end.
+// offsets[b] = first position of key b in sorted keys (b = 0..nkeys), n at the end; the key of
+// an entry is its value shifted right by `shift` bits.
 void offsets_from_sorted(const uint32_t* sorted_keys, int n, int nkeys, int32_t* offsets,
-                         cudaStream_t s);
+                         cudaStream_t s, int shift = 0);
 
 // ---- per-dimension pipeline (clue_dim.cu, one instantiation per N) ----------
 struct Workspace;
@@ -115,6 +116,7 @@ struct Workspace {
   uint32_t* mkeys_alt = nullptr;  // second key buffer of the Morton sort
   int32_t* minv = nullptr;        // tile-sorted position -> Morton position (alias after the sort)
   float4* rec_m = nullptr;        // records in Morton order inside every tile
+  const float4* rec_m_cur = nullptr;  // Morton-ordered records the sweeps of this run read
   float4* sblk = nullptr;         // bounding boxes of 1024-record super-blocks
   int32_t* mq = nullptr;          // Morton position -> tile-sorted position (alias after the sort)
   int32_t* ord_rho = nullptr;     // per-tile home order for the one-sided density sweeps

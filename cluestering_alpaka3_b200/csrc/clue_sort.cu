@@ -206,11 +206,11 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_down(const uint32_t* in, 
   }
 }
 
-__global__ void k_offsets(const uint32_t* __restrict__ keys, int n, int nkeys, int32_t* __restrict__ off) {
+__global__ void k_offsets(const uint32_t* __restrict__ keys, int n, int nkeys, int shift, int32_t* __restrict__ off) {
   const int stride = gridDim.x * blockDim.x;
   for (int pos = blockIdx.x * blockDim.x + threadIdx.x; pos <= n; pos += stride) {
-    const int prev = pos > 0 ? (int)keys[pos - 1] : -1;
-    const int cur = pos < n ? (int)keys[pos] : nkeys;
+    const int prev = pos > 0 ? (int)(keys[pos - 1] >> shift) : -1;
+    const int cur = pos < n ? (int)(keys[pos] >> shift) : nkeys;
     for (int b = prev + 1; b <= cur; ++b) off[b] = pos;
   }
 }
@@ -246,11 +246,12 @@ int radix_sort_pairs(uint32_t* keys[2], int32_t* vals[2], bool vals_identity, in
   return cur;
 }
 
-void offsets_from_sorted(const uint32_t* sorted_keys, int n, int nkeys, int32_t* offsets, cudaStream_t s) {
+void offsets_from_sorted(const uint32_t* sorted_keys, int n, int nkeys, int32_t* offsets, cudaStream_t s,
+                         int shift) {
   const int threads = 256;
   int blocks = (n + 1 + threads - 1) / threads;
   if (blocks > 148 * 16) blocks = 148 * 16;
-  k_offsets<<<blocks, threads, 0, s>>>(sorted_keys, n, nkeys, offsets);
+  k_offsets<<<blocks, threads, 0, s>>>(sorted_keys, n, nkeys, shift, offsets);
 }
 
 }  // namespace clue_b200
