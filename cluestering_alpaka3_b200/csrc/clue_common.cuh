@@ -321,6 +321,62 @@ struct Metric<N, CLUE_METRIC_WEIGHTED_CHEBYSHEV> {
   CLUE_HD static float finish(float s) { return s; }
 };
 
+#if defined(__CUDACC__)
+// Paired single-precision arithmetic (sm_100 f32x2 instructions: two IEEE round-to-nearest
+// operations in one issue slot, each rounded exactly like its scalar form).
+__device__ __forceinline__ unsigned long long pk2(float2 v) {
+  unsigned long long u;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(u) : "f"(v.x), "f"(v.y));
+  return u;
+}
+__device__ __forceinline__ float2 upk2(unsigned long long u) {
+  float2 v;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(v.x), "=f"(v.y) : "l"(u));
+  return v;
+}
+__device__ __forceinline__ float2 add2(float2 a, float2 b) {
+  unsigned long long r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk2(a)), "l"(pk2(b)));
+  return upk2(r);
+}
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
+  unsigned long long r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk2(a)), "l"(pk2(b)));
+  return upk2(r);
+}
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) {
+  unsigned long long r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(pk2(a)), "l"(pk2(b)));
+  return upk2(r);
+}
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) {
+  unsigned long long r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(pk2(a)), "l"(pk2(b)), "l"(pk2(c)));
+  return upk2(r);
+}
+
+// Metric values of one point against two others, bit-identical to two Metric::partial calls;
+// the Euclidean metric takes paired differences and squares.  The sums stay scalar: ptxas
+// (CUDA 12.9) contracts a paired multiply feeding a paired add into a fused multiply-add even
+// under --fmad=false, which would change the rounding.
+template <int N, int MT>
+__device__ __forceinline__ float2 partial_pair(const float* x, const float* a, const float* b, const float* mpar) {
+  if constexpr (MT == CLUE_METRIC_EUCLIDEAN) {
+    float2 df = sub2(make_float2(x[N - 1], x[N - 1]), make_float2(a[N - 1], b[N - 1]));
+    float2 acc = mul2(df, df);
+#pragma unroll
+    for (int d = N - 2; d >= 0; --d) {
+      df = sub2(make_float2(x[d], x[d]), make_float2(a[d], b[d]));
+      const float2 t = mul2(df, df);
+      acc = make_float2(fadd(t.x, acc.x), fadd(t.y, acc.y));
+    }
+    return acc;
+  } else {
+    return make_float2(Metric<N, MT>::partial(x, a, mpar), Metric<N, MT>::partial(x, b, mpar));
+  }
+}
+#endif
+
 // ---- convolutional kernels (core/detail/ConvolutionalKernel.hpp:16-65) -------
 #if defined(__CUDACC__)
 // Hardware approximations used by the spatial-order density (whose sums are not bit-exact):

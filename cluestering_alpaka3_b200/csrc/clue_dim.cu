@@ -1121,10 +1121,7 @@ __global__ void __launch_bounds__(kTileThreads, N <= 2 ? 8 : (N <= 4 ? 6 : 4)) k
                       [&](int p0, int p1, bool need, int64_t lexpos) {
     const int cnt = p1 - p0;
     stage_block<N>(sm, rec_m, p0, cnt, sq, mq);
-    auto pair = [&](int j, bool in_block) {
-      float c[N], rho_j;
-      smem_rec<N>(sm, j, c, rho_j);
-      const float s = M::partial(x, c, kp.mpar);
+    auto consider = [&](int j, float s, float rho_j, bool in_block) {
       if (need && in_block && s <= bnd && rho_j >= rho_i) {
         const int q = sq[j];
         int orig_j = -1;
@@ -1166,9 +1163,21 @@ __global__ void __launch_bounds__(kTileThreads, N <= 2 ? 8 : (N <= 4 ? 6 : 4)) k
         }
       }
     };
-    for (int j0 = 0; j0 < cnt; j0 += 4) {
-#pragma unroll
-      for (int u = 0; u < 4; ++u) pair(j0 + u, j0 + u < cnt);
+    // two candidates at a time: their metric values and densities first, then the update,
+    // entered only when some lane holds a candidate that passes the bound (the bound only
+    // shrinks between the two, and consider() checks it again)
+    for (int j = 0; j < cnt; j += 2) {
+      float ca[N], cb[N], ra, rb;
+      smem_rec<N>(sm, j, ca, ra);
+      smem_rec<N>(sm, j + 1, cb, rb);
+      // paired differences and squares pay from three dimensions on (measured)
+      const float2 s2 = N >= 3 ? partial_pair<N, MT>(x, ca, cb, kp.mpar)
+                               : make_float2(M::partial(x, ca, kp.mpar), M::partial(x, cb, kp.mpar));
+      const bool any = (s2.x <= bnd && ra >= rho_i) || (j + 1 < cnt && s2.y <= bnd && rb >= rho_i);
+      if (__any_sync(0xffffffffu, need && any)) {
+        consider(j, s2.x, ra, true);
+        consider(j + 1, s2.y, rb, j + 1 < cnt);
+      }
     }
   });
   if (valid) {
@@ -1357,6 +1366,19 @@ __global__ void __launch_bounds__(kTileThreads, N <= 4 ? 8 : 4) k_density_sym(
     const float dist = M::kRoot ? sqrt_approx(s) : s;
     return self ? 1.0f : kernel_value_fast(kp.kernel_type, kp.kpar, kp.ginv, dist);
   };
+  const float2 kexp2 = make_float2(kexp, kexp);
+  auto kval2 = [&](float2 s) -> float2 {
+    if (FORM == kDensExpUnit) {
+      const float2 d = M::kRoot ? make_float2(sqrt_approx(s.x), sqrt_approx(s.y)) : s;
+      const float2 e = mul2(kexp2, d);
+      return make_float2(ex2_approx(e.x), ex2_approx(e.y));
+    }
+    if (FORM == kDensGauss0Unit) {
+      const float2 e = mul2(kexp2, M::kRoot ? s : mul2(s, s));
+      return make_float2(ex2_approx(e.x), ex2_approx(e.y));
+    }
+    return make_float2(kval(s.x, false), kval(s.y, false));
+  };
   float acc = 0.0f;
   // block A against itself, one-sided (the self pair gives the reference's self term)
   {
@@ -1392,9 +1414,9 @@ __global__ void __launch_bounds__(kTileThreads, N <= 4 ? 8 : 4) k_density_sym(
         const int first = pb + (b << 5);
         const int cntB = min(32, pe - first);
         const bool cv = lane < cntB;
-        // lane m owns candidate m of the block; at step k lane l meets candidate (l + k) mod 32
-        // and the candidate's owner collects the term from lane (m - k) mod 32, so no value is
-        // carried from one step to the next
+        // lane m owns candidate m of the block; at step k lane l meets candidate l ^ k and the
+        // candidate's owner collects the term from lane m ^ k = l (butterfly shuffles with
+        // immediate lane masks), so no value is carried from one step to the next
         float ox[N], ow;
         load_rec<N>(rec_m, first + (cv ? lane : 0), ox, ow);
         if (!cv) {
@@ -1402,21 +1424,30 @@ __global__ void __launch_bounds__(kTileThreads, N <= 4 ? 8 : 4) k_density_sym(
           for (int d = 0; d < N; ++d) ox[d] = INFINITY;  // never within dc
           ow = 0.0f;
         }
-        float cacc = 0.0f;
-#pragma unroll 4
-        for (int k = 0; k < 32; ++k) {
-          const int src = (lane + k) & 31;
-          float cx[N];
+        // two steps at a time, with paired arithmetic; the own terms of this block are summed
+        // (fused multiply-add) in two running sums, even and odd steps, added at the block's end
+        float2 acc2 = make_float2(0.0f, 0.0f), cacc2 = make_float2(0.0f, 0.0f);
+        const float2 wi2 = make_float2(wi, wi);
 #pragma unroll
-          for (int d = 0; d < N; ++d) cx[d] = __shfl_sync(0xffffffffu, ox[d], src);
-          const float cw = __shfl_sync(0xffffffffu, ow, src);
-          const float sd = M::partial(x, cx, kp.mpar);
-          const bool in = hv && sd <= tdc;
-          const float kv = kval(sd, false);
-          if (in) acc = fadd(acc, kv * cw);
-          const float tc = in ? kv * wi : 0.0f;
-          cacc = fadd(cacc, __shfl_sync(0xffffffffu, tc, (lane - k) & 31));
+        for (int k = 0; k < 32; k += 2) {
+          float ca[N], cb[N];
+#pragma unroll
+          for (int d = 0; d < N; ++d) {
+            ca[d] = __shfl_xor_sync(0xffffffffu, ox[d], k);
+            cb[d] = __shfl_xor_sync(0xffffffffu, ox[d], k + 1);
+          }
+          const float2 cw = make_float2(__shfl_xor_sync(0xffffffffu, ow, k), __shfl_xor_sync(0xffffffffu, ow, k + 1));
+          const float2 sd = partial_pair<N, MT>(x, ca, cb, kp.mpar);
+          float2 kv = kval2(sd);
+          kv.x = hv && sd.x <= tdc ? kv.x : 0.0f;
+          kv.y = hv && sd.y <= tdc ? kv.y : 0.0f;
+          acc2 = fma2(kv, cw, acc2);
+          const float2 tc = mul2(kv, wi2);
+          cacc2 = add2(cacc2, make_float2(__shfl_xor_sync(0xffffffffu, tc.x, k),
+                                          __shfl_xor_sync(0xffffffffu, tc.y, k + 1)));
         }
+        acc = fadd(acc, fadd(acc2.x, acc2.y));
+        const float cacc = fadd(cacc2.x, cacc2.y);
         if (cv && cacc != 0.0f)
           atomicAdd(reinterpret_cast<unsigned long long*>(rho_fix + mq[first + lane]),
                     (unsigned long long)__float2ll_rn(cacc * scale));
