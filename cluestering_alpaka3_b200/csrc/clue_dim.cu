@@ -1121,8 +1121,26 @@ __global__ void __launch_bounds__(kTileThreads, N <= 2 ? 8 : (N <= 4 ? 6 : 4)) k
                       [&](int p0, int p1, bool need, int64_t lexpos) {
     const int cnt = p1 - p0;
     stage_block<N>(sm, rec_m, p0, cnt, sq, mq);
+    // Update of the lane's best by candidate j (called by the whole warp).  The common case, a
+    // strictly denser candidate whose distance rounds strictly below the best one's, is a
+    // predicated update; equal densities (index rule) and distances that may round to the best
+    // one's (rank rule) take the full test, entered only when some lane has such a case.
     auto consider = [&](int j, float s, float rho_j, bool in_block) {
-      if (need && in_block && s <= bnd && rho_j >= rho_i) {
+      const bool c = need && in_block && s <= bnd && rho_j >= rho_i;
+      const bool fast = c && rho_j > rho_i && s * slack < s_best;
+      if (fast) {
+        s_best = s;
+        bnd = fminf(tdm, s * slack);
+        nh = sq[j];
+        lex_best = (int)lexpos;
+        if (TIE != CLUE_TIE_REFERENCE) {
+          rho_best = rho_j;
+          orig_best = -1;  // read from perm when a tie needs it
+        }
+      }
+      const bool slow = c && !fast;
+      if (!__any_sync(0xffffffffu, slow)) return;
+      if (slow) {
         const int q = sq[j];
         int orig_j = -1;
         bool higher = rho_j > rho_i;
