@@ -1084,6 +1084,13 @@ __global__ void __launch_bounds__(kTileThreads) k_density(const KParams kp, Even
 // (or than dm) or holds no density reaching the lane's.  TIE == CLUE_TIE_RHO_INDEX resolves equal
 // distances by higher rho, then lower index.
 
+#ifndef CLUE_NH_COMPACT
+#define CLUE_NH_COMPACT 8
+#endif
+// Largest number of lanes that need a candidate block for the block's candidates to be split
+// among all the warp's lanes.
+constexpr int kNhCompact = CLUE_NH_COMPACT;
+
 template <int N, int MT, int TIE>
 __global__ void __launch_bounds__(kTileThreads, N <= 2 ? 8 : (N <= 4 ? 6 : 4)) k_nearest_higher(
     const KParams kp, Events ev, const int32_t* __restrict__ off, const int32_t* __restrict__ ord,
@@ -1181,6 +1188,71 @@ __global__ void __launch_bounds__(kTileThreads, N <= 2 ? 8 : (N <= 4 ? 6 : 4)) k
         }
       }
     };
+    // Few lanes need this block: its candidates are split among all 32 lanes, G lanes per
+    // needing home (G = 32 / P, P >= the number of such homes, a power of two); each group finds
+    // its home's best candidate of the block, and the home lane takes it through consider().
+    // Inside one block every candidate has the same search-box position, so the best is the
+    // least (rounded distance, then [density, for TIE_RHO_INDEX] then original index), a strict
+    // total order that the group reduces exactly.
+    const unsigned nm = __ballot_sync(0xffffffffu, need);
+    const int k = __popc(nm);
+    if (k <= kNhCompact) {
+      const int lg = k <= 1 ? 5 : (k <= 2 ? 4 : (k <= 4 ? 3 : (k <= 8 ? 2 : 1)));  // log2 G
+      const int lane = threadIdx.x & 31;
+      const int hs = lane >> lg;  // home slot of this lane's group
+      unsigned m = nm;
+      for (int i = 0; i < hs && m; ++i) m &= m - 1;
+      const bool gv = hs < k;
+      const int hl = gv ? __ffs(m) - 1 : 0;  // lane of the group's home
+      float xh[N];
+#pragma unroll
+      for (int d = 0; d < N; ++d) xh[d] = __shfl_sync(0xffffffffu, x[d], hl);
+      const float rho_h = __shfl_sync(0xffffffffu, rho_i, hl);
+      const float bnd_h = __shfl_sync(0xffffffffu, bnd, hl);
+      const int orig_h = __shfl_sync(0xffffffffu, orig_i, hl);
+      // a before b (both higher than the home, same tile)
+      auto less = [&](float sa, float ra, int ja, float sb, float rb, int jb) -> bool {
+        if (sa * slack < sb) return true;
+        if (sb * slack < sa) return false;
+        const float da = M::finish(sa), db = M::finish(sb);
+        if (da != db) return da < db;
+        if (TIE != CLUE_TIE_REFERENCE && ra != rb) return ra > rb;
+        return __ldg(perm + sq[ja]) < __ldg(perm + sq[jb]);
+      };
+      float s_loc = INFINITY, r_loc = 0.0f;
+      int j_loc = -1;
+      const int G = 1 << lg;
+      for (int j = lane & (G - 1); j < cnt; j += G) {
+        float c[N], rj;
+        smem_rec<N>(sm, j, c, rj);
+        const float sj = M::partial(xh, c, kp.mpar);
+        if (gv && sj <= bnd_h && rj >= rho_h) {
+          bool higher = rj > rho_h;
+          if (!higher && rj > 0.0f) higher = __ldg(perm + sq[j]) > orig_h;
+          if (higher && (j_loc < 0 || less(sj, rj, j, s_loc, r_loc, j_loc))) {
+            s_loc = sj;
+            r_loc = rj;
+            j_loc = j;
+          }
+        }
+      }
+      for (int o = G >> 1; o > 0; o >>= 1) {
+        const float s_o = __shfl_xor_sync(0xffffffffu, s_loc, o);
+        const float r_o = __shfl_xor_sync(0xffffffffu, r_loc, o);
+        const int j_o = __shfl_xor_sync(0xffffffffu, j_loc, o);
+        if (j_o >= 0 && (j_loc < 0 || less(s_o, r_o, j_o, s_loc, r_loc, j_loc))) {
+          s_loc = s_o;
+          r_loc = r_o;
+          j_loc = j_o;
+        }
+      }
+      const int src = need ? __popc(nm & ((1u << lane) - 1u)) << lg : 0;
+      const float s_g = __shfl_sync(0xffffffffu, s_loc, src);
+      const float r_g = __shfl_sync(0xffffffffu, r_loc, src);
+      const int j_g = __shfl_sync(0xffffffffu, j_loc, src);
+      consider(j_g >= 0 ? j_g : 0, s_g, r_g, j_g >= 0);
+      return;
+    }
     // two candidates at a time: their metric values and densities first, then the update,
     // entered only when some lane holds a candidate that passes the bound (the bound only
     // shrinks between the two, and consider() checks it again)
