@@ -529,52 +529,80 @@ __device__ __forceinline__ int warp_event(const int32_t* __restrict__ ev_pt, int
   return uniform ? e0 : (active ? find_event(ev_pt, E, i) : e0);
 }
 
-// Bounding box and largest |weight| of many events: grid-stride over points; a warp whose points
-// share an event reduces them before its atomics.
+// Bounding box and largest |weight| of many events.  Every warp takes spans of `span`
+// consecutive points (a multiple of 32) and keeps a running box while its 32-point groups stay
+// inside one event, so a span inside an event costs one warp reduction and 2N + 1 atomics; a
+// group that straddles events falls back to per-lane atomics.
 template <int N>
 __global__ void __launch_bounds__(256) k_bbox_events(InPtrs in, int n, int E, const int32_t* __restrict__ ev_pt,
-                                                     EvGrid* eg, DevStatus* st) {
-  const int stride = gridDim.x * blockDim.x;
+                                                     EvGrid* eg, DevStatus* st, int span) {
+  const int lane = threadIdx.x & 31;
+  const int nwarps = (gridDim.x * blockDim.x) >> 5;
   bool bad = false;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-    bool uniform;
-    const int e = warp_event(ev_pt, E, i, true, uniform);
-    uint32_t emn[N], emx[N];
+  for (int base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * span; base < n; base += nwarps * span) {
+    const int end = min(n, base + span);
+    int cur = -1;  // event of the running box (warp-uniform), -1: none
+    uint32_t amn[N], amx[N], aw = 0;
 #pragma unroll
-    for (int d = 0; d < N; ++d) {
-      const float x = in.c[d][i];
-      bad |= !isfinite(x);
-      emn[d] = emx[d] = enc_float(x);
-    }
-    const float w = in.w[i];
-    bad |= !isfinite(w);
-    uint32_t wm = __float_as_uint(fabsf(w));
-    const unsigned am = __activemask();
-    if (uniform && am == 0xffffffffu) {
+    for (int d = 0; d < N; ++d) amn[d] = amx[d] = 0;
+    auto flush = [&]() {
 #pragma unroll
       for (int d = 0; d < N; ++d) {
-        emn[d] = warp_min_u(emn[d]);
-        emx[d] = warp_max_u(emx[d]);
+        amn[d] = warp_min_u(amn[d]);
+        amx[d] = warp_max_u(amx[d]);
       }
-      wm = warp_max_u(wm);
-      if ((threadIdx.x & 31) == 0) {
+      aw = warp_max_u(aw);
+      if (lane == 0) {
+#pragma unroll
+        for (int d = 0; d < N; ++d) {
+          atomicMin(&eg[cur].enc_min[d], amn[d]);
+          atomicMax(&eg[cur].enc_max[d], amx[d]);
+        }
+        atomicMax(&eg[cur].wmax_bits, aw);
+      }
+    };
+    for (int i0 = base; i0 < end; i0 += 32) {
+      const int i = min(i0 + lane, end - 1);  // lanes past the end repeat the last point
+      bool uniform;
+      const int e = warp_event(ev_pt, E, i, true, uniform);
+      uint32_t emn[N];
+#pragma unroll
+      for (int d = 0; d < N; ++d) {
+        const float x = in.c[d][i];
+        bad |= !isfinite(x);
+        emn[d] = enc_float(x);
+      }
+      const float w = in.w[i];
+      bad |= !isfinite(w);
+      const uint32_t wm = __float_as_uint(fabsf(w));
+      if (uniform && e == cur) {
+#pragma unroll
+        for (int d = 0; d < N; ++d) {
+          amn[d] = min(amn[d], emn[d]);
+          amx[d] = max(amx[d], emn[d]);
+        }
+        aw = max(aw, wm);
+        continue;
+      }
+      if (cur >= 0) flush();
+      if (uniform) {
+        cur = e;
+#pragma unroll
+        for (int d = 0; d < N; ++d) amn[d] = amx[d] = emn[d];
+        aw = wm;
+      } else {
+        cur = -1;
 #pragma unroll
         for (int d = 0; d < N; ++d) {
           atomicMin(&eg[e].enc_min[d], emn[d]);
-          atomicMax(&eg[e].enc_max[d], emx[d]);
+          atomicMax(&eg[e].enc_max[d], emn[d]);
         }
         atomicMax(&eg[e].wmax_bits, wm);
       }
-    } else {
-#pragma unroll
-      for (int d = 0; d < N; ++d) {
-        atomicMin(&eg[e].enc_min[d], emn[d]);
-        atomicMax(&eg[e].enc_max[d], emx[d]);
-      }
-      atomicMax(&eg[e].wmax_bits, wm);
     }
+    if (cur >= 0) flush();
   }
-  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&st->nonfinite, 1u);
+  if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(&st->nonfinite, 1u);
 }
 
 // Tile size (max - min) / nperdim in FP32 (ComputeTiles.hpp:20-23), per event.
@@ -631,6 +659,23 @@ struct MortonBits {
   static constexpr int kBits = kPerDim * N;
 };
 
+// The bits of c (below 2^kPerDim) moved to positions 0, N, 2N, ... of a Morton code.
+template <int N>
+__device__ __forceinline__ uint32_t spread_bits(uint32_t c) {
+  if constexpr (N == 1) {
+    return c;
+  } else if constexpr (N == 2) {  // 8 bits
+    c = (c | (c << 4)) & 0x0f0fu;
+    c = (c | (c << 2)) & 0x3333u;
+    return (c | (c << 1)) & 0x5555u;
+  } else {
+    uint32_t m = 0;
+#pragma unroll
+    for (int bit = 0; bit < MortonBits<N>::kPerDim; ++bit) m |= ((c >> bit) & 1u) << (bit * N);
+    return m;
+  }
+}
+
 // Morton key of every tile-sorted record inside its tile (tile keys are read from tile_keys).
 template <int N>
 __global__ void __launch_bounds__(256) k_morton_keys(const KParams kp, Events ev, const float4* __restrict__ rec,
@@ -681,13 +726,17 @@ __global__ void __launch_bounds__(256) k_bin_composite(const KParams kp, InPtrs 
     uint32_t m = 0;
 #pragma unroll
     for (int d = 0; d < N; ++d) {
+      // getBin without wrapped coordinates (the composite sort is only taken without them):
+      // the quotient also places the point inside its tile for the Morton code
       const float x = in.c[d][i];
-      const int b = get_bin(x, g->mn[d], g->mx[d], g->size[d], kp.wrapped[d] != 0, g->nperdim);
+      const float q = fdiv(fsub(x, g->mn[d]), g->size[d]);
+      int b = cvt_i32(q);
+      b = b < g->nperdim - 1 ? b : g->nperdim - 1;
+      b = b > 0 ? b : 0;
       gb += g->stride[d] * b;
-      const float t0 = g->mn[d] + (float)b * g->size[d];
-      int c = g->size[d] > 0.0f ? (int)((x - t0) / g->size[d] * scale) : 0;
+      int c = g->size[d] > 0.0f ? (int)((q - (float)b) * scale) : 0;
       c = c < 0 ? 0 : (c > (1 << bpd) - 1 ? (1 << bpd) - 1 : c);
-      for (int bit = 0; bit < bpd; ++bit) m |= (uint32_t)((c >> bit) & 1) << (bit * N + d);
+      m |= spread_bits<N>((uint32_t)c) << d;
     }
     keys[i] = ((uint32_t)gb << mbits) | (m >> (MortonBits<N>::kBits - mbits));
   }
@@ -1812,7 +1861,13 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
   if (kp.n_events == 1)
     k_bbox_single<N><<<grid_for(n, 256), 256, 0, s>>>(in, n, ws.ev, ws.status);
   else
-    k_bbox_events<N><<<grid_for(n, 256), 256, 0, s>>>(in, n, kp.n_events, ws.ev_pt, ws.ev, ws.status);
+  {
+    // spans of 32..1024 points: about four spans per resident warp (64 per SM) when there
+    // are enough points, so the loads of many spans are in flight
+    const int span = std::max(32, std::min(1024, (n / (148 * 64 * 4)) & ~31));
+    const int blocks = std::max(1, std::min(grid_for(n, 256), ((n + span - 1) / span + 7) / 8));
+    k_bbox_events<N><<<blocks, 256, 0, s>>>(in, n, kp.n_events, ws.ev_pt, ws.ev, ws.status, span);
+  }
   k_grid<N><<<grid_for(kp.n_events, 256), 256, 0, s>>>(kp.n_events, ws.ev);
   int launches = 4;  // init, bbox, grid, bin
   // density order: the reference's candidate order for the flat kernel (bit-exact sums), spatial

@@ -357,6 +357,29 @@ int oracle_tiles(const oracle_params* p, int32_t n, const float* coords, oracle_
   return 0;
 }
 
+/* Nearest-higher stage alone, on densities the caller supplies (KernelCalculateNearestHigher,
+ * ClusteringKernels.hpp:109-212, over the tiles of setup_tiles).  Lets a test check the
+ * candidate order and tie-break of an implementation whose densities differ from this
+ * restatement's in the last bits. */
+int oracle_nearest_higher(const oracle_params* p, int32_t n, const float* coords, const float* rho,
+                          int32_t* nearest_higher, float* delta, int64_t* distance_ties) {
+  if (check_params(p, n)) return -1;
+  grid_t g;
+  int32_t *off = NULL, *idx = NULL;
+  if (build_tiles(p, n, coords, &g, &off, &idx)) return -2;
+  ctx_t c = {p, &g, n, coords, NULL, off, idx};
+  int64_t cand = 0, ties = 0;
+  for (int32_t i = 0; i < n; ++i) {
+    float dl;
+    nearest_higher[i] = nh_point(&c, rho, i, &dl, &cand, &ties);
+    if (delta) delta[i] = dl;
+  }
+  if (distance_ties) *distance_ties = ties;
+  free(off);
+  free(idx);
+  return 0;
+}
+
 int oracle_run(const oracle_params* p, int32_t n, const float* coords, const float* weight,
                oracle_out* out) {
   if (check_params(p, n)) return -1;

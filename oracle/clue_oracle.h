@@ -80,6 +80,11 @@ int oracle_run(const oracle_params* p, int32_t n, const float* coords, const flo
 
 /* Tile grid + tile CSR (offsets[ntiles+1], indexes[n]); offsets/indexes may be NULL to
  * query the grid only. */
+/* Nearest-higher stage alone on caller-supplied densities (same grid, candidate order and
+ * tie-break as oracle_run).  delta and distance_ties may be NULL. */
+int oracle_nearest_higher(const oracle_params* p, int32_t n, const float* coords, const float* rho,
+                          int32_t* nearest_higher, float* delta, int64_t* distance_ties);
+
 int oracle_tiles(const oracle_params* p, int32_t n, const float* coords, oracle_grid* grid,
                  int32_t* offsets, int32_t* indexes);
 

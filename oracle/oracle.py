@@ -71,6 +71,10 @@ def _load():
         lib.oracle_rho_f64.argtypes = [ctypes.POINTER(_Params), ctypes.c_int32, ctypes.c_void_p,
                                        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double]
         lib.oracle_rho_f64.restype = ctypes.c_int
+        lib.oracle_nearest_higher.argtypes = [ctypes.POINTER(_Params), ctypes.c_int32, ctypes.c_void_p,
+                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                              ctypes.POINTER(ctypes.c_int64)]
+        lib.oracle_nearest_higher.restype = ctypes.c_int
         lib.oracle_metric.argtypes = [ctypes.POINTER(_Params), ctypes.c_void_p, ctypes.c_void_p]
         lib.oracle_metric.restype = ctypes.c_float
         lib.oracle_kernel.argtypes = [ctypes.POINTER(_Params), ctypes.c_float, ctypes.c_int32,
@@ -160,6 +164,27 @@ def run(coords: np.ndarray, weight: np.ndarray, cfg: Config) -> Result:
                                                "candidates_rho", "candidates_nh",
                                                "nh_distance_ties")}
     return res
+
+
+def nearest_higher(coords: np.ndarray, rho: np.ndarray, cfg: Config):
+    """Nearest-higher stage alone on the given densities: (nearest_higher, delta, distance ties).
+
+    Same grid, candidate order and tie-break as ``run`` (ClusteringKernels.hpp:109-212); used to
+    check an implementation's nearest-higher search on its own densities."""
+    lib = _load()
+    c = _soa(coords)
+    ndim, n = c.shape
+    r = np.ascontiguousarray(rho, dtype=np.float32)
+    assert r.shape == (n,)
+    nh = np.empty(n, np.int32)
+    delta = np.empty(n, np.float32)
+    ties = ctypes.c_int64(0)
+    p = cfg.to_struct(ndim)
+    rc = lib.oracle_nearest_higher(ctypes.byref(p), n, c.ctypes.data, r.ctypes.data, nh.ctypes.data,
+                                   delta.ctypes.data, ctypes.byref(ties))
+    if rc != 0:
+        raise ValueError(f"oracle_nearest_higher failed ({rc})")
+    return nh, delta, int(ties.value)
 
 
 def tiles(coords: np.ndarray, cfg: Config):

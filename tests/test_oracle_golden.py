@@ -97,3 +97,19 @@ def test_grid_shape_examples():
         g, off, idx = O.tiles(c, O.Config(1.0, 1.0))
         assert g["nperdim"] == npd
         assert off[-1] == n
+
+
+@pytest.mark.parametrize("tiebreak", ["reference", "rho_index"])
+def test_nearest_higher_stage_matches_full_run(tiebreak):
+    # the stage-alone entry reproduces the full run's nearest higher (before seeds are cut
+    # loose) and delta, on lattice coordinates with many exact distance ties
+    rng = np.random.default_rng(3)
+    c = rng.integers(0, 30, size=(2, 3000)).astype(np.float32)
+    w = np.ones(3000, np.float32)
+    cfg = O.Config(dc=1.5, rhoc=2.0, dm=2.5, tiebreak=tiebreak)
+    ref = O.run(c, w, cfg)
+    nh, delta, ties = O.nearest_higher(c, ref.rho, cfg)
+    keep = ref.is_seed == 0
+    np.testing.assert_array_equal(nh[keep], ref.nearest_higher[keep])
+    np.testing.assert_array_equal(delta.view(np.uint32), ref.delta.view(np.uint32))
+    assert ties == ref.stats["nh_distance_ties"] > 0

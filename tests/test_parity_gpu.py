@@ -292,3 +292,55 @@ def test_symmetric_density_deterministic_and_placement_free(gpu_context):
     res, _ = gpu_context.batch_host(coords, weight, [0, c1.shape[1], coords.shape[1]], p, k, m)
     np.testing.assert_array_equal(res.rho[c1.shape[1]:].view(np.uint32), alone.rho.view(np.uint32))
     np.testing.assert_array_equal(res.cluster_index[c1.shape[1]:], alone.cluster_index)
+
+
+def _nh_on_own_rho(got, c, cfg):
+    """The device's nearest higher and delta against the oracle's nearest-higher stage run on
+    the device's own densities (bit for bit, ties included)."""
+    nh, delta, ties = O.nearest_higher(c, got.rho, cfg)
+    keep = got.is_seed == 0
+    np.testing.assert_array_equal(got.nearest_higher[keep], nh[keep], err_msg="nearest_higher")
+    np.testing.assert_array_equal(got.delta.view(np.uint32), delta.view(np.uint32), err_msg="delta bits")
+    return ties
+
+
+@pytest.mark.parametrize("tiebreak", ["reference", "rho_index"])
+@pytest.mark.parametrize("kernel,metric,ndim", [(("exp", (1.0, 1.0)), ("euclidean", ()), 2),
+                                                (("gaus", (0.0, 0.8, 1.0)), ("euclidean", ()), 3),
+                                                (("exp", (0.7, 2.0)), ("manhattan", ()), 2),
+                                                (("gaus", (0.5, 1.0, 1.3)), ("chebyshev", ()), 2)])
+def test_symmetric_path_nearest_higher_ties_exact(gpu_context, kernel, metric, ndim, tiebreak):
+    # The symmetric density path sorts each tile's points by Morton code, not by index, and
+    # ranks equal distances by (search-box position of the tile, original index).  Integer
+    # lattice coordinates give many exact distance ties; weights from a few values give equal
+    # densities.
+    from parity_util import oracle_cfg, gpu_args
+    rng = np.random.default_rng(120 + ndim)
+    n = 6000
+    c = rng.integers(0, 25 if ndim == 2 else 12, size=(ndim, n)).astype(np.float32)
+    w = rng.choice(np.array([0.5, 1.0, 1.5], np.float32), size=n)
+    kw = dict(dc=1.5, rhoc=2.0, dm=2.5, kernel=kernel, metric=metric, tiebreak=tiebreak)
+    got = gpu_context.make_clusters_host(c, w, *gpu_args(**kw))
+    ties = _nh_on_own_rho(got, c, oracle_cfg(**kw))
+    assert ties > 0
+
+
+def test_symmetric_path_nearest_higher_batched_exact(gpu_context):
+    # the same check per event inside one batched call (events of uneven size)
+    from parity_util import oracle_cfg, gpu_args
+    rng = np.random.default_rng(133)
+    sizes = [1, 40, 700, 3000, 129, 2500]
+    cs = [rng.integers(0, 20, size=(2, s)).astype(np.float32) for s in sizes]
+    ws = [rng.choice(np.array([0.5, 1.0, 1.5], np.float32), size=s) for s in sizes]
+    off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int32)
+    kw = dict(dc=1.5, rhoc=2.0, dm=2.5, kernel=("exp", (1.0, 1.0)))
+    res, _ = gpu_context.batch_host(np.ascontiguousarray(np.concatenate(cs, axis=1)), np.concatenate(ws),
+                                    off, *gpu_args(**kw))
+    cfg = oracle_cfg(**kw)
+    for e, c in enumerate(cs):
+        a, b = off[e], off[e + 1]
+        nh, delta, _ = O.nearest_higher(c, res.rho[a:b], cfg)
+        keep = res.is_seed[a:b] == 0
+        got_nh = res.nearest_higher[a:b]  # batch-wide indices
+        np.testing.assert_array_equal(np.where(got_nh >= 0, got_nh - a, -1)[keep], nh[keep], err_msg=f"event {e}")
+        np.testing.assert_array_equal(res.delta[a:b].view(np.uint32), delta.view(np.uint32), err_msg=f"event {e}")
