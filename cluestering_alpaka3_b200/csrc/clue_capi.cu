@@ -250,6 +250,12 @@ static clue_status reserve_stage(Workspace& ws, size_t bytes) {
 void workspace_release(Workspace& ws) {
   for (auto& e : ws.tev)
     if (e) cudaEventDestroy(e);
+  for (auto& e : ws.pipe_ev)
+    if (e) cudaEventDestroy(e);
+  if (ws.pipe_h2d) cudaStreamDestroy(ws.pipe_h2d);
+  if (ws.pipe_d2h) cudaStreamDestroy(ws.pipe_d2h);
+  if (ws.pipe_status_host) cudaFreeHost(ws.pipe_status_host);
+  if (ws.pipe_pinned) cudaFreeHost(ws.pipe_pinned);
   if (ws.arena) cudaFree(ws.arena);
   if (ws.dstage) cudaFree(ws.dstage);
   if (ws.status_host) cudaFreeHost(ws.status_host);
@@ -962,21 +968,12 @@ static clue_status upload_events(Workspace& ws, int E, cudaStream_t s) {
   return CLUE_OK;
 }
 
-}  // namespace clue_b200
-
-struct clue_graph_s {
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  int device = 0;
-};
-
-extern "C" {
-
-clue_status clue_batch_make_clusters(clue_context ctx, const clue_params* params, const clue_kernel* kernel,
-                                     const clue_metric* metric, int32_t ndim, int32_t n_events,
-                                     const int32_t* event_offsets, const float* coords, const float* weight,
-                                     const clue_outputs* out, int32_t* ev_n_clusters, int32_t memory,
-                                     void* stream, clue_run_info* info) {
+// One pass over the whole batch: inputs copied in (host memory), pipeline, outputs copied out.
+static clue_status batch_plain(clue_context ctx, const clue_params* params, const clue_kernel* kernel,
+                               const clue_metric* metric, int32_t ndim, int32_t n_events,
+                               const int32_t* event_offsets, const float* coords, const float* weight,
+                               const clue_outputs* out, int32_t* ev_n_clusters, int32_t memory, void* stream,
+                               clue_run_info* info) {
   RunArgs a;
   clue_status st = prepare_batch(ctx, params, kernel, metric, ndim, n_events, event_offsets, out, a);
   if (st != CLUE_OK) return st;
@@ -1044,6 +1041,327 @@ clue_status clue_batch_make_clusters(clue_context ctx, const clue_params* params
   if (st == CLUE_OK && info) info->n_per_dim = 0;
   cudaSetDevice(prev);
   return st;
+}
+
+__global__ void k_shift_indices(int32_t* __restrict__ v, int n, int32_t by) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+    if (v[i] >= 0) v[i] += by;
+}
+
+__global__ void k_save_status(const DevStatus* __restrict__ st, const uint32_t* __restrict__ total,
+                              DevStatus* __restrict__ dst, uint32_t* __restrict__ dst_total) {
+  const uint32_t* a = reinterpret_cast<const uint32_t*>(st);
+  uint32_t* b = reinterpret_cast<uint32_t*>(dst);
+  for (int i = threadIdx.x; i < (int)(sizeof(DevStatus) / 4); i += blockDim.x) b[i] = a[i];
+  if (threadIdx.x == 0) *dst_total = *total;
+}
+
+// Host-memory batches of at least this many points overlap their copies with the pipeline.
+constexpr int64_t kPipeMinPoints = 4000000;
+// Points per chunk the overlapped path aims at (2..kPipeMaxChunks chunks).
+#ifndef CLUE_PIPE_CHUNK_POINTS
+#define CLUE_PIPE_CHUNK_POINTS 4400000
+#endif
+constexpr int64_t kPipeChunkPoints = CLUE_PIPE_CHUNK_POINTS;
+
+// Whether a host-memory batch takes the overlapped path: large, several events, valid (an
+// invalid request goes to the plain path, which reports it).
+static bool batch_overlap_ok(clue_context ctx, const clue_params* params, const clue_kernel* kernel,
+                             const clue_metric* metric, int32_t ndim, int32_t n_events, const int32_t* ev_off,
+                             const float* coords, const float* weight, const clue_outputs* out) {
+  if (!ctx || !params || !kernel || !metric || !ev_off || !coords || !weight || !out || !out->cluster_index)
+    return false;
+  if (n_events < 2 || ev_off[0] != 0 || ev_off[n_events] < kPipeMinPoints) return false;
+  if (clue_check_params(params) != CLUE_OK || clue_check_kernel(kernel) != CLUE_OK ||
+      clue_check_metric(metric, ndim) != CLUE_OK)
+    return false;
+  for (int e = 0; e < n_events; ++e) {
+    if (ev_off[e + 1] <= ev_off[e]) return false;
+    int32_t npd, nt;
+    grid_shape(ev_off[e + 1] - ev_off[e], params->points_per_tile, ndim, &npd, &nt);
+    if (nt <= 0) return false;
+  }
+  return true;
+}
+
+// A large host-memory batch in K chunks of whole events, so the copies overlap the pipeline:
+// every chunk's event table and inputs go up on a copy stream (all enqueued at once, each chunk
+// with its own pinned and device event table, since a copy engine runs its queue in order and
+// a small copy on the compute stream would wait behind all the inputs), chunk c runs on the
+// caller's stream once its copies are in, and its outputs come down on a second copy stream
+// while chunk c + 1 runs.  Events are independent and a chunk's results do not depend on the
+// other events in it, so the outputs are those of one pass over the whole batch (nearest-higher
+// indices are shifted to the batch).  The rare chunk whose label chains outlast the fixed
+// pointer-jumping rounds is run again alone.
+static clue_status batch_host_overlapped(clue_context ctx, const clue_params* params, const clue_kernel* kernel,
+                                         const clue_metric* metric, int32_t ndim, int32_t n_events,
+                                         const int32_t* ev_off, const float* coords, const float* weight,
+                                         const clue_outputs* out, int32_t* ev_n_clusters, void* stream,
+                                         clue_run_info* info) {
+  constexpr int KM = Workspace::kPipeMaxChunks;
+  Workspace& ws = ctx->ws;
+  const int64_t n = ev_off[n_events];
+  const size_t nn = (size_t)n;
+  int K = (int)std::min<int64_t>(KM, std::max<int64_t>(2, n / kPipeChunkPoints));
+  K = std::min(K, (int)n_events);
+  // chunk sizes in the ratio 1 : 2 : ... : 2 : 1 -- only the first chunk's copy-in and the last
+  // chunk's copy-out are not hidden behind a pipeline run
+  std::vector<int> cut(1, 0);  // first event of every chunk, then n_events
+  const int64_t parts = 2 * (int64_t)K - 2;
+  for (int e = 1; e < n_events && (int)cut.size() < K; ++e) {
+    const int64_t c = (int64_t)cut.size();  // chunk that would start at e
+    const int64_t before = 2 * c - 1;       // parts in chunks 0 .. c - 1
+    if ((int64_t)ev_off[e] * parts >= before * n) cut.push_back(e);
+  }
+  cut.push_back(n_events);
+  K = (int)cut.size() - 1;
+  size_t max_n = 0, max_tiles = 0, max_ev = 0;
+  std::vector<int64_t> chunk_tiles(K, 0);
+  for (int c = 0; c < K; ++c) {
+    for (int e = cut[c]; e < cut[c + 1]; ++e) {
+      int32_t npd, nt;
+      grid_shape(ev_off[e + 1] - ev_off[e], params->points_per_tile, ndim, &npd, &nt);
+      chunk_tiles[c] += nt;
+    }
+    max_n = std::max(max_n, (size_t)(ev_off[cut[c + 1]] - ev_off[cut[c]]));
+    max_tiles = std::max(max_tiles, (size_t)chunk_tiles[c]);
+    max_ev = std::max(max_ev, (size_t)(cut[c + 1] - cut[c]));
+  }
+  clue_status st = workspace_reserve(ws, ndim, max_n, max_tiles, max_ev);
+  if (st != CLUE_OK) return st;
+  int prev = 0;
+  CLUE_CUDA_TRY(cudaGetDevice(&prev));
+  CLUE_CUDA_TRY(cudaSetDevice(ws.device));
+  struct DeviceGuard {
+    int prev;
+    ~DeviceGuard() { cudaSetDevice(prev); }
+  } guard{prev};
+  const size_t io_bytes = align_up((nn * (size_t)(ndim + 1) + 5 * nn + (size_t)n_events) * 4, 256);
+  const size_t status_bytes = align_up(KM * (sizeof(DevStatus) + 4), 256);
+  std::vector<size_t> dev_tab(K + 1, 0);  // every chunk's device event table, after the statuses
+  for (int c = 0; c < K; ++c) dev_tab[c + 1] = dev_tab[c] + align_up(event_table_bytes(cut[c + 1] - cut[c]), 256);
+  if ((st = reserve_stage(ws, io_bytes + status_bytes + dev_tab[K])) != CLUE_OK) return st;
+  if (!ws.pipe_h2d) {
+    CLUE_CUDA_TRY(cudaStreamCreateWithFlags(&ws.pipe_h2d, cudaStreamNonBlocking));
+    CLUE_CUDA_TRY(cudaStreamCreateWithFlags(&ws.pipe_d2h, cudaStreamNonBlocking));
+    for (auto& e : ws.pipe_ev) CLUE_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    CLUE_CUDA_TRY(cudaMallocHost((void**)&ws.pipe_status_host, KM * (sizeof(DevStatus) + 4)));
+  }
+  const size_t host_tab = event_table_bytes(ws.cap_events);  // one pinned table per chunk
+  if (ws.pipe_pinned_bytes < (size_t)K * host_tab) {
+    if (ws.pipe_pinned) cudaFreeHost(ws.pipe_pinned);
+    ws.pipe_pinned = nullptr;
+    ws.pipe_pinned_bytes = 0;
+    CLUE_CUDA_TRY(cudaMallocHost(&ws.pipe_pinned, (size_t)KM * host_tab));
+    ws.pipe_pinned_bytes = (size_t)KM * host_tab;
+  }
+  cudaStream_t s = (cudaStream_t)stream, h2d = ws.pipe_h2d, d2h = ws.pipe_d2h;
+  float* dcoords = static_cast<float*>(ws.dstage);
+  float* dweight = dcoords + nn * ndim;
+  int32_t* o = reinterpret_cast<int32_t*>(dweight + nn);
+  clue_outputs dev_out{};
+  dev_out.cluster_index = o;
+  dev_out.is_seed = out->is_seed ? o + nn : nullptr;
+  dev_out.rho = out->rho ? reinterpret_cast<float*>(o + 2 * nn) : nullptr;
+  dev_out.nearest_higher = out->nearest_higher ? o + 3 * nn : nullptr;
+  dev_out.delta = out->delta ? reinterpret_cast<float*>(o + 4 * nn) : nullptr;
+  int32_t* dev_ncl = ev_n_clusters ? o + 5 * nn : nullptr;
+  DevStatus* dslot = reinterpret_cast<DevStatus*>(static_cast<char*>(ws.dstage) + io_bytes);
+  uint32_t* dtotal = reinterpret_cast<uint32_t*>(dslot + KM);
+  char* dtab = static_cast<char*>(ws.dstage) + io_bytes + status_bytes;
+  cudaEvent_t ev_start = ws.pipe_ev[0];
+  auto ev_in = [&](int c) { return ws.pipe_ev[1 + 3 * c]; };
+  auto ev_done = [&](int c) { return ws.pipe_ev[3 + 3 * c]; };
+
+  // 1. every chunk's grids and parameters, each event table in its own pinned slot (the host
+  //    never waits for the GPU before all chunks are enqueued)
+  std::vector<RunArgs> args(K);
+  std::vector<int32_t> rel;
+  void* pinned_main = ws.pinned;
+  for (int c = 0; c < K && st == CLUE_OK; ++c) {
+    const int e0 = cut[c], E = cut[c + 1] - e0;
+    rel.assign(ev_off + e0, ev_off + e0 + E + 1);
+    for (auto& v : rel) v -= ev_off[e0];
+    ws.pinned = static_cast<char*>(ws.pipe_pinned) + (size_t)c * host_tab;
+    st = prepare_batch(ctx, params, kernel, metric, ndim, E, rel.data(), out, args[c]);
+  }
+  ws.pinned = pinned_main;
+  if (st != CLUE_OK) return st;
+
+  // 2. copy-in stream: each chunk's event table, then its inputs, so a chunk can start as soon
+  //    as its own copies are done
+  CLUE_CUDA_TRY(cudaEventRecord(ev_start, s));
+  CLUE_CUDA_TRY(cudaStreamWaitEvent(h2d, ev_start, 0));
+  CLUE_CUDA_TRY(cudaStreamWaitEvent(d2h, ev_start, 0));
+  for (int c = 0; c < K; ++c) {
+    const int E = cut[c + 1] - cut[c];
+    const size_t a0 = (size_t)ev_off[cut[c]], cnt = (size_t)ev_off[cut[c + 1]] - a0;
+    if (E > 1) {  // a single event's table is written by the pipeline's first kernel
+      EvGrid *heg, *deg;
+      int32_t *hpt, *htile, *dpt, *dtile;
+      event_table_carve(static_cast<char*>(ws.pipe_pinned) + (size_t)c * host_tab, ws.cap_events, &heg, &hpt,
+                        &htile);
+      event_table_carve(dtab + dev_tab[c], (size_t)E, &deg, &dpt, &dtile);
+      CLUE_CUDA_TRY(cudaMemcpyAsync(deg, heg, (size_t)E * sizeof(EvGrid), cudaMemcpyHostToDevice, h2d));
+      CLUE_CUDA_TRY(cudaMemcpyAsync(dpt, hpt, (size_t)(E + 1) * 4, cudaMemcpyHostToDevice, h2d));
+      CLUE_CUDA_TRY(cudaMemcpyAsync(dtile, htile, (size_t)(E + 1) * 4, cudaMemcpyHostToDevice, h2d));
+    }
+    for (int d = 0; d < ndim; ++d)
+      CLUE_CUDA_TRY(cudaMemcpyAsync(dcoords + (size_t)d * nn + a0, coords + (size_t)d * nn + a0, cnt * 4,
+                                    cudaMemcpyHostToDevice, h2d));
+    CLUE_CUDA_TRY(cudaMemcpyAsync(dweight + a0, weight + a0, cnt * 4, cudaMemcpyHostToDevice, h2d));
+    CLUE_CUDA_TRY(cudaEventRecord(ev_in(c), h2d));
+  }
+  auto drain = [&]() {
+    cudaStreamSynchronize(h2d);
+    cudaStreamSynchronize(s);
+    cudaStreamSynchronize(d2h);
+  };
+
+  // 3. chunks on the caller's stream (each with its own device event table), results out on
+  //    the copy-out stream
+  EvGrid* const ev_main = ws.ev;
+  int32_t* const pt_main = ws.ev_pt;
+  int32_t* const tile_main = ws.ev_tile;
+  for (int c = 0; c < K && st == CLUE_OK; ++c) {
+    const int e0 = cut[c], E = cut[c + 1] - e0;
+    const size_t a0 = (size_t)ev_off[e0], cnt = (size_t)ev_off[cut[c + 1]] - a0;
+    RunArgs& a = args[c];
+    for (int d = 0; d < ndim; ++d) a.coords[d] = dcoords + (size_t)d * nn + a0;
+    a.weight = dweight + a0;
+    a.out.cluster_index = dev_out.cluster_index + a0;
+    a.out.is_seed = dev_out.is_seed ? dev_out.is_seed + a0 : nullptr;
+    a.out.rho = dev_out.rho ? dev_out.rho + a0 : nullptr;
+    a.out.nearest_higher = dev_out.nearest_higher ? dev_out.nearest_higher + a0 : nullptr;
+    a.out.delta = dev_out.delta ? dev_out.delta + a0 : nullptr;
+    a.ev_n_clusters = dev_ncl ? dev_ncl + e0 : nullptr;
+    cudaError_t ce = cudaStreamWaitEvent(s, ev_in(c), 0);
+    if (ce == cudaSuccess) {
+      event_table_carve(dtab + dev_tab[c], (size_t)E, &ws.ev, &ws.ev_pt, &ws.ev_tile);
+      st = run_pipeline_dispatch(ws, a, s);
+      ws.ev = ev_main;
+      ws.ev_pt = pt_main;
+      ws.ev_tile = tile_main;
+    }
+    if (ce == cudaSuccess && st == CLUE_OK) {
+      if (a.out.nearest_higher && a0 > 0)
+        k_shift_indices<<<(int)std::min<size_t>((cnt + 255) / 256, 148 * 8), 256, 0, s>>>(a.out.nearest_higher,
+                                                                                         (int)cnt, (int32_t)a0);
+      k_save_status<<<1, 64, 0, s>>>(ws.status, ws.seed_total, dslot + c, dtotal + c);
+      ce = cudaGetLastError();
+    }
+    if (ce == cudaSuccess && st == CLUE_OK) ce = cudaEventRecord(ev_done(c), s);
+    if (ce == cudaSuccess && st == CLUE_OK) ce = cudaStreamWaitEvent(d2h, ev_done(c), 0);
+    auto back = [&](void* dst, const void* src, size_t bytes) {
+      if (ce == cudaSuccess && dst) ce = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, d2h);
+    };
+    if (st == CLUE_OK) {
+      back(out->cluster_index + a0, dev_out.cluster_index + a0, cnt * 4);
+      back(out->is_seed ? out->is_seed + a0 : nullptr, dev_out.is_seed + (out->is_seed ? a0 : 0), cnt * 4);
+      back(out->rho ? out->rho + a0 : nullptr, dev_out.rho + (out->rho ? a0 : 0), cnt * 4);
+      back(out->nearest_higher ? out->nearest_higher + a0 : nullptr,
+           dev_out.nearest_higher + (out->nearest_higher ? a0 : 0), cnt * 4);
+      back(out->delta ? out->delta + a0 : nullptr, dev_out.delta + (out->delta ? a0 : 0), cnt * 4);
+      back(ev_n_clusters ? ev_n_clusters + e0 : nullptr, dev_ncl + (ev_n_clusters ? e0 : 0), (size_t)E * 4);
+    }
+    if (ce != cudaSuccess) {
+      set_error(std::string("overlapped batch: ") + cudaGetErrorString(ce));
+      st = CLUE_ERR_CUDA;
+    }
+  }
+  if (st == CLUE_OK) {
+    cudaError_t ce = cudaMemcpyAsync(ws.pipe_status_host, dslot, KM * (sizeof(DevStatus) + 4),
+                                     cudaMemcpyDeviceToHost, s);
+    drain();
+    if (ce == cudaSuccess) ce = cudaGetLastError();
+    if (ce != cudaSuccess) {
+      set_error(std::string("overlapped batch: ") + cudaGetErrorString(ce));
+      return CLUE_ERR_CUDA;
+    }
+  } else {
+    drain();
+    return st;
+  }
+  const DevStatus* hs = ws.pipe_status_host;
+  const uint32_t* ht = reinterpret_cast<const uint32_t*>(hs + KM);
+  for (int c = 0; c < K; ++c) {
+    if (hs[c].stage_timeout) {
+      set_error("a bulk-copy wait in the density / nearest-higher sweep timed out");
+      return CLUE_ERR_TIMEOUT;
+    }
+    if (hs[c].nonfinite) {
+      set_error("coordinates or weights contain NaN or Inf");
+      return CLUE_ERR_NONFINITE;
+    }
+  }
+  int64_t seeds = 0, clusters = 0, rounds = 0, tiles = 0;
+  for (int c = 0; c < K; ++c) {
+    int64_t cs = ht[c], cc = hs[c].n_clusters, cr = hs[c].label_rounds;
+    if (hs[c].unresolved[3] != 0) {
+      // label chains beyond the fixed rounds: this chunk again, alone, with the plain path
+      const int e0 = cut[c], E = cut[c + 1] - e0;
+      const size_t a0 = (size_t)ev_off[e0], cnt = (size_t)ev_off[cut[c + 1]] - a0;
+      std::vector<float> cc_in((size_t)ndim * cnt), w_in(cnt);
+      for (int d = 0; d < ndim; ++d)
+        std::memcpy(cc_in.data() + (size_t)d * cnt, coords + (size_t)d * nn + a0, cnt * 4);
+      std::memcpy(w_in.data(), weight + a0, cnt * 4);
+      rel.assign(ev_off + e0, ev_off + e0 + E + 1);
+      for (auto& v : rel) v -= (int32_t)a0;
+      clue_outputs oc{};
+      oc.cluster_index = out->cluster_index + a0;
+      oc.is_seed = out->is_seed ? out->is_seed + a0 : nullptr;
+      oc.rho = out->rho ? out->rho + a0 : nullptr;
+      oc.nearest_higher = out->nearest_higher ? out->nearest_higher + a0 : nullptr;
+      oc.delta = out->delta ? out->delta + a0 : nullptr;
+      clue_run_info ic{};
+      st = batch_plain(ctx, params, kernel, metric, ndim, E, rel.data(), cc_in.data(), w_in.data(), &oc,
+                       ev_n_clusters ? ev_n_clusters + e0 : nullptr, CLUE_MEM_HOST, stream, &ic);
+      if (st != CLUE_OK) return st;
+      if (oc.nearest_higher)
+        for (size_t i = 0; i < cnt; ++i)
+          if (oc.nearest_higher[i] >= 0) oc.nearest_higher[i] += (int32_t)a0;
+      cs = ic.n_seeds;
+      cc = ic.n_clusters;
+      cr = ic.label_rounds;
+    }
+    seeds += cs;
+    clusters += cc;
+    rounds = std::max(rounds, cr);
+    tiles += chunk_tiles[c];
+  }
+  if (info) {
+    info->n_seeds = seeds;
+    info->n_clusters = clusters;
+    info->dropped_seeds = seeds - clusters;
+    info->seed_capacity_used = params->seed_capacity < 0 ? -1 : -2;
+    info->n_tiles = tiles;
+    info->n_per_dim = 0;
+    info->label_rounds = rounds;
+  }
+  return CLUE_OK;
+}
+}  // namespace clue_b200
+
+struct clue_graph_s {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int device = 0;
+};
+
+extern "C" {
+
+clue_status clue_batch_make_clusters(clue_context ctx, const clue_params* params, const clue_kernel* kernel,
+                                     const clue_metric* metric, int32_t ndim, int32_t n_events,
+                                     const int32_t* event_offsets, const float* coords, const float* weight,
+                                     const clue_outputs* out, int32_t* ev_n_clusters, int32_t memory,
+                                     void* stream, clue_run_info* info) {
+  if (memory == CLUE_MEM_HOST && batch_overlap_ok(ctx, params, kernel, metric, ndim, n_events, event_offsets,
+                                                  coords, weight, out))
+    return batch_host_overlapped(ctx, params, kernel, metric, ndim, n_events, event_offsets, coords, weight, out,
+                                 ev_n_clusters, stream, info);
+  return batch_plain(ctx, params, kernel, metric, ndim, n_events, event_offsets, coords, weight, out,
+                     ev_n_clusters, memory, stream, info);
 }
 
 clue_status clue_batch_make_clusters_async(clue_context ctx, const clue_params* params,

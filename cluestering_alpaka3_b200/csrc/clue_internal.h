@@ -136,6 +136,15 @@ struct Workspace {
   void* dstage = nullptr;
   size_t dstage_bytes = 0;
 
+  // overlapped host-memory batches (clue_batch_make_clusters): copy streams, per-chunk events
+  // and a pinned copy of every chunk's status and seed total
+  static constexpr int kPipeMaxChunks = 8;
+  cudaStream_t pipe_h2d = nullptr, pipe_d2h = nullptr;
+  cudaEvent_t pipe_ev[1 + 3 * kPipeMaxChunks] = {};
+  DevStatus* pipe_status_host = nullptr;  // kPipeMaxChunks statuses, then as many uint32 totals
+  void* pipe_pinned = nullptr;            // every chunk's pinned event table
+  size_t pipe_pinned_bytes = 0;
+
   int32_t* perm = nullptr;  // alias of the sorted values buffer after the tile sort
   uint32_t* sorted_keys = nullptr;
 

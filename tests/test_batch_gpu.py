@@ -124,3 +124,42 @@ def test_events_loop_matches_batch(gpu_context):
     np.testing.assert_array_equal(outs["cluster_index"].cpu().numpy(), direct.cluster_index)
     np.testing.assert_array_equal(outs["rho"].cpu().numpy().view(np.uint32), direct.rho.view(np.uint32))
     assert ms.shape == (len(off) - 1,) and (ms > 0).all()
+
+
+@pytest.mark.parametrize("kernel,params", [
+    (("exp", (1.0, 1.0)), dict(dc=2.0, rhoc=4.0, dm=3.0)),
+    (("flat", (0.5,)), dict(dc=2.0, rhoc=4.0, dm=3.0, tiebreak="rho_index")),
+])
+def test_host_batch_overlapped_equals_device_batch(gpu_context, kernel, params):
+    # A host-memory batch of 4M points or more is cut into chunks of whole events whose copies
+    # overlap the pipeline; every output (nearest-higher indices shifted to the batch, per-event
+    # cluster counts, run totals) equals one device-memory pass over the whole batch.
+    import torch
+    evs, off, coords, weight = make_events(77, 3300, lo=200, hi=20000)
+    n = coords.shape[1]
+    assert n >= 4_000_000
+    p, k, m = gpu_args(kernel=kernel, **params)
+    res, ncl = gpu_context.batch_host(coords, weight, off, p, k, m)
+    dc = torch.from_numpy(coords).cuda()
+    dw = torch.from_numpy(weight).cuda()
+    outs = {"cluster_index": torch.empty(n, dtype=torch.int32, device="cuda"),
+            "is_seed": torch.empty(n, dtype=torch.int32, device="cuda"),
+            "rho": torch.empty(n, dtype=torch.float32, device="cuda"),
+            "nearest_higher": torch.empty(n, dtype=torch.int32, device="cuda"),
+            "delta": torch.empty(n, dtype=torch.float32, device="cuda")}
+    dncl = torch.empty(len(off) - 1, dtype=torch.int32, device="cuda")
+    info = gpu_context.batch_device(dc.data_ptr(), dw.data_ptr(), 2, off, {k_: v.data_ptr() for k_, v in outs.items()},
+                                    p, k, m, ncl_ptr=dncl.data_ptr())
+    for name, t in outs.items():
+        np.testing.assert_array_equal(getattr(res, name).view(np.uint32), t.cpu().numpy().view(np.uint32),
+                                      err_msg=name)
+    np.testing.assert_array_equal(ncl, dncl.cpu().numpy())
+    assert res.info.n_seeds == info.n_seeds
+    assert res.info.n_clusters == info.n_clusters
+    assert res.info.dropped_seeds == info.dropped_seeds
+    assert res.info.n_tiles == info.n_tiles
+    assert res.info.seed_capacity_used == info.seed_capacity_used
+    # and a second call on the same context gives the same result
+    res2, ncl2 = gpu_context.batch_host(coords, weight, off, p, k, m)
+    np.testing.assert_array_equal(res2.cluster_index, res.cluster_index)
+    np.testing.assert_array_equal(res2.nearest_higher, res.nearest_higher)
