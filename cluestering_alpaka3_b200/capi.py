@@ -41,7 +41,8 @@ EXPORTED = [
     "clue_batch_make_clusters", "clue_batch_make_clusters_async", "clue_graph_capture_batch",
     "clue_graph_launch", "clue_graph_destroy", "clue_events_loop", "clue_context_reserve_batch",
     "clue_server_create", "clue_server_destroy", "clue_server_submit", "clue_server_wait",
-    "clue_server_stats_read", "clue_server_replay",
+    "clue_server_stats_read", "clue_server_replay", "clue_tuning_defaults", "clue_context_set_tuning",
+    "clue_context_get_tuning", "clue_autotune_batch",
 ]
 
 
@@ -104,6 +105,11 @@ class _ServerStats(ctypes.Structure):
                 ("failed", ctypes.c_int64), ("batches", ctypes.c_int64), ("batched_points", ctypes.c_int64),
                 ("slot_points", ctypes.c_int64), ("slot_events", ctypes.c_int64), ("device_bytes", ctypes.c_int64),
                 ("max_batch_seen", ctypes.c_int32), ("max_in_flight", ctypes.c_int32)]
+
+
+class _Tuning(ctypes.Structure):
+    _fields_ = [("symmetric_density", ctypes.c_int32), ("nh_split_lanes", ctypes.c_int32),
+                ("overlap_chunk_points", ctypes.c_int64)]
 
 
 def _load() -> ctypes.CDLL:
@@ -170,6 +176,10 @@ def _load() -> ctypes.CDLL:
     sig["clue_server_stats_read"] = ([vp, ctypes.POINTER(_ServerStats)], ctypes.c_int)
     sig["clue_server_replay"] = ([vp, i32, vp, vp, vp, vp, vp, ctypes.POINTER(_Outputs), vp, ctypes.POINTER(i32)],
                                  ctypes.c_int)
+    sig["clue_tuning_defaults"] = ([ctypes.POINTER(_Tuning)], None)
+    sig["clue_context_set_tuning"] = ([vp, ctypes.POINTER(_Tuning)], ctypes.c_int)
+    sig["clue_context_get_tuning"] = ([vp, ctypes.POINTER(_Tuning)], ctypes.c_int)
+    sig["clue_autotune_batch"] = (batch_args[:-2] + [vp, ctypes.c_char_p, ctypes.POINTER(_Tuning)], ctypes.c_int)
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
         f.argtypes = args
@@ -390,6 +400,40 @@ class Context:
                                            ctypes.c_void_p(weight_ptr), ctypes.byref(out),
                                            ctypes.c_void_p(stream)))
         return None
+
+    def set_tuning(self, symmetric_density: int | None = None, nh_split_lanes: int | None = None,
+                   overlap_chunk_points: int | None = None):
+        """Set the runtime choices (clue_context_set_tuning); None keeps the current value."""
+        t = _Tuning()
+        check(lib.clue_context_get_tuning(self.handle, ctypes.byref(t)))
+        if symmetric_density is not None:
+            t.symmetric_density = symmetric_density
+        if nh_split_lanes is not None:
+            t.nh_split_lanes = nh_split_lanes
+        if overlap_chunk_points is not None:
+            t.overlap_chunk_points = overlap_chunk_points
+        check(lib.clue_context_set_tuning(self.handle, ctypes.byref(t)))
+
+    def reset_tuning(self):
+        check(lib.clue_context_set_tuning(self.handle, None))
+
+    def tuning(self) -> dict:
+        t = _Tuning()
+        check(lib.clue_context_get_tuning(self.handle, ctypes.byref(t)))
+        return {f: getattr(t, f) for f, _ in _Tuning._fields_}
+
+    def autotune_batch(self, coords_ptr: int, weight_ptr: int, ndim: int, event_offsets, params: Params,
+                       kernel: Kernel | None = None, metric: Metric | None = None, stream: int = 0,
+                       cache_path: str | None = None) -> dict:
+        """Time the runtime choices on a device-resident batch and keep the fastest
+        (clue_autotune_batch); with cache_path, reuse or extend an on-disk cache."""
+        p, k, m, off = self._batch_structs(ndim, params, kernel, metric, event_offsets)
+        t = _Tuning()
+        check(lib.clue_autotune_batch(self.handle, ctypes.byref(p), ctypes.byref(k), ctypes.byref(m), ndim,
+                                      len(off) - 1, off.ctypes.data, ctypes.c_void_p(coords_ptr),
+                                      ctypes.c_void_p(weight_ptr), ctypes.c_void_p(stream),
+                                      cache_path.encode() if cache_path else None, ctypes.byref(t)))
+        return {f: getattr(t, f) for f, _ in _Tuning._fields_}
 
     def set_timing(self, enable: bool = True):
         check(lib.clue_context_set_timing(self.handle, 1 if enable else 0))

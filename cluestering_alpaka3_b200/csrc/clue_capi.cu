@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdio>
 #include <cmath>
 #include <cstring>
 #include <new>
@@ -1059,11 +1060,6 @@ __global__ void k_save_status(const DevStatus* __restrict__ st, const uint32_t* 
 
 // Host-memory batches of at least this many points overlap their copies with the pipeline.
 constexpr int64_t kPipeMinPoints = 4000000;
-// Points per chunk the overlapped path aims at (2..kPipeMaxChunks chunks).
-#ifndef CLUE_PIPE_CHUNK_POINTS
-#define CLUE_PIPE_CHUNK_POINTS 4400000
-#endif
-constexpr int64_t kPipeChunkPoints = CLUE_PIPE_CHUNK_POINTS;
 
 // Whether a host-memory batch takes the overlapped path: large, several events, valid (an
 // invalid request goes to the plain path, which reports it).
@@ -1072,6 +1068,7 @@ static bool batch_overlap_ok(clue_context ctx, const clue_params* params, const 
                              const float* coords, const float* weight, const clue_outputs* out) {
   if (!ctx || !params || !kernel || !metric || !ev_off || !coords || !weight || !out || !out->cluster_index)
     return false;
+  if (ctx->ws.tune_overlap_chunk_points <= 0) return false;
   if (n_events < 2 || ev_off[0] != 0 || ev_off[n_events] < kPipeMinPoints) return false;
   if (clue_check_params(params) != CLUE_OK || clue_check_kernel(kernel) != CLUE_OK ||
       clue_check_metric(metric, ndim) != CLUE_OK)
@@ -1103,7 +1100,8 @@ static clue_status batch_host_overlapped(clue_context ctx, const clue_params* pa
   Workspace& ws = ctx->ws;
   const int64_t n = ev_off[n_events];
   const size_t nn = (size_t)n;
-  int K = (int)std::min<int64_t>(KM, std::max<int64_t>(2, n / kPipeChunkPoints));
+  // points per chunk (clue_tuning.overlap_chunk_points): 2..kPipeMaxChunks chunks
+  int K = (int)std::min<int64_t>(KM, std::max<int64_t>(2, n / ws.tune_overlap_chunk_points));
   K = std::min(K, (int)n_events);
   // chunk sizes in the ratio 1 : 2 : ... : 2 : 1 -- only the first chunk's copy-in and the last
   // chunk's copy-out are not hidden behind a pipeline run
@@ -1362,6 +1360,168 @@ clue_status clue_batch_make_clusters(clue_context ctx, const clue_params* params
                                  ev_n_clusters, stream, info);
   return batch_plain(ctx, params, kernel, metric, ndim, n_events, event_offsets, coords, weight, out,
                      ev_n_clusters, memory, stream, info);
+}
+
+void clue_tuning_defaults(clue_tuning* t) {
+  if (!t) return;
+  const Workspace d{};
+  t->symmetric_density = d.tune_symmetric;
+  t->nh_split_lanes = d.tune_nh_split;
+  t->overlap_chunk_points = d.tune_overlap_chunk_points;
+}
+
+clue_status clue_context_set_tuning(clue_context ctx, const clue_tuning* t) {
+  if (!ctx) {
+    set_error("context is null");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  clue_tuning d;
+  clue_tuning_defaults(&d);
+  if (!t) t = &d;
+  if (t->symmetric_density != 0 && t->symmetric_density != 1) {
+    set_error("symmetric_density must be 0 or 1");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  if (t->nh_split_lanes < 0 || t->nh_split_lanes > 16) {
+    set_error("nh_split_lanes must be in [0, 16]");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  if (t->overlap_chunk_points < 0) {
+    set_error("overlap_chunk_points must be >= 0");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  ctx->ws.tune_symmetric = t->symmetric_density;
+  ctx->ws.tune_nh_split = t->nh_split_lanes;
+  ctx->ws.tune_overlap_chunk_points = t->overlap_chunk_points;
+  return CLUE_OK;
+}
+
+clue_status clue_context_get_tuning(clue_context ctx, clue_tuning* t) {
+  if (!ctx || !t) {
+    set_error("context and tuning must be non-null");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  t->symmetric_density = ctx->ws.tune_symmetric;
+  t->nh_split_lanes = ctx->ws.tune_nh_split;
+  t->overlap_chunk_points = ctx->ws.tune_overlap_chunk_points;
+  return CLUE_OK;
+}
+
+clue_status clue_autotune_batch(clue_context ctx, const clue_params* params, const clue_kernel* kernel,
+                                const clue_metric* metric, int32_t ndim, int32_t n_events,
+                                const int32_t* event_offsets, const float* coords, const float* weight,
+                                void* stream, const char* cache_path, clue_tuning* chosen) {
+  if (!ctx || !params || !kernel || !metric || !event_offsets || n_events <= 0 || !coords || !weight) {
+    set_error("autotune: context, parameters, event offsets and inputs must be given");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  Workspace& ws = ctx->ws;
+  const int64_t n = event_offsets[n_events];
+  if (n <= 0) {
+    set_error("autotune: empty batch");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  auto ceil_log2 = [](int64_t v) {
+    int b = 0;
+    while ((int64_t(1) << b) < v) ++b;
+    return b;
+  };
+  char key[160];
+  std::snprintf(key, sizeof(key), "clue-tune-v1 ndim=%d nbucket=%d ebucket=%d kernel=%d metric=%d flags=%d", ndim,
+                ceil_log2(n), ceil_log2(n_events), kernel->type, metric->type, params->flags);
+  auto apply = [&](int sym, int split) {
+    ws.tune_symmetric = sym;
+    ws.tune_nh_split = split;
+  };
+  auto report = [&]() {
+    if (chosen) clue_context_get_tuning(ctx, chosen);
+  };
+  if (cache_path) {
+    if (FILE* f = std::fopen(cache_path, "r")) {
+      char line[256];
+      int sym = -1, split = -1;
+      const size_t kl = std::strlen(key);
+      while (std::fgets(line, sizeof(line), f))
+        if (std::strncmp(line, key, kl) == 0 && line[kl] == ' ')
+          std::sscanf(line + kl, " | symmetric_density=%d nh_split_lanes=%d", &sym, &split);
+      std::fclose(f);
+      if ((sym == 0 || sym == 1) && split >= 0 && split <= 16) {  // the last entry of the key wins
+        apply(sym, split);
+        report();
+        return CLUE_OK;
+      }
+    }
+  }
+  // candidates: the split threshold first (at the symmetric default), then the density form
+  const bool spatial = (params->flags & CLUE_FLAG_REFERENCE_ORDER) == 0 &&
+                       (kernel->type != CLUE_KERNEL_FLAT || (params->flags & CLUE_FLAG_SPATIAL_DENSITY) != 0);
+  bool sym_ok = spatial && (metric->type == CLUE_METRIC_EUCLIDEAN || metric->type == CLUE_METRIC_MANHATTAN ||
+                            metric->type == CLUE_METRIC_CHEBYSHEV);
+  for (int d = 0; d < ndim && d < CLUE_MAX_DIM; ++d) sym_ok = sym_ok && !params->wrapped[d];
+  int prev = 0;
+  CLUE_CUDA_TRY(cudaGetDevice(&prev));
+  CLUE_CUDA_TRY(cudaSetDevice(ws.device));
+  cudaStream_t s = (cudaStream_t)stream;
+  int32_t* labels = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaError_t ce = cudaMalloc(&labels, (size_t)n * sizeof(int32_t));
+  if (ce == cudaSuccess) ce = cudaEventCreate(&e0);
+  if (ce == cudaSuccess) ce = cudaEventCreate(&e1);
+  clue_status st = ce == cudaSuccess ? CLUE_OK : CLUE_ERR_CUDA;
+  if (st != CLUE_OK) set_error(std::string("autotune: ") + cudaGetErrorString(ce));
+  clue_outputs out{};
+  out.cluster_index = labels;
+  auto measure = [&](int sym, int split) -> float {
+    apply(sym, split);
+    float t[3] = {0, 0, 0};
+    for (int r = 0; r < 4 && st == CLUE_OK; ++r) {  // one warm-up, then three timed runs
+      if (cudaEventRecord(e0, s) != cudaSuccess) st = CLUE_ERR_CUDA;
+      if (st == CLUE_OK)
+        st = clue_batch_make_clusters_async(ctx, params, kernel, metric, ndim, n_events, event_offsets, coords,
+                                            weight, &out, nullptr, stream);
+      if (st == CLUE_OK && (cudaEventRecord(e1, s) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess))
+        st = CLUE_ERR_CUDA;
+      if (st == CLUE_OK && r > 0) cudaEventElapsedTime(&t[r - 1], e0, e1);
+    }
+    std::sort(t, t + 3);
+    return t[1];
+  };
+  const int sym0 = sym_ok ? 1 : ws.tune_symmetric;
+  int best_sym = sym0, best_split = 8;
+  float best = 0.0f;
+  const int splits[] = {8, 0, 4, 16};  // the default first: it wins ties
+  for (int split : splits) {
+    const float ms = measure(sym0, split);
+    if (st != CLUE_OK) break;
+    if (split == 8 || ms < best) {
+      best = ms;
+      best_split = split;
+    }
+  }
+  if (st == CLUE_OK && sym_ok) {
+    const float ms = measure(0, best_split);
+    if (st == CLUE_OK && ms < best) {
+      best = ms;
+      best_sym = 0;
+    }
+  }
+  if (labels) cudaFree(labels);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaSetDevice(prev);
+  if (st != CLUE_OK) return st;
+  apply(best_sym, best_split);
+  if (cache_path) {
+    FILE* f = std::fopen(cache_path, "a");
+    if (!f) {
+      set_error(std::string("autotune: cannot write the cache ") + cache_path);
+      return CLUE_ERR_INVALID_ARG;
+    }
+    std::fprintf(f, "%s | symmetric_density=%d nh_split_lanes=%d | %.4f ms\n", key, best_sym, best_split, best);
+    std::fclose(f);
+  }
+  report();
+  return CLUE_OK;
 }
 
 clue_status clue_batch_make_clusters_async(clue_context ctx, const clue_params* params,

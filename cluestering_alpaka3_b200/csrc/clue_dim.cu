@@ -1133,13 +1133,6 @@ __global__ void __launch_bounds__(kTileThreads) k_density(const KParams kp, Even
 // (or than dm) or holds no density reaching the lane's.  TIE == CLUE_TIE_RHO_INDEX resolves equal
 // distances by higher rho, then lower index.
 
-#ifndef CLUE_NH_COMPACT
-#define CLUE_NH_COMPACT 8
-#endif
-// Largest number of lanes that need a candidate block for the block's candidates to be split
-// among all the warp's lanes.
-constexpr int kNhCompact = CLUE_NH_COMPACT;
-
 template <int N, int MT, int TIE>
 __global__ void __launch_bounds__(kTileThreads, N <= 2 ? 8 : (N <= 4 ? 6 : 4)) k_nearest_higher(
     const KParams kp, Events ev, const int32_t* __restrict__ off, const int32_t* __restrict__ ord,
@@ -1147,7 +1140,7 @@ __global__ void __launch_bounds__(kTileThreads, N <= 2 ? 8 : (N <= 4 ? 6 : 4)) k
     const uint32_t* __restrict__ chunk_total, const float4* __restrict__ rec_r, const float4* __restrict__ rec_m,
     const int32_t* __restrict__ mq, const float4* __restrict__ blk, const float4* __restrict__ sblk,
     const int32_t* __restrict__ minv, const int32_t* __restrict__ perm, int32_t* __restrict__ nh_s,
-    float* __restrict__ delta_s, DevStatus* st) {
+    float* __restrict__ delta_s, DevStatus* st, int split_lanes) {
   using M = Metric<N, MT>;
   ChunkHome h;
   if (!chunk_home(kp, ev, off, ord, chunk_tile, chunk_off, chunk_total, h)) return;
@@ -1245,7 +1238,7 @@ __global__ void __launch_bounds__(kTileThreads, N <= 2 ? 8 : (N <= 4 ? 6 : 4)) k
     // total order that the group reduces exactly.
     const unsigned nm = __ballot_sync(0xffffffffu, need);
     const int k = __popc(nm);
-    if (k <= kNhCompact) {
+    if (k <= split_lanes) {
       const int lg = k <= 1 ? 5 : (k <= 2 ? 4 : (k <= 4 ? 3 : (k <= 8 ? 2 : 1)));  // log2 G
       const int lane = threadIdx.x & 31;
       const int hs = lane >> lg;  // home slot of this lane's group
@@ -1755,14 +1748,19 @@ void launch_density(const KParams& kp, Workspace& ws, cudaStream_t s) {
 }
 template <int N, int MT>
 void launch_nh(const KParams& kp, Workspace& ws, cudaStream_t s) {
+  // a block needed by at most this many lanes is split among all lanes (at most 16: the split
+  // gives every needing lane a group of 2 lanes or more)
+  const int split_lanes = std::max(0, std::min(16, (int)ws.tune_nh_split));
   if (kp.tiebreak == CLUE_TIE_RHO_INDEX)
     k_nearest_higher<N, MT, CLUE_TIE_RHO_INDEX><<<chunk_grid(kp), kTileThreads, 0, s>>>(
         kp, events_of(ws), ws.offsets, ws.mq, ws.chunk_tile, ws.chunk_count, ws.chunk_total, ws.rec_r,
-        ws.rec_m_cur, ws.mq, ws.blk, ws.sblk, ws.minv, ws.perm, ws.nh_s, ws.delta_s, ws.status);
+        ws.rec_m_cur, ws.mq, ws.blk, ws.sblk, ws.minv, ws.perm, ws.nh_s, ws.delta_s, ws.status,
+        split_lanes);
   else
     k_nearest_higher<N, MT, CLUE_TIE_REFERENCE><<<chunk_grid(kp), kTileThreads, 0, s>>>(
         kp, events_of(ws), ws.offsets, ws.mq, ws.chunk_tile, ws.chunk_count, ws.chunk_total, ws.rec_r,
-        ws.rec_m_cur, ws.mq, ws.blk, ws.sblk, ws.minv, ws.perm, ws.nh_s, ws.delta_s, ws.status);
+        ws.rec_m_cur, ws.mq, ws.blk, ws.sblk, ws.minv, ws.perm, ws.nh_s, ws.delta_s, ws.status,
+        split_lanes);
 }
 template <int N, int MT, int FORM>
 void launch_density_spatial_form(const KParams& kp, Workspace& ws, cudaStream_t s, float kexp) {
@@ -1878,7 +1876,8 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
   // (a workspace without the symmetric sweep's buffers, such as the fixed scratch of the
   // no-allocation entry point, keeps the one-sided sweep)
   const bool symmetric =
-      spatial_density && symmetric_density_ok(kp, a.metric, N) && ws.tblk && ws.tblk_off && ws.rho_fix;
+      spatial_density && symmetric_density_ok(kp, a.metric, N) && ws.tblk && ws.tblk_off && ws.rho_fix &&
+      ws.tune_symmetric != 0;
   const int bits = bits_for((uint32_t)(kp.ntiles - 1));
   const int mbits = std::min(MortonBits<N>::kBits, 32 - bits);
   // The symmetric sweep needs no tile order by point index: one sort by (tile, Morton) composite

@@ -136,6 +136,11 @@ struct Workspace {
   void* dstage = nullptr;
   size_t dstage_bytes = 0;
 
+  // runtime choices (clue_context_set_tuning; clue_autotune_batch measures and picks them)
+  int32_t tune_symmetric = 1;                  // symmetric density sweep where it applies
+  int32_t tune_nh_split = 8;                   // nearest higher: split a block needed by <= this many lanes
+  int64_t tune_overlap_chunk_points = 4400000;  // host-memory batches; 0: no overlap
+
   // overlapped host-memory batches (clue_batch_make_clusters): copy streams, per-chunk events
   // and a pinned copy of every chunk's status and seed total
   static constexpr int kPipeMaxChunks = 8;

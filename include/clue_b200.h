@@ -260,6 +260,38 @@ clue_status clue_graph_capture_batch(clue_context ctx, const clue_params* params
 clue_status clue_graph_launch(clue_graph graph, void* stream);
 clue_status clue_graph_destroy(clue_graph graph);
 
+/* ---- runtime choices and their autotuner (no reference counterpart) -----------------------
+ * The reference fixes its launch shape per backend.  Here a few choices that never change the
+ * results beyond the stated tolerance are made at run time per context:
+ *   symmetric_density   1 (default): where the kernel is exponential or Gaussian, the order is
+ *                       spatial and the metric bounds every coordinate difference (Euclidean,
+ *                       Manhattan, Chebyshev, no wrapped coordinate), every pair within dc is
+ *                       evaluated once for both points; 0: one-sided sweep.  Both are within
+ *                       1e-5 of FP64.
+ *   nh_split_lanes      0..16 (default 8): a nearest-higher candidate block that at most this
+ *                       many lanes of a warp still need is split among all 32 lanes; 0 never
+ *                       splits.  Results are identical for every value.
+ *   overlap_chunk_points  host-memory batches of 4M points or more overlap their copies with
+ *                       the pipeline in chunks of about this many points (default 4400000);
+ *                       0 turns the overlap off.  Results are identical.
+ * clue_autotune_batch times the candidate values on a device-resident sample batch (CUDA
+ * events on `stream`), keeps the fastest in the context and, with cache_path non-NULL, appends
+ * it to a text cache keyed by (ndim, size bucket = ceil(log2 n), event-count bucket, kernel,
+ * metric, flags); a later call with the same key reads the cache and times nothing.
+ */
+typedef struct clue_tuning {
+  int32_t symmetric_density;
+  int32_t nh_split_lanes;
+  int64_t overlap_chunk_points;
+} clue_tuning;
+void clue_tuning_defaults(clue_tuning* t);
+clue_status clue_context_set_tuning(clue_context ctx, const clue_tuning* t);
+clue_status clue_context_get_tuning(clue_context ctx, clue_tuning* t);
+clue_status clue_autotune_batch(clue_context ctx, const clue_params* params, const clue_kernel* kernel,
+                                const clue_metric* metric, int32_t ndim, int32_t n_events,
+                                const int32_t* event_offsets, const float* coords, const float* weight,
+                                void* stream, const char* cache_path, clue_tuning* chosen);
+
 /*
  * clue_make_clusters_noalloc -- no counterpart in the reference.
  * The same pipeline for callers that cannot allocate device memory (a runtime that owns all

@@ -121,3 +121,11 @@ def test_no_gpu_calls_fail_cleanly():
         pytest.skip("GPU present")
     with pytest.raises(capi.ClueError):
         capi.Context(0)
+
+
+def test_tuning_defaults():
+    import ctypes
+    from cluestering_alpaka3_b200 import capi
+    t = capi._Tuning()
+    capi.lib.clue_tuning_defaults(ctypes.byref(t))
+    assert (t.symmetric_density, t.nh_split_lanes, t.overlap_chunk_points) == (1, 8, 4400000)

@@ -163,3 +163,46 @@ def test_host_batch_overlapped_equals_device_batch(gpu_context, kernel, params):
     res2, ncl2 = gpu_context.batch_host(coords, weight, off, p, k, m)
     np.testing.assert_array_equal(res2.cluster_index, res.cluster_index)
     np.testing.assert_array_equal(res2.nearest_higher, res.nearest_higher)
+
+
+def test_autotune_batch_cache_and_equivalence(tmp_path):
+    # The autotuner times the runtime choices on a device batch, keeps the fastest and caches it
+    # per (ndim, size bucket, event-count bucket, kernel, metric, flags); every choice gives the
+    # same outputs (the nearest-higher split and the copy overlap exactly, the density form
+    # within the 1e-5 tolerance).
+    import torch
+    from cluestering_alpaka3_b200 import capi
+    evs, off, coords, weight = make_events(55, 300)
+    p, k, m = gpu_args(kernel=("exp", (1.0, 1.0)), dc=2.0, rhoc=4.0, dm=3.0)
+    dc, dw = torch.from_numpy(coords).cuda(), torch.from_numpy(weight).cuda()
+    cache = tmp_path / "clue_tune.txt"
+    tuned = capi.Context(0)
+    chosen = tuned.autotune_batch(dc.data_ptr(), dw.data_ptr(), 2, off, p, k, m, cache_path=str(cache))
+    assert chosen["symmetric_density"] in (0, 1) and chosen["nh_split_lanes"] in (0, 4, 8, 16)
+    assert tuned.tuning() == chosen
+    lines = cache.read_text().splitlines()
+    assert len(lines) == 1 and "ndim=2" in lines[0] and "nh_split_lanes=" in lines[0]
+    other = capi.Context(0)
+    assert other.autotune_batch(dc.data_ptr(), dw.data_ptr(), 2, off, p, k, m, cache_path=str(cache)) == chosen
+    assert cache.read_text().splitlines() == lines  # read from the cache, nothing timed or added
+
+    base = capi.Context(0)
+    ref, ref_ncl = base.batch_host(coords, weight, off, p, k, m)
+    for split in (0, 4, 16):
+        base.set_tuning(nh_split_lanes=split)
+        got, ncl = base.batch_host(coords, weight, off, p, k, m)
+        for name in ("cluster_index", "is_seed", "rho", "nearest_higher", "delta"):
+            np.testing.assert_array_equal(getattr(got, name).view(np.uint32), getattr(ref, name).view(np.uint32),
+                                          err_msg=f"split {split}: {name}")
+        np.testing.assert_array_equal(ncl, ref_ncl)
+    base.set_tuning(nh_split_lanes=8, symmetric_density=0)
+    one_sided, _ = base.batch_host(coords, weight, off, p, k, m)
+    np.testing.assert_allclose(one_sided.rho, ref.rho, rtol=2e-5)
+    with pytest.raises(capi.ClueError):
+        base.set_tuning(nh_split_lanes=17)
+    with pytest.raises(capi.ClueError):
+        base.set_tuning(symmetric_density=2)
+    base.reset_tuning()
+    assert base.tuning() == {"symmetric_density": 1, "nh_split_lanes": 8, "overlap_chunk_points": 4400000}
+    for c in (tuned, other, base):
+        c.close()
