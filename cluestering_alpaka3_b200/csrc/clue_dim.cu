@@ -1134,7 +1134,7 @@ __global__ void __launch_bounds__(kTileThreads) k_density(const KParams kp, Even
 // distances by higher rho, then lower index.
 
 template <int N, int MT, int TIE>
-__global__ void __launch_bounds__(kTileThreads, N <= 2 ? 8 : (N <= 4 ? 6 : 4)) k_nearest_higher(
+__global__ void __launch_bounds__(kTileThreads, (N <= 2 ? 8 : (N <= 4 ? 6 : 4)) * 128 / kTileThreads) k_nearest_higher(
     const KParams kp, Events ev, const int32_t* __restrict__ off, const int32_t* __restrict__ ord,
     const int32_t* __restrict__ chunk_tile, const uint32_t* __restrict__ chunk_off,
     const uint32_t* __restrict__ chunk_total, const float4* __restrict__ rec_r, const float4* __restrict__ rec_m,
@@ -1334,7 +1334,7 @@ enum { kDensGeneric = 0, kDensExpUnit = 1, kDensGauss0Unit = 2 };
 // spatial order.  Blocks farther than dc from every lane are skipped; inside a block, candidates
 // that no lane of the warp holds within dc skip the kernel evaluation.
 template <int N, int MT, int FORM>
-__global__ void __launch_bounds__(kTileThreads, N <= 4 ? 8 : 4) k_density_spatial(
+__global__ void __launch_bounds__(kTileThreads, (N <= 4 ? 8 : 4) * 128 / kTileThreads) k_density_spatial(
     const KParams kp, Events ev, const int32_t* __restrict__ off, const int32_t* __restrict__ ord,
     const int32_t* __restrict__ chunk_tile, const uint32_t* __restrict__ chunk_off,
     const uint32_t* __restrict__ chunk_total, const float4* __restrict__ rec_w, const float4* __restrict__ rec_m,
@@ -1416,12 +1416,12 @@ __global__ void __launch_bounds__(256) k_tblock_bbox(int max_slots, const uint32
                                                     const uint32_t* __restrict__ bo,
                                                     const float4* __restrict__ rec_m, float4* __restrict__ tblk) {
   constexpr int BW = Blk<N>::kWords;
-  const int nslots = min(max_slots, 4 * (int)*chunk_total);
+  const int nslots = min(max_slots, kChunkWarps * (int)*chunk_total);
   const int stride = gridDim.x * blockDim.x;
   for (int sl = blockIdx.x * blockDim.x + threadIdx.x; sl < nslots; sl += stride) {
-    const int c = sl >> 2;
+    const int c = sl / kChunkWarps;
     const int t = chunk_tile[c];
-    const int b = ((c - (int)chunk_off[t]) << 2) + (sl & 3);
+    const int b = (c - (int)chunk_off[t]) * kChunkWarps + sl % kChunkWarps;
     const int first = off[t] + (b << 5);
     const int cnt = min(32, off[t + 1] - first);
     if (cnt <= 0) continue;
@@ -1459,7 +1459,7 @@ __device__ __forceinline__ int fix_exponent(const EvGrid* g, float kmax) {
 }
 
 template <int N, int MT, int FORM>
-__global__ void __launch_bounds__(kTileThreads, N <= 4 ? 8 : 4) k_density_sym(
+__global__ void __launch_bounds__(kTileThreads, (N <= 4 ? 8 : 4) * 128 / kTileThreads) k_density_sym(
     const KParams kp, Events ev, const int32_t* __restrict__ off, const int32_t* __restrict__ chunk_tile,
     const uint32_t* __restrict__ chunk_off, const uint32_t* __restrict__ chunk_total,
     const float4* __restrict__ rec_m, const int32_t* __restrict__ mq, const uint32_t* __restrict__ bo,
@@ -1472,7 +1472,7 @@ __global__ void __launch_bounds__(kTileThreads, N <= 4 ? 8 : 4) k_density_sym(
   if (c >= (int)*chunk_total) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int t = chunk_tile[c];
-  const int a_loc = ((c - (int)chunk_off[t]) << 2) + warp;  // block of the tile
+  const int a_loc = (c - (int)chunk_off[t]) * kChunkWarps + warp;  // block of the tile
   const int startA = off[t] + (a_loc << 5);
   const int cntA = min(32, off[t + 1] - startA);
   if (cntA <= 0) return;  // whole warp: this block of the chunk is past the tile's end
@@ -1933,7 +1933,7 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
 
   const int nblk_threads = ((n + 31) >> 5) * 32;
   const int nsb_threads = ((((n + 31) >> 5) + 31) >> 5) * 32;
-  const int max_slots = 4 * (n / kChunk + kp.ntiles + 1);
+  const int max_slots = kChunkWarps * (n / kChunk + kp.ntiles + 1);
   if (symmetric) {
     if (!composite) {
       k_gather_morton<N><<<grid_for(n, 256), 256, 0, s>>>(ws.rec_w, n, ws.mq, ws.rec_m);
