@@ -332,34 +332,8 @@ __device__ __forceinline__ void spatial_sweep(const KParams& kp, const EvGrid* _
       m *= (int64_t)(hi[d] - lo[d] + 1);
     }
   }
-  int v[N];
-  int phase = 0;  // 0: own tile, 1: first union tile pending, 2: iterating the union
-  while (true) {
-    if (phase == 0) {
-#pragma unroll
-      for (int d = 0; d < N; ++d) v[d] = hb[d];
-      phase = 1;
-    } else {
-      if (phase == 1) {
-#pragma unroll
-        for (int d = 0; d < N; ++d) v[d] = wl[d];
-        phase = 2;
-      } else {
-        int d = N - 1;
-        for (; d >= 0; --d) {
-          if (v[d] < wh[d]) {
-            ++v[d];
-            break;
-          }
-          v[d] = wl[d];
-        }
-        if (d < 0) break;
-      }
-      bool is_home = true;
-#pragma unroll
-      for (int d = 0; d < N; ++d) is_home = is_home && v[d] == hb[d];
-      if (is_home) continue;
-    }
+  // one tile of the search boxes: its super-blocks and blocks that some lane may need
+  auto visit_tile = [&](const int* v, bool is_home_tile) {
     bool inbox = valid;
     int u = g->tile_base;
     int64_t lexpos = 0;
@@ -369,10 +343,10 @@ __device__ __forceinline__ void spatial_sweep(const KParams& kp, const EvGrid* _
       u += g->stride[d] * wrap_bin(v[d], g->nperdim);
       lexpos += (int64_t)(v[d] - lo[d]) * ext[d];
     }
-    if (!__any_sync(0xffffffffu, inbox)) continue;
+    if (!__any_sync(0xffffffffu, inbox)) return;
     const int pb = off[u], pe = off[u + 1];
-    if (pb >= pe) continue;
-    const bool home_tile = PREVISIT && phase == 1;
+    if (pb >= pe) return;
+    const bool home_tile = PREVISIT && is_home_tile;
     if (home_tile && ph_lo <= ph_hi) {
       skip_lo = max(pb >> 5, (ph_lo >> 5) - 1);
       skip_hi = min((pe - 1) >> 5, (ph_hi >> 5) + 1);
@@ -406,6 +380,53 @@ __device__ __forceinline__ void spatial_sweep(const KParams& kp, const EvGrid* _
         if (!__any_sync(0xffffffffu, need)) continue;
         vis(max(sp0, b << 5), min(sp1, (b + 1) << 5), need, lexpos);
       }
+    }
+  };
+  visit_tile(hb, true);
+  int v[N];
+  if (PREVISIT && N <= 3) {
+    // the other tiles ring by ring around the home tile (nearest first, so the bound shrinks
+    // early and far blocks are skipped), lexicographic inside a ring
+    int R = 0;
+#pragma unroll
+    for (int d = 0; d < N; ++d) R = max(R, max(hb[d] - wl[d], wh[d] - hb[d]));
+    for (int r = 1; r <= R; ++r) {
+#pragma unroll
+      for (int d = 0; d < N; ++d) v[d] = wl[d];
+      while (true) {
+        int ring = 0;
+#pragma unroll
+        for (int d = 0; d < N; ++d) ring = max(ring, abs(v[d] - hb[d]));
+        if (ring == r) visit_tile(v, false);
+        int d = N - 1;
+        for (; d >= 0; --d) {
+          if (v[d] < wh[d]) {
+            ++v[d];
+            break;
+          }
+          v[d] = wl[d];
+        }
+        if (d < 0) break;
+      }
+    }
+  } else {
+    // the other tiles of the union box lexicographically
+#pragma unroll
+    for (int d = 0; d < N; ++d) v[d] = wl[d];
+    while (true) {
+      bool is_home = true;
+#pragma unroll
+      for (int d = 0; d < N; ++d) is_home = is_home && v[d] == hb[d];
+      if (!is_home) visit_tile(v, false);
+      int d = N - 1;
+      for (; d >= 0; --d) {
+        if (v[d] < wh[d]) {
+          ++v[d];
+          break;
+        }
+        v[d] = wl[d];
+      }
+      if (d < 0) break;
     }
   }
 }
