@@ -680,6 +680,15 @@ struct MortonBits {
   static constexpr int kBits = kPerDim * N;
 };
 
+// Morton bits the tile-internal order sorts on: the top bits of the interleaved code, a fixed
+// count per dimension, so an event's record order (and with it the bits of its densities) never
+// depends on the batch around it or on which of the two sort paths built it.  Two dimensions keep
+// 15 of 16 bits, so a (tile, Morton) composite key fits 32 bits up to 2^17 tiles.
+template <int N>
+struct MortonSortBits {
+  static constexpr int kBits = N == 2 ? 15 : MortonBits<N>::kBits;
+};
+
 // The bits of c (below 2^kPerDim) moved to positions 0, N, 2N, ... of a Morton code.
 template <int N>
 __device__ __forceinline__ uint32_t spread_bits(uint32_t c) {
@@ -716,12 +725,14 @@ __global__ void __launch_bounds__(256) k_morton_keys(const KParams kp, Events ev
     uint32_t m = 0;
 #pragma unroll
     for (int d = 0; d < N; ++d) {
-      const float t0 = g->mn[d] + (float)hb[d] * g->size[d];
-      int c = g->size[d] > 0.0f ? (int)((x[d] - t0) / g->size[d] * scale) : 0;
+      // position inside the tile from getBin's quotient, as in k_bin_composite
+      const float xd = kp.wrapped[d] ? normalize_coord(x[d], g->mn[d], g->mx[d]) : x[d];
+      const float qd = fdiv(fsub(xd, g->mn[d]), g->size[d]);
+      int c = g->size[d] > 0.0f ? (int)((qd - (float)hb[d]) * scale) : 0;
       c = c < 0 ? 0 : (c > (1 << bpd) - 1 ? (1 << bpd) - 1 : c);
-      for (int bit = 0; bit < bpd; ++bit) m |= (uint32_t)((c >> bit) & 1) << (bit * N + d);
+      m |= spread_bits<N>((uint32_t)c) << d;
     }
-    keys[q] = m;
+    keys[q] = m >> (MortonBits<N>::kBits - MortonSortBits<N>::kBits);
   }
 }
 
@@ -1900,11 +1911,11 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
       spatial_density && symmetric_density_ok(kp, a.metric, N) && ws.tblk && ws.tblk_off && ws.rho_fix &&
       ws.tune_symmetric != 0;
   const int bits = bits_for((uint32_t)(kp.ntiles - 1));
-  const int mbits = std::min(MortonBits<N>::kBits, 32 - bits);
+  const int mbits = MortonSortBits<N>::kBits;
   // The symmetric sweep needs no tile order by point index: one sort by (tile, Morton) composite
   // keys gives its record order, and positions inside a tile are only compared through the
   // points' indices.  The other sweeps take the tile order by index and a Morton order beside it.
-  const bool composite = symmetric && mbits >= 8;
+  const bool composite = symmetric && bits + mbits <= 32;
   if (composite) {
     k_bin_composite<N><<<grid_for(n, 256), 256, 0, s>>>(kp, in, ev, mbits, ws.keys[0]);
     const int cur = radix_sort_pairs(ws.keys, ws.vals, true, n, bits + mbits, ws.hist, ws.scan_scratch, s);
@@ -1929,7 +1940,7 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
     uint32_t* mkeys[2] = {ws.keys[cur ^ 1], ws.mkeys_alt};
     int32_t* mvals[2] = {ws.vals[cur ^ 1], ws.mq_alt};
     k_morton_keys<N><<<grid_for(n, 256), 256, 0, s>>>(kp, ev, ws.rec_w, ws.sorted_keys, mkeys[0]);
-    int mc = radix_sort_pairs(mkeys, mvals, true, n, MortonBits<N>::kBits, ws.hist, ws.scan_scratch, s);
+    int mc = radix_sort_pairs(mkeys, mvals, true, n, MortonSortBits<N>::kBits, ws.hist, ws.scan_scratch, s);
     if (mc != 0) {
       std::swap(mkeys[0], mkeys[1]);
       std::swap(mvals[0], mvals[1]);
@@ -1940,7 +1951,7 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
     ws.minv = mvals[mc ^ 1];
     k_invert<<<grid_for(n, 256), 256, 0, s>>>(ws.mq, n, ws.minv);
     ws.rec_m_cur = ws.rec_m;
-    launches += radix_sort_launches(bits) + 2 + 1 + radix_sort_launches(MortonBits<N>::kBits) + 1 +
+    launches += radix_sort_launches(bits) + 2 + 1 + radix_sort_launches(MortonSortBits<N>::kBits) + 1 +
                 radix_sort_launches(bits) + 1;
   }
   if (symmetric)

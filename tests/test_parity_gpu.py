@@ -344,3 +344,26 @@ def test_symmetric_path_nearest_higher_batched_exact(gpu_context):
         got_nh = res.nearest_higher[a:b]  # batch-wide indices
         np.testing.assert_array_equal(np.where(got_nh >= 0, got_nh - a, -1)[keep], nh[keep], err_msg=f"event {e}")
         np.testing.assert_array_equal(res.delta[a:b].view(np.uint32), delta.view(np.uint32), err_msg=f"event {e}")
+
+
+@pytest.mark.parametrize("n_pad", [100_000, 200_000])
+def test_symmetric_event_bits_independent_of_batch_size(gpu_context, n_pad):
+    # An event gives the same bits alone and inside batches with ~100k tiles (one composite
+    # (tile, Morton) sort) and ~200k tiles (tile sort plus Morton sort): both sort paths order the
+    # records by (tile, the same Morton bits, index).  Single-point events pad the tile count.
+    from parity_util import gpu_args
+    rng = np.random.default_rng(140)
+    c, w = random_blobs(rng, 3000, 2, nblobs=5, extent=25.0)
+    p, k, m = gpu_args(dc=1.5, rhoc=3.0, dm=2.0, kernel=("exp", (1.0, 1.0)))
+    alone = gpu_context.make_clusters_host(c, w, p, k, m)
+    pad = rng.uniform(0, 25, size=(2, n_pad)).astype(np.float32)
+    coords = np.ascontiguousarray(np.concatenate([pad, c], axis=1))
+    weight = np.concatenate([np.ones(n_pad, np.float32), w])
+    off = np.concatenate([np.arange(n_pad + 1), [n_pad + c.shape[1]]]).astype(np.int32)
+    res, _ = gpu_context.batch_host(coords, weight, off, p, k, m)
+    assert res.info.n_tiles > (1 << 16)
+    for name in ("rho", "delta", "cluster_index", "is_seed"):
+        np.testing.assert_array_equal(getattr(res, name)[n_pad:].view(np.uint32), getattr(alone, name).view(np.uint32),
+                                      err_msg=name)
+    nh = res.nearest_higher[n_pad:]
+    np.testing.assert_array_equal(np.where(nh >= 0, nh - n_pad, -1), alone.nearest_higher)
