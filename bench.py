@@ -315,10 +315,17 @@ def main():
     dens_ms = float(stage_avg[1])
     achieved = B["density_kernel"] / (dens_ms / 1e3) / 1e9
     traffic = None
+    issue = None  # the sweeps' real bound: instruction issue and the MUFU (XU) pipe, from ncu
     tfile = os.path.join(ROOT, "profiles", f"traffic_{wl.name}.json")
     if os.path.exists(tfile):
         with open(tfile) as f:
-            traffic = json.load(f).get("density_bytes_per_launch")
+            tj = json.load(f)
+        traffic = tj.get("density_bytes_per_launch")
+        if "density_issue_active" in tj:
+            issue = {"bound": "issue", "kernel": tj.get("density_kernel"),
+                     "issue_active_frac": tj["density_issue_active"], "xu_pipe_frac": tj.get("density_xu_pipe"),
+                     "nearest_higher_issue_active_frac": tj.get("nearest_higher_issue_active"),
+                     "source": tj.get("source")}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -364,6 +371,7 @@ def main():
                          "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": traffic, "algorithmic_bytes": B["density_kernel"], "launch_ms": dens_ms},
+            "secondary_bound": issue,
             "stage_ms": {"tiles": stage_avg[0], "density": stage_avg[1], "nearest_higher": stage_avg[2],
                          "seeds_labels": stage_avg[3]},
             "b_alg_total": B["total"],
