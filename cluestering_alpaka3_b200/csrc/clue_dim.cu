@@ -167,46 +167,50 @@ __device__ __forceinline__ int wrap_bin(int v, int npd) {
   return b < 0 ? b + npd : b;
 }
 
+// Box of one warp's 32 records (lanes past the end repeat a record of the block): lo[N],
+// hi[N] and the largest payload, written as block b.
+template <int N>
+__device__ __forceinline__ void write_block_box(float4* __restrict__ blk, int b, const float* x, float pl) {
+  constexpr int BW = Blk<N>::kWords;
+  const int lane = threadIdx.x & 31;
+  float out[4 * BW];
+#pragma unroll
+  for (int k = 0; k < 4 * BW; ++k) out[k] = 0.0f;
+#pragma unroll
+  for (int d = 0; d < N; ++d) {
+    float a = x[d], z = x[d];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      a = fminf(a, __shfl_xor_sync(0xffffffffu, a, o));
+      z = fmaxf(z, __shfl_xor_sync(0xffffffffu, z, o));
+    }
+    out[d] = a;
+    out[N + d] = z;
+  }
+  float pm = pl;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) pm = fmaxf(pm, __shfl_xor_sync(0xffffffffu, pm, o));
+  out[2 * N] = pm;
+  if (lane < BW) {
+    float4 v;
+#pragma unroll
+    for (int k = 0; k < BW; ++k)
+      if (k == lane) v = make_float4(out[4 * k], out[4 * k + 1], out[4 * k + 2], out[4 * k + 3]);
+    blk[(size_t)b * BW + lane] = v;
+  }
+}
+
 // Bounding box (and largest payload) of every 32 consecutive tile-sorted records.
 template <int N>
 __global__ void __launch_bounds__(256) k_block_bbox(const float4* __restrict__ rec, int n, float4* __restrict__ blk) {
-  constexpr int BW = Blk<N>::kWords;
   const int lane = threadIdx.x & 31;
   const int nblk = (n + 31) >> 5;
   const int wstride = (gridDim.x * blockDim.x) >> 5;
   for (int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nblk; b += wstride) {
     const int q = (b << 5) + lane;
     float x[N], pl;
-    if (q < n) {
-      load_rec<N>(rec, q, x, pl);
-    } else {
-      load_rec<N>(rec, b << 5, x, pl);  // duplicates the block's first record
-    }
-    float out[4 * BW];
-#pragma unroll
-    for (int k = 0; k < 4 * BW; ++k) out[k] = 0.0f;
-#pragma unroll
-    for (int d = 0; d < N; ++d) {
-      float a = x[d], z = x[d];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        a = fminf(a, __shfl_xor_sync(0xffffffffu, a, o));
-        z = fmaxf(z, __shfl_xor_sync(0xffffffffu, z, o));
-      }
-      out[d] = a;
-      out[N + d] = z;
-    }
-    float pm = pl;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) pm = fmaxf(pm, __shfl_xor_sync(0xffffffffu, pm, o));
-    out[2 * N] = pm;
-    if (lane < BW) {
-      float4 v;
-#pragma unroll
-      for (int k = 0; k < BW; ++k)
-        if (k == lane) v = make_float4(out[4 * k], out[4 * k + 1], out[4 * k + 2], out[4 * k + 3]);
-      blk[(size_t)b * BW + lane] = v;
-    }
+    load_rec<N>(rec, q < n ? q : b << 5, x, pl);  // lanes past the end duplicate the first record
+    write_block_box<N>(blk, b, x, pl);
   }
 }
 
@@ -1646,6 +1650,31 @@ __global__ void __launch_bounds__(256) k_density_combine(const KParams kp, Event
   }
 }
 
+// The symmetric density's fixed-point sums added in (as k_density_combine) and the block
+// boxes with the final densities (as k_block_bbox) in one pass over the records, for the
+// composite sort whose tile-ordered records are also the Morton-ordered ones.
+template <int N>
+__global__ void __launch_bounds__(256) k_combine_block_bbox(const KParams kp, Events ev, int n,
+                                                            const int64_t* __restrict__ rho_fix,
+                                                            float4* __restrict__ rec_r, float kmax,
+                                                            float4* __restrict__ blk) {
+  const int lane = threadIdx.x & 31;
+  const int nblk = (n + 31) >> 5;
+  const int wstride = (gridDim.x * blockDim.x) >> 5;
+  for (int b = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nblk; b += wstride) {
+    const int q = (b << 5) + lane;
+    const bool valid = q < n;
+    const int qq = valid ? q : b << 5;
+    bool uniform;
+    const EvGrid* g = ev.eg + warp_event(ev.pt, kp.n_events, qq, true, uniform);
+    float x[N], acc;
+    load_rec<N>(rec_r, qq, x, acc);
+    const float rho = fadd(acc, (float)((double)rho_fix[qq] * ldexp(1.0, -fix_exponent(g, kmax))));
+    if (valid) store_rec<N>(rec_r, q, x, rho);
+    write_block_box<N>(blk, b, x, rho);
+  }
+}
+
 // ---- stage 4: seeds (KernelFindClusters) ---------------------------------------
 template <int N, int MT>
 __global__ void __launch_bounds__(256) k_seeds(const KParams kp, int n, const float4* __restrict__ rec_r,
@@ -1818,7 +1847,7 @@ void launch_density_sym_form(const KParams& kp, Workspace& ws, cudaStream_t s, f
       ws.tblk, ws.rec_r, ws.rho_fix, kexp, kmax);
 }
 template <int N, int MT>
-void launch_density_sym(const KParams& kp, Workspace& ws, cudaStream_t s) {
+void launch_density_sym(const KParams& kp, Workspace& ws, cudaStream_t s, bool fuse_combine) {
   const float log2e = 1.4426950408889634f;
   float kmax = 1.0f;
   if (kp.kernel_type == CLUE_KERNEL_FLAT) kmax = fmaxf(1.0f, fabsf(kp.kpar[0]));
@@ -1831,7 +1860,11 @@ void launch_density_sym(const KParams& kp, Workspace& ws, cudaStream_t s) {
     launch_density_sym_form<N, MT, kDensGauss0Unit>(kp, ws, s, -kp.ginv * log2e, kmax);
   else
     launch_density_sym_form<N, MT, kDensGeneric>(kp, ws, s, 0.0f, kmax);
-  k_density_combine<N><<<grid_for(kp.n, 256), 256, 0, s>>>(kp, events_of(ws), kp.n, ws.rho_fix, ws.rec_r, kmax);
+  if (fuse_combine) {
+    ws.sym_kmax = kmax;  // the combine runs with the nearest-higher block boxes
+  } else {
+    k_density_combine<N><<<grid_for(kp.n, 256), 256, 0, s>>>(kp, events_of(ws), kp.n, ws.rho_fix, ws.rec_r, kmax);
+  }
 }
 // The symmetric sweep covers exactly the reference's candidates when the metric bounds every
 // coordinate difference and no coordinate wraps.
@@ -1843,13 +1876,13 @@ inline bool symmetric_density_ok(const KParams& kp, int metric, int ndim) {
   return true;
 }
 template <int N>
-void launch_density_sym_metric(int metric, const KParams& kp, Workspace& ws, cudaStream_t s) {
+void launch_density_sym_metric(int metric, const KParams& kp, Workspace& ws, cudaStream_t s, bool fuse_combine) {
   if (metric == CLUE_METRIC_MANHATTAN)
-    launch_density_sym<N, CLUE_METRIC_MANHATTAN>(kp, ws, s);
+    launch_density_sym<N, CLUE_METRIC_MANHATTAN>(kp, ws, s, fuse_combine);
   else if (metric == CLUE_METRIC_CHEBYSHEV)
-    launch_density_sym<N, CLUE_METRIC_CHEBYSHEV>(kp, ws, s);
+    launch_density_sym<N, CLUE_METRIC_CHEBYSHEV>(kp, ws, s, fuse_combine);
   else
-    launch_density_sym<N, CLUE_METRIC_EUCLIDEAN>(kp, ws, s);
+    launch_density_sym<N, CLUE_METRIC_EUCLIDEAN>(kp, ws, s, fuse_combine);
 }
 template <int N, int MT>
 void launch_seeds(const KParams& kp, Workspace& ws, cudaStream_t s) {
@@ -1986,25 +2019,29 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
 
   stage_mark(ws, 1, s);
   if (symmetric) {
-    launch_density_sym_metric<N>(a.metric, kp, ws, s);
+    launch_density_sym_metric<N>(a.metric, kp, ws, s, composite);
   } else if (spatial_density) {
     CLUE_METRIC_SWITCH(a.metric, launch_density_spatial, kp, ws, s);
   } else {
     CLUE_METRIC_SWITCH(a.metric, launch_density, kp, ws, s);
   }
-  launches += symmetric ? 2 : 1;
+  launches += symmetric && !composite ? 2 : 1;  // (a composite run combines with the block boxes)
   stage_mark(ws, 2, s);
   // Morton-ordered copy of the records with their densities (the tile-ordered records themselves
   // after a composite sort) and its block / super-block boxes with the largest rho, for the
   // nearest-higher search
   if (composite) {
+    // the tile-ordered records are the Morton-ordered ones; the density's fixed-point sums are
+    // added in while the block boxes are built
     ws.rec_m_cur = ws.rec_r;
+    k_combine_block_bbox<N><<<grid_for(nblk_threads, 256), 256, 0, s>>>(kp, ev, n, ws.rho_fix, ws.rec_r,
+                                                                         ws.sym_kmax, ws.blk);
   } else {
     k_gather_morton<N><<<grid_for(n, 256), 256, 0, s>>>(ws.rec_r, n, ws.mq, ws.rec_m);
     ws.rec_m_cur = ws.rec_m;
     ++launches;
+    k_block_bbox<N><<<grid_for(nblk_threads, 256), 256, 0, s>>>(ws.rec_m_cur, n, ws.blk);
   }
-  k_block_bbox<N><<<grid_for(nblk_threads, 256), 256, 0, s>>>(ws.rec_m_cur, n, ws.blk);
   k_superblock_bbox<N><<<grid_for(nsb_threads, 256), 256, 0, s>>>(ws.blk, n, ws.sblk);
   CLUE_METRIC_SWITCH(a.metric, launch_nh, kp, ws, s);
   stage_mark(ws, 3, s);

@@ -126,6 +126,7 @@ struct Workspace {
   float4* tblk = nullptr;         // boxes of 32-record blocks counted from every tile's start
   uint32_t* tblk_off = nullptr;   // [ntiles] such blocks per tile, then exclusive-scanned
   int64_t* rho_fix = nullptr;     // fixed-point density contributions of the symmetric sweep
+  float sym_kmax = 1.0f;          // their scale's kernel bound, for a combine run later
 
   // pinned host copy of the event tables (same layout as the device block)
   void* pinned = nullptr;
