@@ -1712,17 +1712,38 @@ __global__ void __launch_bounds__(256) k_jump(int32_t* par, int n, int iters, De
   if (round > 0 && st->unresolved[round - 1] == 0) return;
   bool unres = false;
   const int stride = gridDim.x * blockDim.x;
-  for (int pos = blockIdx.x * blockDim.x + threadIdx.x; pos < n; pos += stride) {
-    int p = par[pos];
-    if (p < 0) continue;
-    int it = 0;
-    for (; it < iters; ++it) {
-      const int pp = __ldcg(par + p);
-      if (pp < 0) break;
-      p = pp;
-      par[pos] = p;
+  // four chains per thread walked in lockstep: each step's four parent loads are independent,
+  // so they are in flight together (the walk is bound by load latency, not bandwidth)
+  constexpr int K = 4;
+  for (int64_t pos0 = blockIdx.x * blockDim.x + threadIdx.x; pos0 < n; pos0 += (int64_t)K * stride) {
+    int p[K];
+    bool act[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int64_t pos = pos0 + (int64_t)k * stride;
+      p[k] = pos < n ? par[pos] : -1;
+      act[k] = p[k] >= 0;
     }
-    if (it == iters && __ldcg(par + p) >= 0) unres = true;
+    for (int it = 0; it < iters; ++it) {
+      bool any = false;
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        if (act[k]) {
+          const int pp = __ldcg(par + p[k]);
+          if (pp < 0) {
+            act[k] = false;
+          } else {
+            p[k] = pp;
+            par[pos0 + (int64_t)k * stride] = pp;
+          }
+        }
+        any |= act[k];
+      }
+      if (!any) break;
+    }
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+      if (act[k] && __ldcg(par + p[k]) >= 0) unres = true;  // still climbing after `iters` jumps
   }
   if (__any_sync(0xffffffffu, unres) && (threadIdx.x & 31) == 0) atomicAdd(&st->unresolved[round], 1u);
   if (blockIdx.x == 0 && threadIdx.x == 0) atomicMax(&st->label_rounds, (uint32_t)round + 1);
