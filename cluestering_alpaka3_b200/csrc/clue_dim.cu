@@ -1213,15 +1213,16 @@ __global__ void __launch_bounds__(kTileThreads, (N <= 2 ? 8 : (N <= 4 ? 6 : 4)) 
     auto consider = [&](int j, float s, float rho_j, bool in_block) {
       const bool c = need && in_block && s <= bnd && rho_j >= rho_i;
       const bool fast = c && rho_j > rho_i && s * slack < s_best;
-      if (fast) {
-        s_best = s;
-        bnd = fminf(tdm, s * slack);
-        nh = sq[j];
-        lex_best = (int)lexpos;
-        if (TIE != CLUE_TIE_REFERENCE) {
-          rho_best = rho_j;
-          orig_best = -1;  // read from perm when a tie needs it
-        }
+      // selects rather than a branch: the candidate's position is a shared-memory broadcast
+      const int qj = sq[j];
+      const float bj = fminf(tdm, s * slack);
+      s_best = fast ? s : s_best;
+      bnd = fast ? bj : bnd;
+      nh = fast ? qj : nh;
+      lex_best = fast ? (int)lexpos : lex_best;
+      if (TIE != CLUE_TIE_REFERENCE) {
+        rho_best = fast ? rho_j : rho_best;
+        orig_best = fast ? -1 : orig_best;  // -1: read from perm when a tie needs it
       }
       const bool slow = c && !fast;
       if (!__any_sync(0xffffffffu, slow)) return;
