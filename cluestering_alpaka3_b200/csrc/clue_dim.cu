@@ -1210,7 +1210,12 @@ __global__ void __launch_bounds__(kTileThreads, (N <= 2 ? 8 : (N <= 4 ? 6 : 4)) 
     // strictly denser candidate whose distance rounds strictly below the best one's, is a
     // predicated update; equal densities (index rule) and distances that may round to the best
     // one's (rank rule) take the full test, entered only when some lane has such a case.
-    auto consider = [&](int j, float s, float rho_j, bool in_block) {
+    // Update of the lane's best by candidate j, in two parts.  consider_fast() takes the common
+    // case, a strictly denser candidate whose distance rounds strictly below the best one's, with
+    // selects, and returns whether the candidate needs the full test (equal densities: index
+    // rule; distances that may round to the best one's: rank rule).  consider_full() is that
+    // test; it may run after other candidates' updates, since the best is an exact minimum.
+    auto consider_fast = [&](int j, float s, float rho_j, bool in_block) -> bool {
       const bool c = need && in_block && s <= bnd && rho_j >= rho_i;
       const bool fast = c && rho_j > rho_i && s * slack < s_best;
       // selects rather than a branch: the candidate's position is a shared-memory broadcast
@@ -1224,48 +1229,51 @@ __global__ void __launch_bounds__(kTileThreads, (N <= 2 ? 8 : (N <= 4 ? 6 : 4)) 
         rho_best = fast ? rho_j : rho_best;
         orig_best = fast ? -1 : orig_best;  // -1: read from perm when a tie needs it
       }
-      const bool slow = c && !fast;
-      if (!__any_sync(0xffffffffu, slow)) return;
-      if (slow) {
-        const int q = sq[j];
-        int orig_j = -1;
-        bool higher = rho_j > rho_i;
-        if (!higher && rho_j > 0.0f) {
-          orig_j = __ldg(perm + q);
-          higher = orig_j > orig_i;
-        }
-        if (higher) {
-          bool better;
-          if (s * slack < s_best) {
-            better = true;  // its distance rounds strictly below the best one's
-          } else {
-            // the two distances may round to the same value: decide on the rounded distances,
-            // then on the iteration rank (search-box position of the tile, then the original
-            // index, which orders the points of one tile in the reference's iteration)
-            const float dist = M::finish(s), dbest = M::finish(s_best);
-            if (dist != dbest || nh < 0) {
-              better = dist < dbest;
-            } else if (TIE == CLUE_TIE_REFERENCE && (int)lexpos != lex_best) {
-              better = (int)lexpos < lex_best;
-            } else {
-              if (orig_j < 0) orig_j = __ldg(perm + q);
-              const int ob = TIE == CLUE_TIE_REFERENCE || orig_best < 0 ? __ldg(perm + nh) : orig_best;
-              better = TIE == CLUE_TIE_REFERENCE ? orig_j < ob
-                                                 : rho_j > rho_best || (rho_j == rho_best && orig_j < ob);
-            }
-          }
-          if (better) {
-            s_best = s;
-            bnd = fminf(tdm, s * slack);
-            nh = q;
-            lex_best = (int)lexpos;
-            if (TIE != CLUE_TIE_REFERENCE) {
-              rho_best = rho_j;
-              orig_best = orig_j;
-            }
-          }
+      return c && !fast;
+    };
+    auto consider_full = [&](int j, float s, float rho_j) {
+      const int q = sq[j];
+      int orig_j = -1;
+      bool higher = rho_j > rho_i;
+      if (!higher && rho_j > 0.0f) {
+        orig_j = __ldg(perm + q);
+        higher = orig_j > orig_i;
+      }
+      if (!higher) return;
+      bool better;
+      if (s * slack < s_best) {
+        better = true;  // its distance rounds strictly below the best one's
+      } else {
+        // the two distances may round to the same value: decide on the rounded distances,
+        // then on the iteration rank (search-box position of the tile, then the original
+        // index, which orders the points of one tile in the reference's iteration)
+        const float dist = M::finish(s), dbest = M::finish(s_best);
+        if (dist != dbest || nh < 0) {
+          better = dist < dbest;
+        } else if (TIE == CLUE_TIE_REFERENCE && (int)lexpos != lex_best) {
+          better = (int)lexpos < lex_best;
+        } else {
+          if (orig_j < 0) orig_j = __ldg(perm + q);
+          const int ob = TIE == CLUE_TIE_REFERENCE || orig_best < 0 ? __ldg(perm + nh) : orig_best;
+          better = TIE == CLUE_TIE_REFERENCE ? orig_j < ob
+                                             : rho_j > rho_best || (rho_j == rho_best && orig_j < ob);
         }
       }
+      if (better) {
+        s_best = s;
+        bnd = fminf(tdm, s * slack);
+        nh = q;
+        lex_best = (int)lexpos;
+        if (TIE != CLUE_TIE_REFERENCE) {
+          rho_best = rho_j;
+          orig_best = orig_j;
+        }
+      }
+    };
+    // both parts for one candidate (called by the whole warp)
+    auto consider = [&](int j, float s, float rho_j, bool in_block) {
+      const bool slow = consider_fast(j, s, rho_j, in_block);
+      if (__any_sync(0xffffffffu, slow) && slow) consider_full(j, s, rho_j);
     };
     // Few lanes need this block: its candidates are split among all 32 lanes, G lanes per
     // needing home (G = 32 / P, P >= the number of such homes, a power of two); each group finds
@@ -1344,8 +1352,12 @@ __global__ void __launch_bounds__(kTileThreads, (N <= 2 ? 8 : (N <= 4 ? 6 : 4)) 
                                : make_float2(M::partial(x, ca, kp.mpar), M::partial(x, cb, kp.mpar));
       const bool any = (s2.x <= bnd && ra >= rho_i) || (j + 1 < cnt && s2.y <= bnd && rb >= rho_i);
       if (__any_sync(0xffffffffu, need && any)) {
-        consider(j, s2.x, ra, true);
-        consider(j + 1, s2.y, rb, j + 1 < cnt);
+        const bool slow_a = consider_fast(j, s2.x, ra, true);
+        const bool slow_b = consider_fast(j + 1, s2.y, rb, j + 1 < cnt);
+        if (__any_sync(0xffffffffu, slow_a || slow_b)) {  // one vote for both full tests
+          if (slow_a) consider_full(j, s2.x, ra);
+          if (slow_b) consider_full(j + 1, s2.y, rb);
+        }
       }
     }
   });
