@@ -5,7 +5,10 @@
 // (include/CLUEstering/core/detail/Clusterer.hpp:134-171):
 //   k_bbox_* / k_grid    compute_tile_size        core/detail/ComputeTiles.hpp:13-27
 //   k_bin + radix sort   Tiles::fill              data_structures/internal/Tiles.hpp:92-96
+//   (k_bin_composite)    (one (tile, Morton) sort on the symmetric density path)
 //   k_density            KernelCalculateLocalDensity  core/detail/ClusteringKernels.hpp:66-107
+//   k_density_sym /      the same sums in spatial order (exponential / Gaussian kernels):
+//   k_density_spatial    symmetric pair sweep or one-sided sweep over Morton blocks
 //   k_nearest_higher     KernelCalculateNearestHigher core/detail/ClusteringKernels.hpp:109-212
 //   k_seeds              KernelFindClusters       core/detail/ClusteringKernels.hpp:214-244
 //   k_jump + k_finalize  Followers::fill + KernelAssignClusters
@@ -17,10 +20,13 @@
 // own reference grid; tile keys are event-major, so one stable sort of (tile, index) pairs
 // orders every event by tile while keeping events contiguous.
 //
-// Layout in HBM: points are reordered by tile (stable: ascending index inside a tile)
-// into float4 records {coords..., payload}.  A CTA processes a chunk of 128 home points of
-// one tile; the candidate tiles of the chunk are staged into shared memory with bulk copies
-// and every candidate record is one broadcast 16-byte shared-memory load per warp.
+// Layout in HBM: points are reordered by tile into float4 records {coords..., payload}: by
+// ascending index inside a tile for the reference-order density, by Morton code inside a tile
+// for the spatial sweeps.  A CTA processes a chunk of 128 home points of one tile (four warps
+// of 32).  The reference-order density stages whole candidate tiles into shared memory with
+// bulk copies; the spatial sweeps stage one 32-record Morton block per warp, skip blocks whose
+// bounding box is out of reach, and read every candidate as one broadcast 16-byte
+// shared-memory load (nearest higher) or from its owner lane by shuffle (symmetric density).
 #include "clue_internal.h"
 #include "clue_tma.cuh"
 
