@@ -1571,15 +1571,33 @@ __global__ void __launch_bounds__(kTileThreads, (N <= 4 ? 8 : 4) * 128 / kTileTh
   {
     float4* sm = s_rec[warp];
     stage_block<N>(sm, rec_m, startA, cntA);
-    for (int j = 0; j < cntA; ++j) {
-      float cx[N], wj;
-      smem_rec<N>(sm, j, cx, wj);
-      const float sd = M::partial(x, cx, kp.mpar);
-      const bool in = hv && sd <= tdc;
-      if (__any_sync(0xffffffffu, in)) {
-        const float t2 = kval(sd, j == lane) * wj;
-        if (in) acc = fadd(acc, t2);
+    if (FORM == kDensGeneric) {  // the generic kernel needs the self test
+      for (int j = 0; j < cntA; ++j) {
+        float cx[N], wj;
+        smem_rec<N>(sm, j, cx, wj);
+        const float sd = M::partial(x, cx, kp.mpar);
+        const bool in = hv && sd <= tdc;
+        if (__any_sync(0xffffffffu, in)) {
+          const float t2 = kval(sd, j == lane) * wj;
+          if (in) acc = fadd(acc, t2);
+        }
       }
+    } else {
+      // two candidates at a time, no branch (the own block almost always has pairs within dc);
+      // a record past the block's end (stale shared memory) is masked with its weight
+      float2 acc2 = make_float2(0.0f, 0.0f);
+      for (int j = 0; j < cntA; j += 2) {
+        float ca[N], cb[N], wa, wb;
+        smem_rec<N>(sm, j, ca, wa);
+        smem_rec<N>(sm, j + 1, cb, wb);
+        const bool bv = j + 1 < cntA;
+        const float2 sd = partial_pair<N, MT>(x, ca, cb, kp.mpar);
+        float2 kv = kval2(sd);
+        kv.x = hv && sd.x <= tdc ? kv.x : 0.0f;
+        kv.y = hv && bv && sd.y <= tdc ? kv.y : 0.0f;
+        acc2 = fma2(kv, make_float2(wa, bv ? wb : 0.0f), acc2);
+      }
+      acc = fadd(acc, fadd(acc2.x, acc2.y));
     }
   }
   // later blocks of the own tile, then the later tiles of the union box, both ways
