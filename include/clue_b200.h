@@ -224,6 +224,10 @@ uint64_t clue_context_kernel_launches(clue_context ctx);
  * own reference tile grid and its labels are numbered from 0 inside the event, exactly as if
  * it had been clustered alone.  ev_n_clusters (optional, n_events entries, same memory space
  * as the outputs) receives every event's cluster count; `info` holds the totals.
+ * With CLUE_MEM_HOST, a batch of 4M points or more is run in chunks of whole events whose
+ * copies overlap the previous chunk's pipeline (clue_tuning.overlap_chunk_points); the outputs
+ * are the same as one pass, and the call returns when they are in `out`.  Pinned host buffers
+ * are needed for the copies to overlap.
  */
 clue_status clue_batch_make_clusters(clue_context ctx, const clue_params* params, const clue_kernel* kernel,
                                      const clue_metric* metric, int32_t ndim, int32_t n_events,
