@@ -42,7 +42,7 @@ EXPORTED = [
     "clue_graph_launch", "clue_graph_destroy", "clue_events_loop", "clue_context_reserve_batch",
     "clue_server_create", "clue_server_destroy", "clue_server_submit", "clue_server_wait",
     "clue_server_stats_read", "clue_server_replay", "clue_tuning_defaults", "clue_context_set_tuning",
-    "clue_context_get_tuning", "clue_autotune_batch",
+    "clue_context_get_tuning", "clue_autotune_batch", "clue_silhouette",
 ]
 
 
@@ -176,6 +176,7 @@ def _load() -> ctypes.CDLL:
     sig["clue_server_stats_read"] = ([vp, ctypes.POINTER(_ServerStats)], ctypes.c_int)
     sig["clue_server_replay"] = ([vp, i32, vp, vp, vp, vp, vp, ctypes.POINTER(_Outputs), vp, ctypes.POINTER(i32)],
                                  ctypes.c_int)
+    sig["clue_silhouette"] = ([vp, i32, i32, vp, vp, vp, ctypes.POINTER(f32), vp], ctypes.c_int)
     sig["clue_tuning_defaults"] = ([ctypes.POINTER(_Tuning)], None)
     sig["clue_context_set_tuning"] = ([vp, ctypes.POINTER(_Tuning)], ctypes.c_int)
     sig["clue_context_get_tuning"] = ([vp, ctypes.POINTER(_Tuning)], ctypes.c_int)
@@ -434,6 +435,16 @@ class Context:
                                       ctypes.c_void_p(weight_ptr), ctypes.c_void_p(stream),
                                       cache_path.encode() if cache_path else None, ctypes.byref(t)))
         return {f: getattr(t, f) for f, _ in _Tuning._fields_}
+
+    def silhouette_device(self, coords_ptr: int, labels_ptr: int, ndim: int, n: int, per_point_ptr: int = 0,
+                          stream: int = 0) -> float:
+        """Silhouette score on the GPU (clue_silhouette) of device coordinates (SoA) and labels;
+        per_point_ptr (device, n floats) optionally receives every point's score."""
+        mean = ctypes.c_float(0.0)
+        check(lib.clue_silhouette(self.handle, ndim, n, ctypes.c_void_p(coords_ptr), ctypes.c_void_p(labels_ptr),
+                                  ctypes.c_void_p(per_point_ptr or None), ctypes.byref(mean),
+                                  ctypes.c_void_p(stream)))
+        return float(mean.value)
 
     def set_timing(self, enable: bool = True):
         check(lib.clue_context_set_timing(self.handle, 1 if enable else 0))

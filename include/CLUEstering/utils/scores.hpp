@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstddef>
 #include <limits>
+#include <memory>
 #include <vector>
 
 namespace clue {
@@ -64,6 +65,38 @@ namespace clue {
       ++count;
     }
     return sum / static_cast<float>(count);
+  }
+
+  // The same score computed on the GPU (clue_silhouette) from device points and their labels,
+  // bit for bit equal to silhouette(points) on a host copy.  Coordinates that are not one
+  // contiguous SoA block are copied into one first.
+  template <concepts::Queue TQueue, std::size_t Ndim>
+  inline float silhouette(TQueue& queue, const PointsDevice<DevType<TQueue>, Ndim>& points) {
+    const int32_t n = points.size();
+    const float* base = points.coords(0).data();
+    bool contiguous = true;
+    for (std::size_t d = 1; d < Ndim; ++d) contiguous = contiguous && points.coords(d).data() == base + d * n;
+    void* tmp = nullptr;
+    if (!contiguous) {
+      detail::check(clue_device_alloc(queue.getDevice().id, Ndim * (std::size_t)n * sizeof(float), &tmp));
+      for (std::size_t d = 0; d < Ndim; ++d)
+        detail::check(clue_memcpy_dtod(static_cast<float*>(tmp) + d * n, points.coords(d).data(),
+                                       (std::size_t)n * sizeof(float), queue.stream()));
+      base = static_cast<const float*>(tmp);
+    }
+    std::unique_ptr<void, clue_status (*)(void*)> guard(tmp, clue_device_free);
+    static thread_local std::unique_ptr<clue_context_s, clue_status (*)(clue_context)> ctx(nullptr, clue_context_destroy);
+    static thread_local int32_t ctx_dev = -1;
+    if (!ctx || ctx_dev != queue.getDevice().id) {
+      clue_context c = nullptr;
+      detail::check(clue_context_create(queue.getDevice().id, &c));
+      ctx.reset(c);
+      ctx_dev = queue.getDevice().id;
+    }
+    float mean = 0.f;
+    detail::check(clue_silhouette(ctx.get(), static_cast<int32_t>(Ndim), n, base, points.clusterIndexes().data(), nullptr,
+                                  &mean, queue.stream()));
+    return mean;
   }
 
 }  // namespace clue

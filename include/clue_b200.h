@@ -329,6 +329,20 @@ clue_status clue_get_clusters(clue_context ctx, int32_t n, const int32_t* cluste
                               int32_t* offsets, int32_t* points, int32_t* n_clusters_out,
                               int32_t* n_clustered_out, void* stream);
 
+/*
+ * Silhouette score on the GPU (reference include/CLUEstering/utils/detail/scores.hpp:17-99,
+ * computed there on the host): for a point of a cluster with at least two points,
+ * s = (b - a) / max(a, b) with a the mean distance to the other points of its cluster and b the
+ * smallest mean distance to another cluster's points; Euclidean distances, cluster sums in
+ * ascending point order as the reference's association map gives them.  coords (SoA) and
+ * cluster_index are device arrays of n points (-1 = not clustered).  per_point (device, n
+ * floats, optional) receives every point's score, NaN for points not scored; *mean (host,
+ * optional) the average over the scored points.  n x (clustered points) distances; allocates
+ * its temporaries and synchronises `stream`.
+ */
+clue_status clue_silhouette(clue_context ctx, int32_t ndim, int32_t n, const float* coords,
+                            const int32_t* cluster_index, float* per_point, float* mean, void* stream);
+
 /* ---- serving (no reference counterpart) -------------------------------------------------
  * A request loop with continuous batching on one GPU.  Callers submit single events (host
  * memory) from any thread; a dispatcher thread owned by the server packs every pending event

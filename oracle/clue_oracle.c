@@ -577,3 +577,65 @@ int oracle_rho_f64(const oracle_params* p, int32_t n, const float* coords, const
   free(idx);
   return 0;
 }
+
+/* Silhouette score (include/CLUEstering/utils/detail/scores.hpp:17-99): per point of a cluster
+ * with at least two points, a = sum of distances to the other points of its cluster / (size-1),
+ * b = min over the other clusters (ascending label) of sum of distances / size, both sums over
+ * the cluster's points in ascending index order; s = (b - a) / max(a, b).  Distances:
+ * d = 0; d += (l - r) * (l - r) per dimension in order; sqrt(d), separately rounded.  per_point
+ * gets NAN for points not scored; *mean the FP32 sum of the scores in index order / count. */
+int oracle_silhouette(int32_t ndim, int32_t n, const float* coords, const int32_t* labels, float* per_point,
+                      float* mean) {
+  if (n <= 0 || ndim < 1 || ndim > ORACLE_MAX_DIM) return -1;
+  int32_t k = 0;
+  for (int32_t i = 0; i < n; ++i)
+    if (labels[i] + 1 > k) k = labels[i] + 1;
+  int32_t* off = (int32_t*)calloc((size_t)k + 1, sizeof(int32_t));
+  int32_t* idx = (int32_t*)malloc(sizeof(int32_t) * (size_t)n);
+  int32_t* fill = (int32_t*)calloc((size_t)k + 1, sizeof(int32_t));
+  if (!off || !idx || !fill) return -2;
+  for (int32_t i = 0; i < n; ++i)
+    if (labels[i] >= 0) ++off[labels[i] + 1];
+  for (int32_t c = 0; c < k; ++c) off[c + 1] += off[c];
+  for (int32_t i = 0; i < n; ++i)
+    if (labels[i] >= 0) idx[off[labels[i]] + fill[labels[i]]++] = i; /* ascending index */
+  float acc = 0.0f;
+  int64_t cnt = 0;
+  for (int32_t i = 0; i < n; ++i) {
+    const int32_t own = labels[i];
+    if (own < 0 || off[own + 1] - off[own] < 2) {
+      per_point[i] = NAN;
+      continue;
+    }
+    float a = 0.0f, b = FLT_MAX;
+    for (int32_t c = 0; c < k; ++c) {
+      float sum = 0.0f;
+      for (int32_t q = off[c]; q < off[c + 1]; ++q) {
+        const int32_t j = idx[q];
+        if (c == own && j == i) continue;
+        float d = 0.0f;
+        for (int dd = 0; dd < ndim; ++dd) {
+          const float t = coords[(size_t)dd * n + i] - coords[(size_t)dd * n + j];
+          d = d + t * t;
+        }
+        sum = sum + sqrtf(d);
+      }
+      const int32_t sz = off[c + 1] - off[c];
+      if (c == own) {
+        a = sum / (float)(sz - 1);
+      } else if (sz > 0) {
+        const float m = sum / (float)sz;
+        b = m < b ? m : b;
+      }
+    }
+    const float sc = (b - a) / (a < b ? b : a); /* std::max(a, b) */
+    per_point[i] = sc;
+    acc += sc;
+    ++cnt;
+  }
+  if (mean) *mean = acc / (float)cnt;
+  free(off);
+  free(idx);
+  free(fill);
+  return 0;
+}

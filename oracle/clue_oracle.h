@@ -85,6 +85,10 @@ int oracle_run(const oracle_params* p, int32_t n, const float* coords, const flo
 int oracle_nearest_higher(const oracle_params* p, int32_t n, const float* coords, const float* rho,
                           int32_t* nearest_higher, float* delta, int64_t* distance_ties);
 
+/* Silhouette score of labelled points (per point, NAN where not scored, and the mean). */
+int oracle_silhouette(int32_t ndim, int32_t n, const float* coords, const int32_t* labels, float* per_point,
+                      float* mean);
+
 int oracle_tiles(const oracle_params* p, int32_t n, const float* coords, oracle_grid* grid,
                  int32_t* offsets, int32_t* indexes);
 

@@ -75,6 +75,9 @@ def _load():
                                               ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
                                               ctypes.POINTER(ctypes.c_int64)]
         lib.oracle_nearest_higher.restype = ctypes.c_int
+        lib.oracle_silhouette.argtypes = [ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.c_void_p, ctypes.POINTER(ctypes.c_float)]
+        lib.oracle_silhouette.restype = ctypes.c_int
         lib.oracle_metric.argtypes = [ctypes.POINTER(_Params), ctypes.c_void_p, ctypes.c_void_p]
         lib.oracle_metric.restype = ctypes.c_float
         lib.oracle_kernel.argtypes = [ctypes.POINTER(_Params), ctypes.c_float, ctypes.c_int32,
@@ -185,6 +188,22 @@ def nearest_higher(coords: np.ndarray, rho: np.ndarray, cfg: Config):
     if rc != 0:
         raise ValueError(f"oracle_nearest_higher failed ({rc})")
     return nh, delta, int(ties.value)
+
+
+def silhouette(coords: np.ndarray, labels: np.ndarray):
+    """Silhouette score of labelled points: (per-point scores with NaN where not scored, mean).
+
+    Restates include/CLUEstering/utils/detail/scores.hpp:17-99 with separately rounded FP32."""
+    lib = _load()
+    c = _soa(coords)
+    ndim, n = c.shape
+    lab = np.ascontiguousarray(labels, dtype=np.int32)
+    per = np.empty(n, np.float32)
+    mean = ctypes.c_float(0.0)
+    rc = lib.oracle_silhouette(ndim, n, c.ctypes.data, lab.ctypes.data, per.ctypes.data, ctypes.byref(mean))
+    if rc != 0:
+        raise ValueError(f"oracle_silhouette failed ({rc})")
+    return per, float(mean.value)
 
 
 def tiles(coords: np.ndarray, cfg: Config):

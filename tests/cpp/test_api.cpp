@@ -304,8 +304,12 @@ static int run_gpu(const std::string& in, float dc, float rhoc, float dm, const 
     f << h_points.coords(0)[i] << "," << h_points.coords(1)[i] << "," << h_points.weights()[i] << "," << ref[i] << ","
       << is_seed[i] << "," << nh[i] << "," << bits(rho[i]) << "," << bits(delta[i]) << "\n";
   f.close();
-  std::printf("silhouette=%.6f n_clusters=%lld dropped=%lld\n", clue::silhouette(h_points),
-              (long long)info.n_clusters, (long long)info.dropped_seeds);
+  // silhouette on the GPU equals the host evaluation bit for bit
+  const float sil = clue::silhouette(h_points);
+  const float sil_dev = clue::silhouette(queue, d_points);
+  CHECK(bits(sil) == bits(sil_dev));
+  std::printf("silhouette=%.6f n_clusters=%lld dropped=%lld\n", sil, (long long)info.n_clusters,
+              (long long)info.dropped_seeds);
   return 0;
 }
 

@@ -61,3 +61,53 @@ def test_get_clusters_rejects_labels_out_of_range(gpu_context):
     labels = np.array([0, 1, 7, -1, -2], np.int32)  # 7 >= n and -2 < -1
     with pytest.raises(capi.ClueError):
         device_csr(gpu_context, labels)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,ndim", [("data_4096", 2), ("blobs3d", 3)])
+def test_silhouette_gpu_matches_oracle(gpu_context, name, ndim):
+    # clue_silhouette against the oracle's restatement of the reference's scores.hpp: every
+    # point's score bit for bit (cluster sums in ascending point order, separately rounded
+    # FP32), points not scored NaN, and the FP32 mean in index order
+    import os
+    import torch
+    from oracle import oracle as O
+    if name == "data_4096":
+        z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", name + ".npz"))
+        coords, weight = z["coords"], z["weight"]
+        dc_, rhoc_, dm_ = (float(v) for v in z["params"])
+        kw = dict(dc=dc_, rhoc=rhoc_, dm=dm_)
+    else:
+        rng = np.random.default_rng(151)
+        coords, weight = random_blobs(rng, 3000, 3, nblobs=6, extent=30.0, sigma=0.8)
+        kw = dict(dc=1.2, rhoc=3.0, dm=1.6)
+    res = gpu_context.make_clusters_host(coords, weight, *gpu_args(**kw))
+    labels = res.cluster_index
+    assert labels.max() >= 1  # at least two clusters
+    n = coords.shape[1]
+    dc = torch.from_numpy(np.ascontiguousarray(coords, dtype=np.float32)).cuda()
+    dl = torch.from_numpy(labels.astype(np.int32)).cuda()
+    per = torch.empty(n, dtype=torch.float32, device="cuda")
+    mean = gpu_context.silhouette_device(dc.data_ptr(), dl.data_ptr(), ndim, n, per.data_ptr())
+    ref_per, ref_mean = O.silhouette(coords, labels)
+    got = per.cpu().numpy()
+    np.testing.assert_array_equal(np.isnan(got), np.isnan(ref_per))
+    ok = ~np.isnan(ref_per)
+    np.testing.assert_array_equal(got[ok].view(np.uint32), ref_per[ok].view(np.uint32))
+    assert np.float32(mean).view(np.uint32) == np.float32(ref_mean).view(np.uint32)
+
+
+@pytest.mark.gpu
+def test_silhouette_gpu_reference_known_answer(gpu_context):
+    # the reference's check on data_32768 (tests/test_device_points.cpp:252-268): 20 clusters
+    # with silhouette >= 0.9
+    import os
+    import torch
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "data_32768.npz"))
+    coords, weight = z["coords"], z["weight"]
+    res = gpu_context.make_clusters_host(coords, weight, *gpu_args(dc=1.3, rhoc=10.0, dm=1.3))
+    assert res.info.n_clusters == 20
+    n = coords.shape[1]
+    dc = torch.from_numpy(np.ascontiguousarray(coords, dtype=np.float32)).cuda()
+    dl = torch.from_numpy(res.cluster_index.astype(np.int32)).cuda()
+    assert gpu_context.silhouette_device(dc.data_ptr(), dl.data_ptr(), 2, n) >= 0.9

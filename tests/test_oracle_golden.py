@@ -113,3 +113,47 @@ def test_nearest_higher_stage_matches_full_run(tiebreak):
     np.testing.assert_array_equal(nh[keep], ref.nearest_higher[keep])
     np.testing.assert_array_equal(delta.view(np.uint32), ref.delta.view(np.uint32))
     assert ties == ref.stats["nh_distance_ties"] > 0
+
+
+def test_silhouette_restatement_matches_scalar_float32():
+    # the oracle's silhouette against a plain float32 evaluation of the reference's definition
+    # (scores.hpp:17-99) on a small labelled set
+    rng = np.random.default_rng(12)
+    n = 90
+    c = rng.normal(size=(2, n)).astype(np.float32)
+    c[0, :40] += np.float32(4.0)
+    lab = np.where(np.arange(n) < 40, 0, np.where(np.arange(n) < 75, 1, 2)).astype(np.int32)
+    lab[::11] = -1
+    per, mean = O.silhouette(c, lab)
+    f = np.float32
+    k = int(lab.max()) + 1
+    members = [np.nonzero(lab == q)[0] for q in range(k)]
+    scores = []
+    for i in range(n):
+        own = lab[i]
+        if own < 0 or members[own].size < 2:
+            assert np.isnan(per[i])
+            continue
+        a, b = f(0), f(np.finfo(np.float32).max)
+        for q in range(k):
+            s = f(0)
+            for j in members[q]:
+                if q == own and j == i:
+                    continue
+                d = f(0)
+                for dd in range(2):
+                    t = f(c[dd, i] - c[dd, j])
+                    d = f(d + f(t * t))
+                s = f(s + f(np.sqrt(d)))
+            if q == own:
+                a = f(s / f(members[q].size - 1))
+            else:
+                m = f(s / f(members[q].size))
+                b = m if m < b else b
+        sc = f(f(b - a) / (b if a < b else a))
+        assert per[i].view(np.uint32) == sc.view(np.uint32), i
+        scores.append(sc)
+    acc = f(0)
+    for sc in scores:
+        acc = f(acc + sc)
+    assert np.float32(mean).view(np.uint32) == f(acc / f(len(scores))).view(np.uint32)
