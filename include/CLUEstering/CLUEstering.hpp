@@ -13,3 +13,4 @@
 #include "CLUEstering/utils/get_clusters.hpp"
 #include "CLUEstering/utils/read_csv.hpp"
 #include "CLUEstering/utils/scores.hpp"
+#include "CLUEstering/utils/validation.hpp"

@@ -211,6 +211,26 @@ static void test_properties_io(const std::string& dir) {
   CHECK(gm.size() == 2 && gm.count(1) == 3);
   const float s = clue::silhouette(res);
   CHECK(std::isfinite(s) && s > -1.f && s <= 1.f);
+  // validate_results: cluster count and sizes, whatever the labels
+  auto write_labels = [&](const std::string& path, const int (&labels)[6]) {
+    std::ofstream f(path);
+    f << "x0,x1,weight,cluster_ids,is_seed\n";
+    for (int i = 0; i < 6; ++i) f << i << "," << 2 * i << ",1," << labels[i] << ",0\n";
+  };
+  const int relabelled[6] = {1, 1, 0, -1, 0, 0};
+  const int moved[6] = {0, 0, 1, -1, -1, 1};
+  const int merged[6] = {0, 0, 0, -1, 0, 0};
+  write_labels(dir + "/relabelled.csv", relabelled);
+  write_labels(dir + "/moved.csv", moved);
+  write_labels(dir + "/merged.csv", merged);
+  auto same = clue::read_output(dim, out);
+  auto rel = clue::read_output(dim, dir + "/relabelled.csv");
+  auto mov = clue::read_output(dim, dir + "/moved.csv");
+  auto mer = clue::read_output(dim, dir + "/merged.csv");
+  CHECK(clue::validate_results(res, same));
+  CHECK(clue::validate_results(res, rel) && clue::validate_results(rel, res));
+  CHECK(!clue::validate_results(res, mov));  // same count, sizes {2, 3} against {2, 2}
+  CHECK(!clue::validate_results(res, mer));  // one cluster against two
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -308,6 +328,7 @@ static int run_gpu(const std::string& in, float dc, float rhoc, float dm, const 
   const float sil = clue::silhouette(h_points);
   const float sil_dev = clue::silhouette(queue, d_points);
   CHECK(bits(sil) == bits(sil_dev));
+  CHECK(clue::validate_results(back, h_points));
   std::printf("silhouette=%.6f n_clusters=%lld dropped=%lld\n", sil, (long long)info.n_clusters,
               (long long)info.dropped_seeds);
   return 0;
