@@ -25,7 +25,8 @@ METRIC_EUCLIDEAN, METRIC_WEIGHTED_EUCLIDEAN, METRIC_PERIODIC_EUCLIDEAN, METRIC_M
     METRIC_CHEBYSHEV, METRIC_WEIGHTED_CHEBYSHEV = range(6)
 TIE_REFERENCE, TIE_RHO_INDEX = 0, 1
 MEM_DEVICE, MEM_HOST = 0, 1
-FLAG_REFERENCE_ORDER, FLAG_SPATIAL_DENSITY = 1, 2
+FLAG_REFERENCE_ORDER, FLAG_SPATIAL_DENSITY, FLAG_NEAR_TIES = 1, 2, 4
+NEAR_TOL = 1e-5
 
 # Every symbol declared in include/clue_b200.h.
 EXPORTED = [
@@ -42,7 +43,7 @@ EXPORTED = [
     "clue_graph_launch", "clue_graph_destroy", "clue_events_loop", "clue_context_reserve_batch",
     "clue_server_create", "clue_server_destroy", "clue_server_submit", "clue_server_wait",
     "clue_server_stats_read", "clue_server_replay", "clue_tuning_defaults", "clue_context_set_tuning",
-    "clue_context_get_tuning", "clue_autotune_batch", "clue_silhouette",
+    "clue_context_get_tuning", "clue_autotune_batch", "clue_silhouette", "clue_context_read_near_counts",
 ]
 
 
@@ -86,6 +87,11 @@ class _RunInfo(ctypes.Structure):
                 ("dropped_seeds", ctypes.c_int64), ("seed_capacity_used", ctypes.c_int64),
                 ("n_tiles", ctypes.c_int64), ("n_per_dim", ctypes.c_int64),
                 ("label_rounds", ctypes.c_int64)]
+
+
+class _NearCounts(ctypes.Structure):
+    _fields_ = [("rho_near_rhoc", ctypes.c_int64), ("delta_near_seed_dc", ctypes.c_int64),
+                ("delta_near_dm", ctypes.c_int64), ("nh_near_ties", ctypes.c_int64)]
 
 
 class _ServerConfig(ctypes.Structure):
@@ -149,6 +155,7 @@ def _load() -> ctypes.CDLL:
                                       ctypes.POINTER(_Metric), i32, i32, vp, vp,
                                       ctypes.POINTER(_Outputs), vp], ctypes.c_int),
         "clue_context_read_info": ([vp, vp, ctypes.POINTER(_RunInfo)], ctypes.c_int),
+        "clue_context_read_near_counts": ([vp, vp, ctypes.POINTER(_NearCounts)], ctypes.c_int),
         "clue_context_set_timing": ([vp, i32], ctypes.c_int),
         "clue_context_stage_times": ([vp, ctypes.POINTER(f32), i32], ctypes.c_int),
         "clue_context_kernel_launches": ([vp], ctypes.c_uint64),
@@ -258,7 +265,7 @@ class Params:
     wrapped: tuple = ()
     seed_capacity: int = 0       # reference SeedArray policy; < 0 keeps every seed
     tiebreak: int = TIE_REFERENCE
-    flags: int = 0               # FLAG_REFERENCE_ORDER / FLAG_SPATIAL_DENSITY
+    flags: int = 0               # FLAG_REFERENCE_ORDER / FLAG_SPATIAL_DENSITY / FLAG_NEAR_TIES
 
     def struct(self) -> _Params:
         p = _Params()
@@ -396,6 +403,14 @@ class Context:
                                          ctypes.c_void_p(weight_ptr), ctypes.byref(out), MEM_DEVICE,
                                          ctypes.c_void_p(stream), ctypes.byref(info)))
             return RunInfo(**{f: getattr(info, f) for f, _ in _RunInfo._fields_})
+
+    def near_counts(self, stream: int = 0) -> dict:
+        """Near-threshold decisions of the last run (relative tolerance NEAR_TOL): densities near
+        rhoc, nearest-higher distances near seed_dc and dm, and (runs with FLAG_NEAR_TIES, else -1)
+        points whose nearest-higher choice compares densities within the tolerance."""
+        c = _NearCounts()
+        check(lib.clue_context_read_near_counts(self.handle, ctypes.c_void_p(stream), ctypes.byref(c)))
+        return {f: int(getattr(c, f)) for f, _ in _NearCounts._fields_}
         check(lib.clue_make_clusters_async(self.handle, ctypes.byref(p), ctypes.byref(k),
                                            ctypes.byref(m), ndim, n, ctypes.c_void_p(coords_ptr),
                                            ctypes.c_void_p(weight_ptr), ctypes.byref(out),

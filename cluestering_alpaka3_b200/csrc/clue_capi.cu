@@ -775,6 +775,39 @@ clue_status clue_context_read_info(clue_context ctx, void* stream, clue_run_info
   return st;
 }
 
+clue_status clue_context_read_near_counts(clue_context ctx, void* stream, clue_near_counts* counts) {
+  if (!ctx || !ctx->ws.arena || !counts) {
+    set_error("context has no completed run");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  Workspace& ws = ctx->ws;
+  const bool ties = (ws.last_kp.flags & CLUE_FLAG_NEAR_TIES) != 0;
+  if (ws.near_from_host) {
+    counts->rho_near_rhoc = ws.near_sum[0];
+    counts->delta_near_seed_dc = ws.near_sum[1];
+    counts->delta_near_dm = ws.near_sum[2];
+    counts->nh_near_ties = ties ? ws.near_sum[3] : -1;
+    return CLUE_OK;
+  }
+  int prev = 0;
+  CLUE_CUDA_TRY(cudaGetDevice(&prev));
+  CLUE_CUDA_TRY(cudaSetDevice(ws.device));
+  cudaStream_t s = (cudaStream_t)stream;
+  DevStatus* h = ws.status_host;
+  cudaError_t e = cudaMemcpyAsync(h, ws.status, sizeof(DevStatus), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  cudaSetDevice(prev);
+  if (e != cudaSuccess) {
+    set_error(std::string("read near counts: ") + cudaGetErrorString(e));
+    return CLUE_ERR_CUDA;
+  }
+  counts->rho_near_rhoc = h->near_rhoc;
+  counts->delta_near_seed_dc = h->near_seed_dc;
+  counts->delta_near_dm = h->near_dm;
+  counts->nh_near_ties = ties ? (int64_t)h->nh_near_ties : -1;
+  return CLUE_OK;
+}
+
 clue_status clue_context_set_timing(clue_context ctx, int32_t enable) {
   if (!ctx) return CLUE_ERR_INVALID_ARG;
   int prev = 0;
@@ -1328,6 +1361,14 @@ static clue_status batch_host_overlapped(clue_context ctx, const clue_params* pa
     rounds = std::max(rounds, cr);
     tiles += chunk_tiles[c];
   }
+  ws.near_from_host = true;
+  for (int k = 0; k < 4; ++k) ws.near_sum[k] = 0;
+  for (int c = 0; c < K; ++c) {
+    ws.near_sum[0] += hs[c].near_rhoc;
+    ws.near_sum[1] += hs[c].near_seed_dc;
+    ws.near_sum[2] += hs[c].near_dm;
+    ws.near_sum[3] += hs[c].nh_near_ties;
+  }
   if (info) {
     info->n_seeds = seeds;
     info->n_clusters = clusters;
@@ -1345,6 +1386,7 @@ struct clue_graph_s {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int device = 0;
+  clue_b200::Workspace* ws = nullptr;  // the captured context's workspace
 };
 
 extern "C" {
@@ -1571,6 +1613,7 @@ clue_status clue_graph_capture_batch(clue_context ctx, const clue_params* params
   auto* g = new (std::nothrow) clue_graph_s;
   if (!g) return CLUE_ERR_OUT_OF_MEMORY;
   g->device = ws.device;
+  g->ws = &ws;
   cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
   if (e == cudaSuccess) {
     st = upload_events(ws, n_events, s);
@@ -1593,6 +1636,7 @@ clue_status clue_graph_capture_batch(clue_context ctx, const clue_params* params
 
 clue_status clue_graph_launch(clue_graph graph, void* stream) {
   if (!graph || !graph->exec) return CLUE_ERR_INVALID_ARG;
+  if (graph->ws) graph->ws->near_from_host = false;  // the replay's counts land on the device
   CLUE_CUDA_TRY(cudaGraphLaunch(graph->exec, (cudaStream_t)stream));
   return CLUE_OK;
 }

@@ -87,8 +87,15 @@ struct DevStatus {
   uint32_t label_rounds;
   uint32_t stage_timeout;  // a bulk-copy wait in a staged sweep gave up
   uint32_t n_clusters;     // seeds kept in the seed lists, summed over events
-  uint32_t pad;
+  // near-threshold decisions (relative tolerance kNearTol, counted by k_seeds and k_near_ties)
+  uint32_t near_rhoc;      // |rho - rhoc| <= tol * rhoc
+  uint32_t near_seed_dc;   // nearest higher found and |delta - seed_dc| <= tol * seed_dc
+  uint32_t near_dm;        // nearest higher found and |delta - dm| <= tol * dm
+  uint32_t nh_near_ties;   // nearest-higher choice compares densities within tol (CLUE_FLAG_NEAR_TIES)
 };
+
+// Relative tolerance of the near-threshold counts: the tolerance rho is held to against FP64.
+constexpr float kNearTol = 1e-5f;
 
 // float -> int32 truncation with x86 cvttss2si semantics (NaN and out-of-range give
 // INT32_MIN), which is what the reference's static_cast<int>(float) does on its

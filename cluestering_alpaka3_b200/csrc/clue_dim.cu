@@ -1008,6 +1008,15 @@ constexpr uint64_t kWaitLimitNs = 1000000000ull;  // 1 s per bulk-copy wait
 // Runs the staged sweep; `vis(inbox, staged_records, first_position, count)` is called for
 // every staged segment of a tile the warp needs.  Returns false if a bulk copy did not
 // complete within the wait limit (the caller reports it and the CTA exits).
+//
+// The give-up decision is made for the whole CTA: every thread waits on the piece's mbarrier
+// with its own time limit, a warp whose lanes did not all see the copy complete skips the
+// piece as a whole (no lane leaves the warp's shuffles and votes), and the barrier that ends
+// the piece is __syncthreads_or of the warps' give-ups, so every thread leaves the loop at the
+// same point and no thread passes a barrier that its siblings do not reach.  Before the CTA
+// returns, the copies it has issued (the timed-out piece and the one issued ahead of it) are
+// waited for once more, again with a time limit: a bulk copy cannot be cancelled, and shared
+// memory must not be released to the next CTA while one may still write into it.
 template <int N, class Visit>
 __device__ bool staged_sweep(const EvGrid* __restrict__ g, const int32_t* __restrict__ off,
                              const float4* __restrict__ rec, StageSmem<N>& sm, const int* lo, const int* hi,
@@ -1054,29 +1063,38 @@ __device__ bool staged_sweep(const EvGrid* __restrict__ g, const int32_t* __rest
   bool done = sm.any_valid == 0;
   if (threadIdx.x == 0) sm.has[0] = build_piece<N>(g, off, rec, sm, it, done, 0) > 0;
   __syncthreads();
-  bool ok = true;
   for (int p = 0; sm.has[p & 1]; ++p) {
     const int b = p & 1;
     if (threadIdx.x == 0) sm.has[b ^ 1] = build_piece<N>(g, off, rec, sm, it, done, b ^ 1) > 0;
-    if (!mbar_wait_bounded(&sm.full[b], (uint32_t)((p >> 1) & 1), kWaitLimitNs)) {
-      ok = false;
-      break;
-    }
-    const int nseg = sm.nseg[b];
-    for (int s = 0; s < nseg; ++s) {
-      bool wneed = warp_valid, inbox = valid;
+    const bool arrived = mbar_wait_bounded(&sm.full[b], (uint32_t)((p >> 1) & 1), kWaitLimitNs);
+    // warp-uniform: a warp visits the piece only if all of its lanes saw the copy complete
+    const bool warp_gave_up = __any_sync(0xffffffffu, !arrived);
+    if (!warp_gave_up) {
+      const int nseg = sm.nseg[b];
+      for (int s = 0; s < nseg; ++s) {
+        bool wneed = warp_valid, inbox = valid;
 #pragma unroll
-      for (int d = 0; d < N; ++d) {
-        const int vd = sm.seg_v[b][s][d];
-        wneed = wneed && vd >= wl[d] && vd <= wh[d];
-        inbox = inbox && vd >= lo[d] && vd <= hi[d];
+        for (int d = 0; d < N; ++d) {
+          const int vd = sm.seg_v[b][s][d];
+          wneed = wneed && vd >= wl[d] && vd <= wh[d];
+          inbox = inbox && vd >= lo[d] && vd <= hi[d];
+        }
+        if (!wneed) continue;
+        vis(inbox, &sm.buf[b][sm.seg_boff[b][s] * W], sm.seg_qb[b][s], sm.seg_cnt[b][s]);
       }
-      if (!wneed) continue;
-      vis(inbox, &sm.buf[b][sm.seg_boff[b][s] * W], sm.seg_qb[b][s], sm.seg_cnt[b][s]);
     }
-    __syncthreads();
+    // CTA-uniform: every thread takes the same branch after this barrier
+    if (__syncthreads_or(warp_gave_up ? 1 : 0)) {
+      // drain what this CTA has issued: piece p (timed out) and piece p + 1 (issued above)
+      if (threadIdx.x == 0) {
+        mbar_wait_bounded(&sm.full[b], (uint32_t)((p >> 1) & 1), kWaitLimitNs);
+        if (sm.has[b ^ 1]) mbar_wait_bounded(&sm.full[b ^ 1], (uint32_t)(((p + 1) >> 1) & 1), kWaitLimitNs);
+      }
+      __syncthreads();
+      return false;
+    }
   }
-  return ok;
+  return true;
 }
 
 // Chunk of the CTA: tile, event grid and home position of this thread.
@@ -1713,13 +1731,17 @@ __global__ void __launch_bounds__(256) k_combine_block_bbox(const KParams kp, Ev
 }
 
 // ---- stage 4: seeds (KernelFindClusters) ---------------------------------------
+// Also counts the near-threshold decisions of this stage: densities within kNearTol of rhoc and
+// nearest-higher distances within kNearTol of seed_dc or dm.
 template <int N, int MT>
 __global__ void __launch_bounds__(256) k_seeds(const KParams kp, int n, const float4* __restrict__ rec_r,
                                                const int32_t* __restrict__ nh_s,
                                                const int32_t* __restrict__ perm, int32_t* __restrict__ is_seed_s,
-                                               int32_t* __restrict__ par, uint32_t* __restrict__ seed_flag) {
+                                               int32_t* __restrict__ par, uint32_t* __restrict__ seed_flag,
+                                               DevStatus* st) {
   using M = Metric<N, MT>;
   const int stride = gridDim.x * blockDim.x;
+  uint32_t c_rhoc = 0, c_seed_dc = 0, c_dm = 0;
   for (int pos = blockIdx.x * blockDim.x + threadIdx.x; pos < n; pos += stride) {
     float x[N], rho, c[N], pl;
     load_rec<N>(rec_r, pos, x, rho);
@@ -1735,7 +1757,79 @@ __global__ void __launch_bounds__(256) k_seeds(const KParams kp, int n, const fl
     is_seed_s[pos] = seed ? 1 : 0;
     par[pos] = seed ? -1 : nh;
     seed_flag[perm[pos]] = seed ? 1u : 0u;
+    c_rhoc += fabsf(rho - kp.rhoc) <= kNearTol * kp.rhoc ? 1u : 0u;
+    c_seed_dc += nh >= 0 && fabsf(dist - kp.seed_dc) <= kNearTol * kp.seed_dc ? 1u : 0u;
+    c_dm += nh >= 0 && fabsf(dist - kp.dm) <= kNearTol * kp.dm ? 1u : 0u;
   }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    c_rhoc += __shfl_xor_sync(0xffffffffu, c_rhoc, o);
+    c_seed_dc += __shfl_xor_sync(0xffffffffu, c_seed_dc, o);
+    c_dm += __shfl_xor_sync(0xffffffffu, c_dm, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    if (c_rhoc) atomicAdd(&st->near_rhoc, c_rhoc);
+    if (c_seed_dc) atomicAdd(&st->near_seed_dc, c_seed_dc);
+    if (c_dm) atomicAdd(&st->near_dm, c_dm);
+  }
+}
+
+// Near-tie count of the nearest-higher stage (CLUE_FLAG_NEAR_TIES), after k_nearest_higher:
+// a point counts when its chosen nearest higher, or a candidate of its search box at most as
+// far as that one (within dm when none was found) that is not its own record, has a density
+// within kNearTol of the point's own.  These are the points whose nearest higher can change
+// when densities move by that much (ClusteringKernels.hpp:129-143).  A pruned sweep like
+// nearest higher's: blocks beyond the chosen distance, or whose densities all lie below
+// rho_i - tol |rho_i|, are skipped.
+template <int N, int MT>
+__global__ void __launch_bounds__(kTileThreads) k_near_ties(
+    const KParams kp, Events ev, const int32_t* __restrict__ off, const int32_t* __restrict__ ord,
+    const int32_t* __restrict__ chunk_tile, const uint32_t* __restrict__ chunk_off,
+    const uint32_t* __restrict__ chunk_total, const float4* __restrict__ rec_r, const float4* __restrict__ rec_m,
+    const int32_t* __restrict__ mq, const float4* __restrict__ blk, const float4* __restrict__ sblk,
+    const int32_t* __restrict__ minv, const int32_t* __restrict__ nh_s, DevStatus* st) {
+  using M = Metric<N, MT>;
+  ChunkHome h;
+  if (!chunk_home(kp, ev, off, ord, chunk_tile, chunk_off, chunk_total, h)) return;
+  const int pos = h.pos;
+  const bool valid = h.valid;
+  float x[N], rho_i;
+  load_rec<N>(rec_r, pos, x, rho_i);
+  int hb[N], lo[N], hi[N];
+  home_bins<N>(h.g, h.t, hb);
+  lane_box<N>(kp, h.g, x, kp.dm, hb, lo, hi);
+  if (!__any_sync(0xffffffffu, valid)) return;
+  __shared__ float4 s_rec[kTileThreads / 32][32 * Rec<N>::kWords];
+  __shared__ int32_t s_q[kTileThreads / 32][32];
+  float4* sm = s_rec[threadIdx.x >> 5];
+  int32_t* sq = s_q[threadIdx.x >> 5];
+  auto near = [&](float r) {
+    const float m = fmaxf(fabsf(r), fabsf(rho_i));
+    return m > 0.0f && fabsf(r - rho_i) <= kNearTol * m;
+  };
+  const int nh = nh_s[pos];
+  float bnd = kp.t_dm;
+  bool flag = false;
+  if (nh >= 0) {
+    float c[N], rho_nh;
+    load_rec<N>(rec_r, nh, c, rho_nh);
+    bnd = M::partial(x, c, kp.mpar);
+    flag = near(rho_nh);
+  }
+  const float pmin = rho_i - kNearTol * fabsf(rho_i);
+  spatial_sweep<N, M, false>(kp, h.g, off, hb, lo, hi, valid, x, blk, sblk, pmin, minv[pos], [&]() { return bnd; },
+                             [&](int p0, int p1, bool need, int64_t) {
+    const int cnt = p1 - p0;
+    stage_block<N>(sm, rec_m, p0, cnt, sq, mq);
+    for (int j = 0; j < cnt; ++j) {
+      float c[N], rj;
+      smem_rec<N>(sm, j, c, rj);
+      const float s = M::partial(x, c, kp.mpar);
+      flag = flag || (need && s <= bnd && sq[j] != pos && near(rj));
+    }
+  });
+  const uint32_t cnt_w = __ballot_sync(0xffffffffu, valid && flag);
+  if ((threadIdx.x & 31) == 0 && cnt_w) atomicAdd(&st->nh_near_ties, (uint32_t)__popc(cnt_w));
 }
 
 // ---- stage 5: labels ---------------------------------------------------------
@@ -1945,7 +2039,13 @@ void launch_density_sym_metric(int metric, const KParams& kp, Workspace& ws, cud
 template <int N, int MT>
 void launch_seeds(const KParams& kp, Workspace& ws, cudaStream_t s) {
   k_seeds<N, MT><<<grid_for(kp.n, 256), 256, 0, s>>>(kp, kp.n, ws.rec_r, ws.nh_s, ws.perm, ws.is_seed_s, ws.par,
-                                                     ws.seed_flag);
+                                                     ws.seed_flag, ws.status);
+}
+template <int N, int MT>
+void launch_near_ties(const KParams& kp, Workspace& ws, cudaStream_t s) {
+  k_near_ties<N, MT><<<chunk_grid(kp), kTileThreads, 0, s>>>(
+      kp, events_of(ws), ws.offsets, ws.mq, ws.chunk_tile, ws.chunk_count, ws.chunk_total, ws.rec_r, ws.rec_m_cur,
+      ws.mq, ws.blk, ws.sblk, ws.minv, ws.nh_s, ws.status);
 }
 
 #define CLUE_METRIC_SWITCH(mt, FN, ...)                                           \
@@ -1976,6 +2076,7 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
   for (int d = 0; d < N; ++d) in.c[d] = a.coords[d];
   in.w = a.weight;
   const Events ev = events_of(ws);
+  ws.near_from_host = false;  // this run's counts land in the device status block
 
   stage_mark(ws, 0, s);
   k_init<N><<<grid_for(kp.n_events, 256), 256, 0, s>>>(kp, ev, ws.ev_pt, ws.ev_tile, ws.status);
@@ -2102,6 +2203,10 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
   }
   k_superblock_bbox<N><<<grid_for(nsb_threads, 256), 256, 0, s>>>(ws.blk, n, ws.sblk);
   CLUE_METRIC_SWITCH(a.metric, launch_nh, kp, ws, s);
+  if (kp.flags & CLUE_FLAG_NEAR_TIES) {
+    CLUE_METRIC_SWITCH(a.metric, launch_near_ties, kp, ws, s);
+    ++launches;
+  }
   stage_mark(ws, 3, s);
   CLUE_METRIC_SWITCH(a.metric, launch_seeds, kp, ws, s);
   exclusive_scan(ws.seed_flag, ws.seed_flag, (size_t)n, ws.scan_scratch, ws.seed_total, s);

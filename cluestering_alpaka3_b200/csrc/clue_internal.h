@@ -155,6 +155,10 @@ struct Workspace {
   uint32_t* sorted_keys = nullptr;
 
   KParams last_kp{};  // parameters of the last enqueued run (for clue_context_read_info)
+  // near-threshold counts summed on the host over the chunks of an overlapped host-memory
+  // batch (near_from_host); every other run leaves them in the device status block
+  bool near_from_host = false;
+  int64_t near_sum[4] = {0, 0, 0, 0};
 
   // optional per-stage timing (clue_context_set_timing)
   bool timing = false;

@@ -1,8 +1,8 @@
 // clue_tma.cuh -- mbarrier + bulk-copy (TMA, non-tensor) helpers for sm_100a.
 //
-// Only the untiled cp.async.bulk global -> shared form is used, without multicast:
-// source and destination are 16-byte aligned and sizes are multiples of 16 bytes
-// (tile-sorted point records are float4 words).  Every wait is bounded in time.
+// Only the untiled cp.async.bulk global -> shared form is used, from this GPU's own memory
+// into this CTA's own shared memory: source and destination are 16-byte aligned and sizes are
+// multiples of 16 bytes (tile-sorted point records are float4 words).  Every wait is bounded in time.
 #pragma once
 
 #include <cstdint>

@@ -7,7 +7,7 @@
 #include <pybind11/pybind11.h>
 
 PYBIND11_MODULE(CLUE_Convolutional_Kernels, m) {
-  m.doc() = "Binding of the convolutional kernels used in the CLUE algorithm.";
+  m.doc() = "FlatKernel, ExponentialKernel and GaussianKernel for the density sums of libclue_b200.";
   pybind11::class_<clue::FlatKernel>(m, "FlatKernel").def(pybind11::init<float>());
   pybind11::class_<clue::ExponentialKernel>(m, "ExponentialKernel").def(pybind11::init<float, float>());
   pybind11::class_<clue::GaussianKernel>(m, "GaussianKernel").def(pybind11::init<float, float, float>());

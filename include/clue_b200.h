@@ -106,6 +106,9 @@ typedef struct clue_params {
  * spatial order that skips far candidate blocks (rho within 1e-5 relative of FP64). */
 #define CLUE_FLAG_REFERENCE_ORDER 1 /* reference order for every kernel */
 #define CLUE_FLAG_SPATIAL_DENSITY 2 /* spatial order for the flat kernel too */
+/* Count the points whose nearest-higher choice compares two densities within the near-threshold
+ * tolerance (clue_near_counts.nh_near_ties).  Costs one extra pruned neighbour sweep. */
+#define CLUE_FLAG_NEAR_TIES 4
 
 /* Output arrays, caller-owned, n elements each, all in the memory space given by
  * `memory` in clue_make_clusters.  Only cluster_index is required. */
@@ -126,6 +129,20 @@ typedef struct clue_run_info {
   int64_t n_per_dim;
   int64_t label_rounds;        /* pointer-jumping rounds that changed a parent */
 } clue_run_info;
+
+/* Decisions of the last run taken on values within a relative tolerance CLUE_NEAR_TOL of their
+ * threshold (ClusteringKernels.hpp:129-143 nearest higher, :232-233 seeds in the reference):
+ * where another summation order or another exp rounds a density differently, these are the
+ * only points whose seed flag or nearest higher can change.  Counted on the device in every
+ * run; nh_near_ties only with CLUE_FLAG_NEAR_TIES (else -1). */
+#define CLUE_NEAR_TOL 1e-5
+typedef struct clue_near_counts {
+  int64_t rho_near_rhoc;      /* |rho - rhoc| <= tol * rhoc */
+  int64_t delta_near_seed_dc; /* nearest higher found and |delta - seed_dc| <= tol * seed_dc */
+  int64_t delta_near_dm;      /* nearest higher found and |delta - dm| <= tol * dm */
+  int64_t nh_near_ties;       /* the chosen nearest higher, or a nearer candidate that is not higher,
+                                 has a density within tol of the point's own; -1: not counted */
+} clue_near_counts;
 
 typedef enum clue_memory { CLUE_MEM_DEVICE = 0, CLUE_MEM_HOST = 1 } clue_memory;
 
@@ -205,6 +222,10 @@ clue_status clue_make_clusters_async(clue_context ctx, const clue_params* params
                                      int32_t ndim, int32_t n, const float* coords,
                                      const float* weight, const clue_outputs* out, void* stream);
 clue_status clue_context_read_info(clue_context ctx, void* stream, clue_run_info* info);
+/* Near-threshold counts of the context's last run (synchronises `stream`, the stream the run
+ * was enqueued on; host-memory batches report the sum over their chunks).  No counterpart in
+ * the reference, which neither counts nor reports these decisions. */
+clue_status clue_context_read_near_counts(clue_context ctx, void* stream, clue_near_counts* counts);
 
 /* Per-stage device timing of the following runs (CUDA events on the run's stream):
  * stage 0 = tile build (bounding box, bins, sort, records), 1 = local density,

@@ -369,6 +369,11 @@ int oracle_nearest_higher(const oracle_params* p, int32_t n, const float* coords
   if (build_tiles(p, n, coords, &g, &off, &idx)) return -2;
   ctx_t c = {p, &g, n, coords, NULL, off, idx};
   int64_t cand = 0, ties = 0;
+  const int nt = p->nthreads > 1 ? p->nthreads : 1;
+  (void)nt;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static) num_threads(nt) reduction(+ : cand, ties)
+#endif
   for (int32_t i = 0; i < n; ++i) {
     float dl;
     nearest_higher[i] = nh_point(&c, rho, i, &dl, &cand, &ties);
@@ -638,4 +643,181 @@ int oracle_silhouette(int32_t ndim, int32_t n, const float* coords, const int32_
   free(idx);
   free(fill);
   return 0;
+}
+
+/* ---- per-event runs (a batch of independent events, OpenMP over events) ----------------
+ * The reference clusters one event per make_clusters call; a caller with many events loops
+ * over them.  These helpers run that loop with one event per thread (each event serial, as
+ * the serial backend computes it), which is the fastest use of the host cores for a batch of
+ * small events.  Event e owns points [offsets[e], offsets[e+1]) of the SoA arrays (stride ld). */
+
+static float* gather_event(const float* coords, int32_t ld, int N, int32_t b, int32_t ne) {
+  float* c = (float*)malloc(sizeof(float) * (size_t)N * (size_t)(ne > 0 ? ne : 1));
+  if (!c) return NULL;
+  for (int d = 0; d < N; ++d) memcpy(c + (size_t)d * ne, coords + (size_t)d * ld + b, sizeof(float) * (size_t)ne);
+  return c;
+}
+
+int oracle_run_events(const oracle_params* p, int32_t n_events, const int32_t* offsets, int32_t ld,
+                      const float* coords, const float* weight, oracle_out* out, int64_t* ev_n_clusters) {
+  const int nt = p->nthreads > 1 ? p->nthreads : 1;
+  (void)nt;
+  int64_t n_seeds = 0, n_clusters = 0, dropped = 0, cand_rho = 0, cand_nh = 0, ties = 0, max_stack = 0;
+  int err = 0;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nt) \
+    reduction(+ : n_seeds, n_clusters, dropped, cand_rho, cand_nh, ties) reduction(max : max_stack) reduction(| : err)
+#endif
+  for (int32_t e = 0; e < n_events; ++e) {
+    const int32_t b = offsets[e], ne = offsets[e + 1] - offsets[e];
+    if (ne <= 0) continue;
+    oracle_params pe = *p;
+    pe.nthreads = 1;
+    float* c = gather_event(coords, ld, p->ndim, b, ne);
+    if (!c) {
+      err |= 1;
+      continue;
+    }
+    oracle_out oe;
+    memset(&oe, 0, sizeof(oe));
+    oe.cluster_index = out->cluster_index + b;
+    oe.is_seed = out->is_seed + b;
+    oe.rho = out->rho + b;
+    oe.nearest_higher = out->nearest_higher + b;
+    oe.delta = out->delta ? out->delta + b : NULL;
+    if (oracle_run(&pe, ne, c, weight + b, &oe) != 0) err |= 1;
+    free(c);
+    for (int32_t i = 0; i < ne; ++i)
+      if (oe.nearest_higher[i] >= 0) oe.nearest_higher[i] += b; /* batch-global index */
+    n_seeds += oe.n_seeds;
+    n_clusters += oe.n_clusters;
+    dropped += oe.dropped_seeds;
+    cand_rho += oe.candidates_rho;
+    cand_nh += oe.candidates_nh;
+    ties += oe.nh_distance_ties;
+    if (oe.max_dfs_stack > max_stack) max_stack = oe.max_dfs_stack;
+    if (ev_n_clusters) ev_n_clusters[e] = oe.n_clusters;
+  }
+  out->n_seeds = n_seeds;
+  out->n_clusters = n_clusters;
+  out->dropped_seeds = dropped;
+  out->seed_capacity_used = -1;
+  out->max_dfs_stack = max_stack;
+  out->candidates_rho = cand_rho;
+  out->candidates_nh = cand_nh;
+  out->nh_distance_ties = ties;
+  return err ? -2 : 0;
+}
+
+/* ---- near-threshold classification ------------------------------------------------------
+ * Two density vectors of the same points -- rho_a from this restatement, rho_b from another
+ * implementation that sums the same terms in another order or with another exp -- agree to a
+ * few ulp.  The nearest-higher and seed stages (ClusteringKernels.hpp:129-143, 232-233) turn
+ * them into discrete decisions, and a decision can differ only where it compares values that
+ * are that close.  oracle_near_flags marks those decision points per point:
+ *   ORACLE_NEAR_RHOC     rho_a and rho_b lie on different sides of rhoc, or |rho_a - rhoc| <= tol*rhoc
+ *   ORACLE_NEAR_FLIP     some candidate j of i's dm search box with d(i, j) <= dm is higher than i
+ *                        under one vector and not under the other (the rule of
+ *                        ClusteringKernels.hpp:129-131)
+ *   ORACLE_NEAR_TIE      some such candidate has |rho_a[j] - rho_a[i]| <= tol * max(|rho_a[i]|, |rho_a[j]|)
+ *   ORACLE_NEAR_SEED_DC  |delta_a - seed_dc| <= tol * seed_dc
+ *   ORACLE_NEAR_DM       |delta_a - dm| <= tol * dm
+ * max_flip_rel (may be NULL) receives the largest |rho_a[j] - rho_a[i]| / max(|rho_a[i]|, |rho_a[j]|)
+ * over the flipped pairs: small when every flip is a genuine near-tie. */
+
+static inline int is_higher(float rho_i, float rho_j, int32_t i, int32_t j) {
+  return (rho_j > rho_i) || ((rho_j == rho_i) && (rho_j > 0.0f) && (j > i));
+}
+
+int oracle_near_flags(const oracle_params* p, int32_t n, const float* coords, const float* rho_a,
+                      const float* rho_b, const float* delta_a, double tol, uint8_t* flags,
+                      double* max_flip_rel) {
+  if (check_params(p, n)) return -1;
+  grid_t g;
+  int32_t *off = NULL, *idx = NULL;
+  if (build_tiles(p, n, coords, &g, &off, &idx)) return -2;
+  const int N = p->ndim;
+  const int nt = p->nthreads > 1 ? p->nthreads : 1;
+  (void)nt;
+  double worst = 0.0;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nt) reduction(max : worst)
+#endif
+  for (int32_t i = 0; i < n; ++i) {
+    float xi[ORACLE_MAX_DIM], xj[ORACLE_MAX_DIM];
+    int32_t lo[ORACLE_MAX_DIM], hi[ORACLE_MAX_DIM];
+    uint8_t f = 0;
+    const float ra = rho_a[i], rb = rho_b[i];
+    if ((ra >= p->rhoc) != (rb >= p->rhoc) || fabs((double)ra - p->rhoc) <= tol * p->rhoc) f |= ORACLE_NEAR_RHOC;
+    if (delta_a) {
+      if (fabs((double)delta_a[i] - p->seed_dc) <= tol * p->seed_dc) f |= ORACLE_NEAR_SEED_DC;
+      if (fabs((double)delta_a[i] - p->dm) <= tol * p->dm) f |= ORACLE_NEAR_DM;
+    }
+    load_point(N, n, coords, i, xi);
+    search_box(&g, xi, p->dm, lo, hi);
+    BOX_LOOP_BEGIN(&g, lo, hi)
+    for (int32_t q = off[tile_]; q < off[tile_ + 1]; ++q) {
+      const int32_t j = idx[q];
+      if (j == i) continue;
+      load_point(N, n, coords, j, xj);
+      if (!(oracle_metric(p, xi, xj) <= p->dm)) continue;
+      const double m = fmax(fabs((double)ra), fabs((double)rho_a[j]));
+      const double gap = fabs((double)rho_a[j] - (double)ra);
+      if (gap <= tol * m) f |= ORACLE_NEAR_TIE;
+      if (is_higher(ra, rho_a[j], i, j) != is_higher(rb, rho_b[j], i, j)) {
+        f |= ORACLE_NEAR_FLIP;
+        const double rel = m > 0.0 ? gap / m : 0.0;
+        if (rel > worst) worst = rel;
+      }
+    }
+    BOX_LOOP_END(&g, lo, hi)
+    flags[i] = f;
+  }
+  if (max_flip_rel) *max_flip_rel = worst;
+  free(off);
+  free(idx);
+  return 0;
+}
+
+/* Per-event forms of the FP64 density, the nearest-higher stage on given densities and the
+ * near-threshold flags (nearest highers returned batch-global). */
+int oracle_events_aux(int kind, const oracle_params* p, int32_t n_events, const int32_t* offsets, int32_t ld,
+                      const float* coords, const float* weight, const float* rho_a, const float* rho_b,
+                      const float* delta_a, double tol, double* rho64, uint8_t* flags, int32_t* nearest_higher,
+                      float* delta, double* max_flip_rel) {
+  const int nt = p->nthreads > 1 ? p->nthreads : 1;
+  (void)nt;
+  int err = 0;
+  double worst = 0.0;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nt) reduction(| : err) reduction(max : worst)
+#endif
+  for (int32_t e = 0; e < n_events; ++e) {
+    const int32_t b = offsets[e], ne = offsets[e + 1] - offsets[e];
+    if (ne <= 0) continue;
+    oracle_params pe = *p;
+    pe.nthreads = 1;
+    float* c = gather_event(coords, ld, p->ndim, b, ne);
+    if (!c) {
+      err |= 1;
+      continue;
+    }
+    int rc = 0;
+    if (kind == ORACLE_AUX_RHO_F64) {
+      rc = oracle_rho_f64(&pe, ne, c, weight + b, rho64 + b, flags ? flags + b : NULL, tol);
+    } else if (kind == ORACLE_AUX_NEAREST_HIGHER) {
+      int64_t t = 0;
+      rc = oracle_nearest_higher(&pe, ne, c, rho_a + b, nearest_higher + b, delta ? delta + b : NULL, &t);
+      for (int32_t i = 0; i < ne && rc == 0; ++i)
+        if (nearest_higher[b + i] >= 0) nearest_higher[b + i] += b;
+    } else {
+      double w = 0.0;
+      rc = oracle_near_flags(&pe, ne, c, rho_a + b, rho_b + b, delta_a ? delta_a + b : NULL, tol, flags + b, &w);
+      if (w > worst) worst = w;
+    }
+    if (rc != 0) err |= 1;
+    free(c);
+  }
+  if (max_flip_rel) *max_flip_rel = worst;
+  return err ? -2 : 0;
 }

@@ -105,6 +105,36 @@ float oracle_metric(const oracle_params* p, const float* a, const float* b);
 /* Convolutional kernel value for a distance, exposed for kernel known-answer tests. */
 float oracle_kernel(const oracle_params* p, float dist, int32_t i, int32_t j);
 
+
+/* Batch of independent events (event e = points [offsets[e], offsets[e+1]) of SoA arrays with
+ * stride ld), one event per OpenMP thread, each event clustered alone as oracle_run does.
+ * out's arrays cover the whole batch; nearest highers are batch-global; stats are summed
+ * (max_dfs_stack: maximum).  ev_n_clusters (may be NULL) receives each event's clusters. */
+int oracle_run_events(const oracle_params* p, int32_t n_events, const int32_t* offsets, int32_t ld,
+                      const float* coords, const float* weight, oracle_out* out, int64_t* ev_n_clusters);
+
+/* Near-threshold decision points of two density vectors of the same points (see
+ * clue_oracle.c).  flags[i] is an OR of the bits below. */
+enum {
+  ORACLE_NEAR_RHOC = 1,
+  ORACLE_NEAR_FLIP = 2,
+  ORACLE_NEAR_TIE = 4,
+  ORACLE_NEAR_SEED_DC = 8,
+  ORACLE_NEAR_DM = 16
+};
+int oracle_near_flags(const oracle_params* p, int32_t n, const float* coords, const float* rho_a,
+                      const float* rho_b, const float* delta_a, double tol, uint8_t* flags,
+                      double* max_flip_rel);
+
+/* Per-event forms (OpenMP over events): kind ORACLE_AUX_RHO_F64 fills rho64 (and the near-dc
+ * flags when flags is not NULL); ORACLE_AUX_NEAREST_HIGHER fills nearest_higher (batch-global)
+ * and delta from the densities rho_a; ORACLE_AUX_NEAR_FLAGS fills flags and max_flip_rel. */
+enum { ORACLE_AUX_RHO_F64 = 0, ORACLE_AUX_NEAREST_HIGHER = 1, ORACLE_AUX_NEAR_FLAGS = 2 };
+int oracle_events_aux(int kind, const oracle_params* p, int32_t n_events, const int32_t* offsets, int32_t ld,
+                      const float* coords, const float* weight, const float* rho_a, const float* rho_b,
+                      const float* delta_a, double tol, double* rho64, uint8_t* flags, int32_t* nearest_higher,
+                      float* delta, double* max_flip_rel);
+
 #ifdef __cplusplus
 }
 #endif

@@ -14,8 +14,30 @@ from dataclasses import dataclass, field
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-_LIB_PATH = os.path.join(_HERE, "_build", "libclue_oracle.so")
 MAX_DIM = 10
+
+
+def _cpu_tag() -> str:
+    """Short tag of this host's CPU: the library is built with -march=native, so each CPU
+    model (and instruction-set flag list) gets its own build directory."""
+    import hashlib
+    import platform
+    model, flags = platform.processor(), ""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name") and model in ("", platform.processor()):
+                    model = line.split(":", 1)[1].strip()
+                elif line.startswith("flags"):
+                    flags = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return hashlib.sha1((model + "|" + flags).encode()).hexdigest()[:12]
+
+
+_BUILD_DIR = os.path.join(_HERE, "_build", _cpu_tag())
+_LIB_PATH = os.path.join(_BUILD_DIR, "libclue_oracle.so")
 
 KERNELS = {"flat": 0, "exp": 1, "gaus": 2}
 METRICS = {"euclidean": 0, "weighted_euclidean": 1, "periodic_euclidean": 2,
@@ -48,8 +70,9 @@ class _Grid(ctypes.Structure):
 
 
 def build() -> str:
-    """Compile the restatement with its Makefile (gcc, -ffp-contract=off)."""
-    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    """Compile the restatement with its Makefile (gcc -O2 -march=native, -ffp-contract=off) into
+    this CPU's build directory."""
+    subprocess.run(["make", "-s", "-C", _HERE, "OUT=" + os.path.relpath(_BUILD_DIR, _HERE)], check=True)
     return _LIB_PATH
 
 
@@ -83,6 +106,19 @@ def _load():
         lib.oracle_kernel.argtypes = [ctypes.POINTER(_Params), ctypes.c_float, ctypes.c_int32,
                                       ctypes.c_int32]
         lib.oracle_kernel.restype = ctypes.c_float
+        lib.oracle_run_events.argtypes = [ctypes.POINTER(_Params), ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32,
+                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(_Out), ctypes.c_void_p]
+        lib.oracle_run_events.restype = ctypes.c_int
+        lib.oracle_near_flags.argtypes = [ctypes.POINTER(_Params), ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p,
+                                          ctypes.POINTER(ctypes.c_double)]
+        lib.oracle_near_flags.restype = ctypes.c_int
+        lib.oracle_events_aux.argtypes = [ctypes.c_int, ctypes.POINTER(_Params), ctypes.c_int32, ctypes.c_void_p,
+                                          ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_double, ctypes.c_void_p,
+                                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                          ctypes.POINTER(ctypes.c_double)]
+        lib.oracle_events_aux.restype = ctypes.c_int
         _lib = lib
     return _lib
 
@@ -271,3 +307,88 @@ def canonicalize(labels: np.ndarray, outlier: int = -1) -> np.ndarray:
     rank[np.argsort(first)] = np.arange(len(uniq), dtype=labels.dtype)
     out[mask] = rank[np.searchsorted(uniq, vals)]
     return out
+
+
+# ---- batches of independent events and near-threshold classification ----------------------
+
+NEAR_RHOC, NEAR_FLIP, NEAR_TIE, NEAR_SEED_DC, NEAR_DM = 1, 2, 4, 8, 16
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+def run_events(coords: np.ndarray, weight: np.ndarray, offsets: np.ndarray, cfg: Config) -> Result:
+    """Every event of a batch clustered alone (as ``run``), one event per OpenMP thread
+    (``cfg.nthreads`` threads).  Nearest highers are batch-global; stats are summed and
+    ``stats["ev_n_clusters"]`` holds each event's clusters."""
+    lib = _load()
+    c = _soa(coords)
+    ndim, n = c.shape
+    w = np.ascontiguousarray(weight, dtype=np.float32)
+    off = np.ascontiguousarray(offsets, dtype=np.int32)
+    E = len(off) - 1
+    res = Result(np.empty(n, np.int32), np.empty(n, np.int32), np.empty(n, np.float32),
+                 np.empty(n, np.int32), np.empty(n, np.float32))
+    out = _Out()
+    out.cluster_index = res.cluster_index.ctypes.data
+    out.is_seed = res.is_seed.ctypes.data
+    out.rho = res.rho.ctypes.data
+    out.nearest_higher = res.nearest_higher.ctypes.data
+    out.delta = res.delta.ctypes.data
+    evc = np.zeros(E, np.int64)
+    p = cfg.to_struct(ndim)
+    rc = lib.oracle_run_events(ctypes.byref(p), E, off.ctypes.data, n, c.ctypes.data, w.ctypes.data,
+                               ctypes.byref(out), evc.ctypes.data)
+    if rc != 0:
+        raise ValueError(f"oracle_run_events failed ({rc})")
+    res.stats = {k: getattr(out, k) for k in ("n_seeds", "n_clusters", "dropped_seeds", "max_dfs_stack",
+                                               "candidates_rho", "candidates_nh", "nh_distance_ties")}
+    res.stats["ev_n_clusters"] = evc
+    return res
+
+
+def _events_aux(kind, coords, offsets, cfg, weight=None, rho_a=None, rho_b=None, delta_a=None, tol=1e-5,
+                want_rho64=False, want_flags=False, want_nh=False):
+    lib = _load()
+    c = _soa(coords)
+    ndim, n = c.shape
+    off = np.ascontiguousarray(offsets, dtype=np.int32)
+    conv = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float32)  # noqa: E731
+    w, ra, rb, da = conv(weight), conv(rho_a), conv(rho_b), conv(delta_a)
+    rho64 = np.empty(n, np.float64) if want_rho64 else None
+    flags = np.zeros(n, np.uint8) if want_flags else None
+    nh = np.empty(n, np.int32) if want_nh else None
+    delta = np.empty(n, np.float32) if want_nh else None
+    worst = ctypes.c_double(0.0)
+    p = cfg.to_struct(ndim)
+    rc = lib.oracle_events_aux(kind, ctypes.byref(p), len(off) - 1, off.ctypes.data, n, c.ctypes.data, _ptr(w),
+                               _ptr(ra), _ptr(rb), _ptr(da), tol, _ptr(rho64), _ptr(flags), _ptr(nh), _ptr(delta),
+                               ctypes.byref(worst))
+    if rc != 0:
+        raise ValueError(f"oracle_events_aux({kind}) failed ({rc})")
+    return rho64, flags, nh, delta, float(worst.value)
+
+
+def rho_f64_events(coords, weight, offsets, cfg: Config, rel_tol: float = 1e-5):
+    """FP64 densities of every event alone, with the near-dc flags: (rho64, near_dc)."""
+    rho64, near, _, _, _ = _events_aux(0, coords, offsets, cfg, weight=weight, tol=rel_tol, want_rho64=True,
+                                       want_flags=True)
+    return rho64, near.astype(bool)
+
+
+def nearest_higher_events(coords, rho, offsets, cfg: Config):
+    """Nearest-higher stage of every event alone on the given densities: (nearest_higher
+    batch-global, delta)."""
+    _, _, nh, delta, _ = _events_aux(1, coords, offsets, cfg, rho_a=rho, want_nh=True)
+    return nh, delta
+
+
+def near_flags(coords, rho_a, rho_b, delta_a, cfg: Config, tol: float = 1e-5, offsets=None):
+    """Near-threshold decision points of two density vectors (NEAR_* bits per point) and the
+    largest relative density gap over the pairs whose higher-relation flipped."""
+    if offsets is None:
+        offsets = np.array([0, _soa(coords).shape[1]], np.int32)
+    _, flags, _, _, worst = _events_aux(2, coords, offsets, cfg, rho_a=rho_a, rho_b=rho_b, delta_a=delta_a,
+                                        tol=tol, want_flags=True)
+    return flags, worst

@@ -3,8 +3,8 @@
 Reads the reference's data/*.csv inputs and data/truth_files/*_truth.csv outputs
 (cluster_ids, is_seed per point) and stores them as compact .npz files, float32
 coordinates parsed like the reference's read_csv (utils/detail/read_csv.hpp:18-49).
-Run from the repository root with the reference checkout at REFERENCE_ROOT
-(default /root/reference):  python tests/golden/make_golden.py
+Run from the repository root with REFERENCE_ROOT naming the reference checkout:
+  REFERENCE_ROOT=<path to CLUEstering_alpaka3> python tests/golden/make_golden.py
 """
 import os
 import sys
@@ -12,7 +12,9 @@ import sys
 import numpy as np
 import pandas as pd
 
-REF = os.environ.get("REFERENCE_ROOT", "/root/reference")
+REF = os.environ.get("REFERENCE_ROOT")
+if not REF:
+    sys.exit("set REFERENCE_ROOT to the reference checkout (the directory holding data/)")
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 # (input csv, truth csv, ndim, parameters used by the reference's own tests for that file)
