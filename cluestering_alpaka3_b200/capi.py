@@ -403,14 +403,6 @@ class Context:
                                          ctypes.c_void_p(weight_ptr), ctypes.byref(out), MEM_DEVICE,
                                          ctypes.c_void_p(stream), ctypes.byref(info)))
             return RunInfo(**{f: getattr(info, f) for f, _ in _RunInfo._fields_})
-
-    def near_counts(self, stream: int = 0) -> dict:
-        """Near-threshold decisions of the last run (relative tolerance NEAR_TOL): densities near
-        rhoc, nearest-higher distances near seed_dc and dm, and (runs with FLAG_NEAR_TIES, else -1)
-        points whose nearest-higher choice compares densities within the tolerance."""
-        c = _NearCounts()
-        check(lib.clue_context_read_near_counts(self.handle, ctypes.c_void_p(stream), ctypes.byref(c)))
-        return {f: int(getattr(c, f)) for f, _ in _NearCounts._fields_}
         check(lib.clue_make_clusters_async(self.handle, ctypes.byref(p), ctypes.byref(k),
                                            ctypes.byref(m), ndim, n, ctypes.c_void_p(coords_ptr),
                                            ctypes.c_void_p(weight_ptr), ctypes.byref(out),
@@ -580,6 +572,14 @@ class Context:
         info = _RunInfo()
         check(lib.clue_context_read_info(self.handle, ctypes.c_void_p(stream), ctypes.byref(info)))
         return RunInfo(**{f: getattr(info, f) for f, _ in _RunInfo._fields_})
+
+    def near_counts(self, stream: int = 0) -> dict:
+        """Near-threshold decisions of the last run (relative tolerance NEAR_TOL): densities near
+        rhoc, nearest-higher distances near seed_dc and dm, and (runs with FLAG_NEAR_TIES, else -1)
+        points whose nearest-higher choice compares densities within the tolerance."""
+        c = _NearCounts()
+        check(lib.clue_context_read_near_counts(self.handle, ctypes.c_void_p(stream), ctypes.byref(c)))
+        return {f: int(getattr(c, f)) for f, _ in _NearCounts._fields_}
 
 
 class Graph:

@@ -1,7 +1,7 @@
 """Batched events: one pass over many events equals clustering every event alone.
 
 Each event is checked against the CPU oracle run on that event alone (bit for bit for the
-flat kernel; within tolerance for the exponential kernel), and the CUDA-graph replay of the
+flat kernel; by the tolerance rule of parity_util.check_tolerant for the exponential kernel), and the CUDA-graph replay of the
 batched pipeline is checked against the direct call.
 """
 import numpy as np
@@ -56,21 +56,14 @@ def test_batch_equals_events_alone_exact(gpu_context, ndim, kernel, params):
 
 
 def test_batch_exponential_kernel_tolerance(gpu_context):
+    import os
+    from parity_util import check_tolerant
     evs, off, coords, weight = make_events(7, 30)
     kw = dict(dc=2.0, rhoc=4.0, dm=3.0, kernel=("exp", (1.0, 1.0)))
     res, ncl = gpu_context.batch_host(coords, weight, off, *gpu_args(**kw))
-    from parity_util import tolerance_report
-    mism, near = 0, 0
-    for e, (c, w) in enumerate(evs):
-        a, b = off[e], off[e + 1]
-        cfg = O.Config(dc=2.0, rhoc=4.0, dm=3.0, kernel="exp", kernel_par=(1.0, 1.0))
-        ref = O.run(c, w, cfg)
-        rep = tolerance_report(res.rho[a:b], ref.rho, c, w, cfg, res.cluster_index[a:b], ref.cluster_index)
-        assert rep["max_rel_far"] <= 1e-5, (e, rep)
-        mism += rep["label_mismatch"]
-        near += rep["near_dc"]
-    print("label mismatches", mism, "points near dc", near)
-    assert mism <= max(2, off[-1] // 1000)
+    cfg = O.Config(dc=2.0, rhoc=4.0, dm=3.0, kernel="exp", kernel_par=(1.0, 1.0), nthreads=os.cpu_count() or 1)
+    rep = check_tolerant(coords, weight, cfg, res, offsets=off, tag="30 events")
+    assert rep["events"] == 30
 
 
 def test_single_event_batch_equals_plain(gpu_context):

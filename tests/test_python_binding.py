@@ -120,9 +120,14 @@ def test_mainrun_exp_gauss_labels(gpu_context, mods, kernel):
     k = K.ExponentialKernel(*kernel[1]) if kernel[0] == "exp" else K.GaussianKernel(*kernel[1])
     res = np.zeros(10000, np.int32)
     B.mainRun(2.0, 4.0, 3.0, 2.0, 128, [0, 0], soa(c, w), res, k, 2, 10000, 256, 0)
-    # rho is summed in a spatial order for these kernels (within 1e-5 of FP64), so a label may
-    # flip only where a density sits on a threshold
-    assert np.mean(res == ref.cluster_index) >= 0.995
+    # mainRun returns labels only: they equal the C ABI run of the same pipeline, whose full
+    # outputs meet the tolerance rule (rho within 1e-5 of FP64, later stages exact on the device's
+    # densities, every label difference from the restatement caused by a near-threshold point)
+    from parity_util import check_tolerant, gpu_args
+    got = gpu_context.make_clusters_host(c, w, *gpu_args(dc=2.0, rhoc=4.0, dm=3.0, kernel=kernel))
+    np.testing.assert_array_equal(res, got.cluster_index)
+    cfg = O.Config(dc=2.0, rhoc=4.0, dm=3.0, kernel=kernel[0], kernel_par=kernel[1], nthreads=os.cpu_count() or 1)
+    check_tolerant(c, w, cfg, got, ref=ref, tag="mainRun " + kernel[0])
 
 
 @pytest.mark.gpu
