@@ -3,20 +3,30 @@
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload NAME]
 
-A step is one pass of the five CLUE stages over one synthetic workload already resident in
-HBM (`value`, device time from CUDA events on the launching stream, L2 flushed between steps
-by writing a 256 MiB buffer).  `e2e` repeats the step through the C ABI with pinned host
-buffers: host->device copy of coordinates and weights, the stages, and device->host copy of
-the labels, seed flags, densities, nearest highers and deltas, all inside the timed region.
-Under torchrun every rank clusters its own replica of the workload (seeded by rank, no
-collective on the data path, scaling "weak"); the step time is the max over ranks.
+A step is one replay of the CUDA graph of the whole batched pipeline (bounding boxes, tile
+sort, local density, nearest higher, seeds, labels, output scatter) over this rank's events,
+already resident in HBM (`value`: device time from CUDA events on the launching stream, L2
+flushed between steps by writing a 256 MiB buffer).  `e2e` repeats the step through the C ABI
+(clue_batch_make_clusters) with pinned host buffers: the host->device copy of coordinates and
+weights, the pipeline, and the device->host copy of the labels and seed flags (what the
+reference's make_clusters hands back to the caller), all inside the timed region.
 
---impl reference times the CPU restatement of the reference's serial path (OpenMP over points,
-all host cores) on the same workload, on rank 0 only.
+Under torchrun the workload is 4096 calorimeter events per rank (block b of 4096 events is
+generated with seed 4000 + b, so block 0 is the single-GPU workload); the events of all blocks
+are partitioned over the ranks by size (sharding.partition_events), every rank clusters its
+share with no collective on the data path ("scaling": "weak"), the step time is the max over
+ranks, and rank 0 gathers the per-event cluster counts (sharding.gather_event_results) and
+prints a checksum of block 0's events, comparable between runs on any number of GPUs.
+
+--impl reference times the CPU restatement of the reference's serial path (oracle/, the
+reference itself cannot be built: its alpaka3 dependency is fetched over the network) on a
+bounded sample of the same workload, with all host cores, on rank 0 only.  It emits the same
+`config` object as the GPU arm.
 """
 from __future__ import annotations
 
 import argparse
+import hashlib
 import json
 import os
 import statistics
@@ -31,6 +41,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "points/sec batched vs plain launch on 1 B200; p50/p99 event latency"
+EVENTS_PER_GPU = 4096
+CPU_SAMPLE_STRIDE = 8      # cpu baseline / reference arm: every 8th event of block 0 (512 events)
+SERIAL_SAMPLE_STRIDE = 64  # serial restatement: every 64th event of block 0 (64 events)
 
 
 def load_peaks():
@@ -43,29 +56,69 @@ def load_peaks():
 
 
 class Events:
-    """A batched workload: events concatenated into one SoA buffer with offsets."""
+    """A batched workload: events concatenated into one SoA buffer with offsets.  `ids` are the
+    events' numbers in the whole job (block b holds ids [4096 b, 4096 (b + 1)))."""
 
-    def __init__(self, name, events, dc, rhoc, dm, kernel):
+    def __init__(self, name, events, dc, rhoc, dm, kernel, ids=None):
         self.name = name
         self.events = events
+        self.ids = np.arange(len(events)) if ids is None else np.asarray(ids)
         self.offsets = np.concatenate([[0], np.cumsum([e[0].shape[1] for e in events])]).astype(np.int32)
         self.coords = np.ascontiguousarray(np.concatenate([e[0] for e in events], axis=1))
         self.weight = np.ascontiguousarray(np.concatenate([e[1] for e in events]))
         self.dc, self.rhoc, self.dm, self.kernel = dc, rhoc, dm, kernel
 
+    def subset(self, ids):
+        ids = np.asarray(ids)
+        return Events(self.name, [self.events[i] for i in ids], self.dc, self.rhoc, self.dm, self.kernel,
+                      self.ids[ids])
 
-def make_workload(name: str, rank: int):
+
+def make_workload(name: str, world: int):
+    """The whole job's workload (every rank builds the same one)."""
     from cluestering_alpaka3_b200 import synthetic
     if name == "calo4096":
-        evs, p = synthetic.calo_events(4096, seed=4000 + rank)
+        evs, p = [], None
+        for b in range(world):
+            blk, p = synthetic.calo_events(EVENTS_PER_GPU, seed=4000 + b)
+            evs.extend(blk)
         return Events("calo4096", evs, p["dc"], p["rhoc"], p["dm"], p["kernel"])
     if name == "blobs2d_1m":
-        return synthetic.blobs_2d_1m(seed=2000 + rank)
+        return synthetic.blobs_2d_1m()
     if name == "blobs2d_16k":
-        return synthetic.blobs_2d_16k(seed=1000 + rank)
+        return synthetic.blobs_2d_16k()
     if name == "blobs3d_4m":
-        return synthetic.blobs_3d_4m(seed=3000 + rank)
+        return synthetic.blobs_3d_4m()
     raise SystemExit(f"unknown workload {name}")
+
+
+def rank_share(wl, world: int, rank: int):
+    """This rank's part: its events of a batched workload (partitioned by size), or a replica
+    of a single-event workload."""
+    if not isinstance(wl, Events) or world == 1:
+        return wl
+    from cluestering_alpaka3_b200.sharding import partition_events
+    sizes = np.diff(wl.offsets)
+    return wl.subset(partition_events(sizes, world)[rank])
+
+
+def workload_config(wl, world: int) -> dict:
+    """The `config` object of both arms: the workload and how it is run, nothing measured."""
+    ndim, n = wl.coords.shape
+    kname, kpar = wl.kernel
+    cfg = {"workload": wl.name, "n_points": int(n), "ndim": int(ndim), "dc": wl.dc, "rhoc": wl.rhoc, "dm": wl.dm,
+           "kernel": [kname, list(kpar)], "metric": "euclidean", "points_per_tile": 128,
+           "l2": "flushed between steps (256 MiB write)"}
+    if isinstance(wl, Events):
+        cfg.update({"n_events": len(wl.events), "events_per_gpu": EVENTS_PER_GPU,
+                    "event_sizes": "lognormal(median 2000, sigma 1) clipped to [100, 60000]",
+                    "seeds": f"4000 + block, {world} block(s) of {EVENTS_PER_GPU} events",
+                    "parallelism": "single" if world == 1 else f"events sharded over {world} ranks",
+                    "step": "one CUDA-graph replay of the batched pipeline over the rank's events"})
+    else:
+        cfg.update({"n_events": 1, "parallelism": "single" if world == 1 else f"{world} replicas",
+                    "step": "one CUDA-graph replay of the pipeline over the whole input"})
+    return cfg
 
 
 class Clocks:
@@ -108,61 +161,258 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-CPU_SAMPLE_EVENTS = 512
+# ---- CPU restatement (baseline / reference arm) ---------------------------------------------
+
+def cpu_sample(wl, stride: int):
+    """A bounded sample of the workload: every `stride`-th event of block 0 (batched workloads;
+    sizes follow the same distribution), or the whole input (single-event workloads)."""
+    if not isinstance(wl, Events):
+        return wl
+    ids = np.nonzero((wl.ids < EVENTS_PER_GPU) & (wl.ids % stride == 0))[0]
+    return wl.subset(ids)
 
 
-def cpu_baseline_run(wl, nthreads: int):
-    """The CPU restatement on the workload (batched workloads: its first CPU_SAMPLE_EVENTS
-    events, each clustered alone).  Returns (seconds, points, last result)."""
+def run_cpu(sample, mode: str, threads: int):
+    """One pass of the restatement over the sample; returns (seconds, points).  mode "events":
+    events in parallel, one per thread, each clustered serially; "points": events one after the
+    other, OpenMP over the points of each (the reference's OpenMP backend runs one make_clusters
+    call that way); "serial": one thread."""
     from oracle import oracle as O
-    kname, kpar = wl.kernel
-    cfg = O.Config(dc=wl.dc, rhoc=wl.rhoc, dm=wl.dm, kernel=kname, kernel_par=kpar, nthreads=nthreads)
-    if isinstance(wl, Events):
-        pts, r = 0, None
-        t0 = time.perf_counter()
-        for c, w in wl.events[:CPU_SAMPLE_EVENTS]:
-            r = O.run(c, w, cfg)
-            pts += c.shape[1]
-        return time.perf_counter() - t0, pts, r
+    kname, kpar = sample.kernel
+    nt = 1 if mode == "serial" else threads
+    cfg = O.Config(dc=sample.dc, rhoc=sample.rhoc, dm=sample.dm, kernel=kname, kernel_par=kpar, nthreads=nt)
+    c, w = sample.coords, sample.weight
+    off = sample.offsets if isinstance(sample, Events) else np.array([0, c.shape[1]], np.int32)
     t0 = time.perf_counter()
-    r = O.run(wl.coords, wl.weight, cfg)
-    return time.perf_counter() - t0, wl.coords.shape[1], r
+    if mode == "points":
+        for e in range(len(off) - 1):
+            O.run(c[:, off[e]:off[e + 1]], w[off[e]:off[e + 1]], cfg)
+    else:
+        O.run_events(c, w, off, cfg)
+    return time.perf_counter() - t0, int(off[-1])
 
 
-def sample_text(wl) -> str:
-    if isinstance(wl, Events):
-        n = int(wl.offsets[min(CPU_SAMPLE_EVENTS, len(wl.events))])
-        return f"first {CPU_SAMPLE_EVENTS} of {len(wl.events)} {wl.name} events ({n} points), each clustered alone"
-    return f"full {wl.name} workload ({wl.coords.shape[1]} points)"
+def sample_text(sample, stride: int) -> str:
+    if isinstance(sample, Events):
+        return (f"every {stride}th of the first {EVENTS_PER_GPU} {sample.name} events "
+                f"({len(sample.events)} events, {int(sample.offsets[-1])} points), each clustered alone")
+    return f"the whole {sample.name} input ({sample.coords.shape[1]} points)"
 
 
-def reference_arm(args, rank: int):
-    """The reference's path restated in C (the reference itself cannot be built: its alpaka3
-    dependency is fetched over the network), timed on the host cores."""
+def cpu_modes(sample) -> tuple:
+    return ("events", "points") if isinstance(sample, Events) and len(sample.events) > 1 else ("points",)
+
+
+def reference_arm(args, rank: int, world: int):
+    """The reference's path restated in C, timed on the host cores of rank 0 (other ranks exit)."""
     if rank != 0:
         return
     from oracle import oracle as O
     O.build()
-    wl = make_workload(args.workload, 0)
-    n = wl.coords.shape[1]
+    wl = make_workload(args.workload, world)
+    sample = cpu_sample(wl, CPU_SAMPLE_STRIDE)
     cores = os.cpu_count() or 1
-    cpu_baseline_run(wl, cores)
+    # warm-up: each parallel form once, then the faster one
+    tried = {m: run_cpu(sample, m, cores)[0] for m in cpu_modes(sample)}
+    mode = min(tried, key=tried.get)
+    for _ in range(max(0, args.warmup - len(tried))):
+        run_cpu(sample, mode, cores)
     times, pts = [], 0
     for _ in range(args.steps):
-        dt, pts, _ = cpu_baseline_run(wl, cores)
+        dt, pts = run_cpu(sample, mode, cores)
         times.append(dt)
     tot = sum(times)
     v = pts * len(times) / tot
-    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "points/s", "n_gpus": args.gpus,
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "points/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic",
-            "config": {"workload": wl.name, "n_points": n, "ndim": wl.coords.shape[0], "dc": wl.dc,
-                       "rhoc": wl.rhoc, "dm": wl.dm, "kernel": list(wl.kernel)},
+            "data": "synthetic", "config": workload_config(wl, world),
             "cpu_baseline": {"value": v, "unit": "points/s", "cores": cores, "kind": "port",
-                             "sample": sample_text(wl) + " per step, OpenMP over points"},
+                             "sample": sample_text(sample, CPU_SAMPLE_STRIDE) + f" per step; {mode}-parallel "
+                                       f"(faster in warm-up: {', '.join(f'{m} {1e3 * t:.0f} ms' for m, t in tried.items())})",
+                             "build": "gcc -O2 -march=native -ffp-contract=off -fopenmp"},
             "e2e": {"value": v, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(wl, cores: int) -> dict:
+    """The restatement on this host's cores beside the GPU numbers: both parallel forms on the
+    bounded sample (value = the faster) and the serial restatement on a smaller one."""
+    sample = cpu_sample(wl, CPU_SAMPLE_STRIDE)
+    forms = {}
+    for m in cpu_modes(sample):
+        dt, pts = run_cpu(sample, m, cores)
+        forms[m] = pts / dt
+    best = max(forms, key=forms.get)
+    out = {"value": forms[best], "unit": "points/s", "cores": cores, "kind": "port",
+           "sample": sample_text(sample, CPU_SAMPLE_STRIDE) + f"; {best}-parallel",
+           "forms_points_per_s": forms, "build": "gcc -O2 -march=native -ffp-contract=off -fopenmp"}
+    if isinstance(wl, Events):
+        ssample = cpu_sample(wl, SERIAL_SAMPLE_STRIDE)
+        dt, pts = run_cpu(ssample, "serial", 1)
+        out["serial"] = {"value": pts / dt, "unit": "points/s", "cores": 1,
+                         "sample": sample_text(ssample, SERIAL_SAMPLE_STRIDE)}
+    return out
+
+
+# ---- GPU arm ----------------------------------------------------------------------------------
+
+class DeviceRun:
+    """One workload resident on this rank's GPU: inputs, outputs, and the captured graph of the
+    batched pipeline (a single-event workload is a batch of one event, the plain path)."""
+
+    def __init__(self, capi, torch, ctx, wl, stream, dev):
+        self.wl = wl
+        self.ctx, self.stream, self.sp = ctx, stream, stream.cuda_stream
+        self.ndim, self.n = wl.coords.shape
+        self.offsets = wl.offsets if isinstance(wl, Events) else np.array([0, self.n], np.int32)
+        self.E = len(self.offsets) - 1
+        kname, kpar = wl.kernel
+        self.kernel = {"flat": capi.FlatKernel, "exp": capi.ExponentialKernel, "gaus": capi.GaussianKernel}[kname](*kpar)
+        self.params = capi.Params(dc=wl.dc, rhoc=wl.rhoc, dm=wl.dm)
+        self.metric = capi.Metric()
+        self.dcoords = torch.from_numpy(wl.coords).to(dev)
+        self.dweight = torch.from_numpy(wl.weight).to(dev)
+        self.outs = {k: torch.empty(self.n, dtype=dt, device=dev) for k, dt in
+                     (("cluster_index", torch.int32), ("is_seed", torch.int32), ("rho", torch.float32),
+                      ("nearest_higher", torch.int32), ("delta", torch.float32))}
+        self.optr = {k: v.data_ptr() for k, v in self.outs.items()}
+        self.ncl = torch.zeros(self.E, dtype=torch.int32, device=dev)
+        self.graph = ctx.capture_batch(self.dcoords.data_ptr(), self.dweight.data_ptr(), self.ndim, self.offsets,
+                                       self.optr, self.params, self.kernel, self.metric,
+                                       ncl_ptr=self.ncl.data_ptr(), stream=self.sp)
+
+    def direct(self, params=None):
+        """The same pipeline enqueued directly (not from the graph)."""
+        self.ctx.batch_device(self.dcoords.data_ptr(), self.dweight.data_ptr(), self.ndim, self.offsets, self.optr,
+                              params or self.params, self.kernel, self.metric, ncl_ptr=self.ncl.data_ptr(),
+                              stream=self.sp, blocking=False)
+
+    def close(self):
+        self.graph.close()
+
+
+def time_replays(torch, run: DeviceRun, flush, steps: int, warmup: int):
+    """Per-step device ms of `steps` graph replays (after `warmup`), L2 flushed before each."""
+    for _ in range(warmup):
+        run.graph.launch(run.sp)
+    torch.cuda.synchronize()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    for k in range(steps):
+        with torch.cuda.stream(run.stream):
+            flush.zero_()
+            starts[k].record(run.stream)
+        run.graph.launch(run.sp)
+        with torch.cuda.stream(run.stream):
+            ends[k].record(run.stream)
+    torch.cuda.synchronize()
+    return [s.elapsed_time(e) for s, e in zip(starts, ends)]
+
+
+def stage_times(torch, run: DeviceRun, flush, reps: int = 3) -> np.ndarray:
+    """Mean per-stage device ms (tiles, density, nearest higher, seeds + labels) of direct runs."""
+    run.ctx.set_timing(True)
+    acc = np.zeros(4)
+    for _ in range(reps):
+        with torch.cuda.stream(run.stream):
+            flush.zero_()
+        run.direct()
+        acc += np.array(run.ctx.stage_times())
+    run.ctx.set_timing(False)
+    return acc / reps
+
+
+def near_counts(run: DeviceRun, capi) -> dict:
+    """Near-threshold counts of one direct run with the near-tie count enabled (outside timing)."""
+    import dataclasses
+    run.direct(dataclasses.replace(run.params, flags=capi.FLAG_NEAR_TIES))
+    c = run.ctx.near_counts(run.sp)
+    c["tolerance"] = capi.NEAR_TOL
+    return c
+
+
+def e2e_host(torch, run: DeviceRun, steps: int) -> tuple:
+    """Wall ms per step of the batch through the C ABI from pinned host memory (inputs copied
+    in, labels and seed flags copied back), and the bytes copied each way per step."""
+    wl, n, E = run.wl, run.n, run.E
+    hc = torch.from_numpy(wl.coords).pin_memory().numpy()
+    hw = torch.from_numpy(wl.weight).pin_memory().numpy()
+    hout = {k: torch.empty(n, dtype=torch.int32).pin_memory().numpy() for k in ("cluster_index", "is_seed")}
+    hncl = torch.empty(E, dtype=torch.int32).pin_memory().numpy()
+    for _ in range(2):
+        run.ctx.batch_host(hc, hw, run.offsets, run.params, run.kernel, run.metric, stream=run.sp, out=hout, ncl=hncl)
+    ms = []
+    for _ in range(steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        run.ctx.batch_host(hc, hw, run.offsets, run.params, run.kernel, run.metric, stream=run.sp, out=hout, ncl=hncl)
+        ms.append(1e3 * (time.perf_counter() - t0))
+    h2d = int(n * (run.ndim + 1) * 4 + 276 * E + 8)  # coordinates, weights, event table (276 B per event)
+    d2h = int(n * 2 * 4 + 4 * E)                     # labels, seed flags, clusters per event
+    return ms, h2d, d2h
+
+
+def plain_block(capi, torch, local: int, dev, flush, peak: float, steps: int, warmup: int) -> dict:
+    """The plain single-event path on the two large single-instance configurations: 1M 2-D points
+    with the flat kernel and 4M 3-D points with the Gaussian kernel, one graph replay per step."""
+    from cluestering_alpaka3_b200 import bytes_model
+    out = {}
+    ctx = capi.Context(local)
+    stream = torch.cuda.Stream(device=local)
+    try:
+        for name in ("blobs2d_1m", "blobs3d_4m"):
+            wl = make_workload(name, 1)
+            run = DeviceRun(capi, torch, ctx, wl, stream, dev)
+            try:
+                ms = time_replays(torch, run, flush, steps, warmup)
+                st = stage_times(torch, run, flush)
+                e2e_ms, h2d, d2h = e2e_host(torch, run, max(3, steps // 4))
+                nc = near_counts(run, capi)
+                ncl = int(run.ncl.sum().item())
+            finally:
+                run.close()
+            B = bytes_model.algorithmic_bytes(wl.coords, wl.dc, wl.dm)
+            t = float(np.mean(ms))
+            n = wl.coords.shape[1]
+            out[name] = {
+                "n_points": n, "ndim": wl.coords.shape[0], "kernel": [wl.kernel[0], list(wl.kernel[1])],
+                "dc": wl.dc, "rhoc": wl.rhoc, "dm": wl.dm, "n_clusters": ncl,
+                "device_ms": t, "points_per_s": n / (t / 1e3),
+                "e2e": {"points_per_s": n / (float(np.mean(e2e_ms)) / 1e3), "h2d_bytes": h2d, "d2h_bytes": d2h},
+                "stage_ms": dict(zip(("tiles", "density", "nearest_higher", "seeds_labels"), map(float, st))),
+                "b_alg": B["total"], "b_alg_term1": B["term1"],
+                "pipeline_hbm_frac": B["total"] / (t / 1e3) / 1e9 / peak,
+                "density_hbm_frac": B["density_kernel"] / (st[1] / 1e3) / 1e9 / peak,
+                "nearest_higher_hbm_frac": B["nearest_higher_kernel"] / (st[2] / 1e3) / 1e9 / peak,
+                "near_threshold": nc}
+    finally:
+        ctx.close()
+    return out
+
+
+def serving_block():
+    from cluestering_alpaka3_b200 import serve_bench
+    pc, pw, po, _ = serve_bench.make_pool(512)
+    srv = serve_bench.make_server(slots=3, budget_gb=6.0)
+    try:
+        serve_bench.run_rate(srv, pc, pw, po, 2000.0, 0.3, seed=99)  # warm-up
+        rates = [serve_bench.run_rate(srv, pc, pw, po, r, 2.0, seed=1000 + i)
+                 for i, r in enumerate((5000.0, 20000.0, 50000.0))]
+    finally:
+        srv.close()
+    return {"workload": "Poisson stream of 4-D events (lognormal sizes, median 2000, clipped [100, 200000]), "
+                        "dc=2.5 rhoc=6 dm=2.5 FlatKernel(0.5), 3 slots, 6 GiB device budget",
+            "rates": [{k: r[k] for k in ("offered_events_per_s", "p50_ms", "p99_ms", "points_per_s",
+                                         "achieved_events_per_s", "events_per_batch", "refused")} for r in rates]}
+
+
+def events_checksum(per_event: dict) -> dict:
+    """Checksum of the per-event cluster counts of block 0 (event ids below EVENTS_PER_GPU)."""
+    ids = sorted(e for e in per_event if e < EVENTS_PER_GPU)
+    arr = np.array([per_event[e] for e in ids], np.int32)
+    return {"events": len(ids), "clusters": int(arr.sum()),
+            "sha1_16": hashlib.sha1(np.ascontiguousarray(arr).tobytes()).hexdigest()[:16]}
 
 
 def main():
@@ -171,10 +421,10 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="calo4096",
-                    choices=["calo4096", "blobs2d_16k", "blobs2d_1m", "blobs3d_4m"])
+    ap.add_argument("--workload", default="calo4096", choices=["calo4096", "blobs2d_16k", "blobs2d_1m", "blobs3d_4m"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -182,7 +432,7 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
 
     if args.impl == "reference":
-        reference_arm(args, rank)
+        reference_arm(args, rank, world)
         return
 
     import torch
@@ -194,128 +444,78 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
 
     from cluestering_alpaka3_b200 import bytes_model, capi
+    from cluestering_alpaka3_b200.sharding import gather_event_results
 
-    wl = make_workload(args.workload, rank)
+    wl_all = make_workload(args.workload, world)
+    wl = rank_share(wl_all, world, rank)
     batched = isinstance(wl, Events)
-    ndim, n = wl.coords.shape
     dev = f"cuda:{local}"
-    kname, kpar = wl.kernel
-    kernel = {"flat": capi.FlatKernel, "exp": capi.ExponentialKernel, "gaus": capi.GaussianKernel}[kname](*kpar)
-    params = capi.Params(dc=wl.dc, rhoc=wl.rhoc, dm=wl.dm)
-    metric = capi.Metric()
-
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     ctx = capi.Context(local)
     stream = torch.cuda.Stream(device=local)
-    sp = stream.cuda_stream
-    dcoords = torch.from_numpy(wl.coords).to(dev)
-    dweight = torch.from_numpy(wl.weight).to(dev)
-    outs = {k: torch.empty(n, dtype=dt, device=dev) for k, dt in
-            (("cluster_index", torch.int32), ("is_seed", torch.int32), ("rho", torch.float32),
-             ("nearest_higher", torch.int32), ("delta", torch.float32))}
-    optr = {k: v.data_ptr() for k, v in outs.items()}
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
-    E = len(wl.offsets) - 1 if batched else 1
-    offsets = wl.offsets if batched else np.array([0, n], np.int32)
-    ncl = torch.zeros(E, dtype=torch.int32, device=dev)
+    run = DeviceRun(capi, torch, ctx, wl, stream, dev)
+    n, E = run.n, run.E
 
-    # the step: one replay of the whole pipeline captured in a CUDA graph
-    graph = ctx.capture_batch(dcoords.data_ptr(), dweight.data_ptr(), ndim, offsets, optr, params, kernel, metric,
-                              ncl_ptr=ncl.data_ptr(), stream=sp)
-
-    def step():
-        graph.launch(sp)
-
-    torch.cuda.synchronize()
+    # ---- timed device-resident steps: one graph replay each ---------------------------------
     for _ in range(args.warmup):
-        step()
+        run.graph.launch(run.sp)
     torch.cuda.synchronize()
-
-    # ---- timed device-resident steps --------------------------------------
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
     launches0 = ctx.kernel_launches
     clocks = Clocks(local)
-    for k in range(args.steps):
-        with torch.cuda.stream(stream):
-            flush.zero_()
-            starts[k].record(stream)
-        step()
-        with torch.cuda.stream(stream):
-            ends[k].record(stream)
-    torch.cuda.synchronize()
+    ms = time_replays(torch, run, flush, args.steps, 0)
     clk = clocks.stop()
-    ms = [s_.elapsed_time(e_) for s_, e_ in zip(starts, ends)]
     total_ms = float(sum(ms))
+    job_points = int(wl_all.coords.shape[1]) if batched else world * n
     if world > 1:
         t = torch.tensor([total_ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
         dist.barrier()
-    value = world * n * args.steps / (total_ms / 1e3)
-    n_clusters = int(ncl.sum().item())
+    value = job_points * args.steps / (total_ms / 1e3)
+    ev_ncl = run.ncl.cpu().numpy()
 
-    # launches per graph replay = the launches the capture enqueued
-    ctx.batch_device(dcoords.data_ptr(), dweight.data_ptr(), ndim, offsets, optr, params, kernel, metric,
-                     stream=sp, blocking=False)
-    per_step_launches = ctx.kernel_launches - launches0
-    launches = per_step_launches * args.steps
+    # launches per replay = the launches the capture enqueued (one direct run counts them)
+    run.direct()
+    torch.cuda.synchronize()
+    launches = (ctx.kernel_launches - launches0) * args.steps
+    stage_avg = stage_times(torch, run, flush)
+    near = near_counts(run, capi)
 
-    # ---- per-stage device times of the same pipeline (events around stages) ------
-    ctx.set_timing(True)
-    stage_ms = np.zeros(4)
-    for _ in range(3):
-        with torch.cuda.stream(stream):
-            flush.zero_()
-        ctx.batch_device(dcoords.data_ptr(), dweight.data_ptr(), ndim, offsets, optr, params, kernel, metric,
-                         stream=sp, blocking=False)
-        stage_ms += np.array(ctx.stage_times())
-    ctx.set_timing(False)
-    stage_avg = stage_ms / 3
+    # ---- per-event results gathered on rank 0 (comparable at every N) ------------------------
+    local_res = {int(i): int(c) for i, c in zip(wl.ids, ev_ncl)} if batched else {0: int(ev_ncl.sum())}
+    merged = gather_event_results(local_res, world, rank) if batched else local_res
+    checksum = events_checksum(merged) if (batched and rank == 0) else None
 
-    # ---- the plain per-event launch loop on the same events -----------------------
-    plain = None
+    # ---- the plain per-event launch loop on the same events ---------------------------------
+    plain_loop = None
     if batched:
         torch.cuda.synchronize()
-        ev_ms = ctx.events_loop(dcoords.data_ptr(), dweight.data_ptr(), ndim, offsets, optr, params, kernel,
-                                metric, stream=sp, event_times=True)
-        ev_ms = ctx.events_loop(dcoords.data_ptr(), dweight.data_ptr(), ndim, offsets, optr, params, kernel,
-                                metric, stream=sp, event_times=True)
+        for _ in range(2):
+            ev_ms = ctx.events_loop(run.dcoords.data_ptr(), run.dweight.data_ptr(), run.ndim, run.offsets, run.optr,
+                                    run.params, run.kernel, run.metric, stream=run.sp, event_times=True)
         loop_ms = float(ev_ms.sum())
-        plain = {"points_per_s": n / (loop_ms / 1e3), "ms_per_pass": loop_ms,
-                 "event_latency_ms": {"p50": float(np.percentile(ev_ms, 50)),
-                                      "p99": float(np.percentile(ev_ms, 99))}}
+        plain_loop = {"points_per_s": n / (loop_ms / 1e3), "ms_per_pass": loop_ms,
+                      "event_latency_ms": {"p50": float(np.percentile(ev_ms, 50)),
+                                           "p99": float(np.percentile(ev_ms, 99))}}
 
-    # ---- end to end through the C ABI with pinned host buffers ----------------
-    # inputs and the step's result (labels and seed flags, as the reference's make_clusters
-    # returns them) live in pinned host memory; densities and nearest highers stay on the device
-    hc = torch.from_numpy(wl.coords).pin_memory().numpy()
-    hw = torch.from_numpy(wl.weight).pin_memory().numpy()
-    hout = {k: torch.empty(n, dtype=torch.int32).pin_memory().numpy() for k in ("cluster_index", "is_seed")}
-    hncl_buf = torch.empty(E, dtype=torch.int32).pin_memory().numpy()
-    for _ in range(2):
-        res, hncl = ctx.batch_host(hc, hw, offsets, params, kernel, metric, stream=sp, out=hout, ncl=hncl_buf)
-    e2e_ms = []
-    for _ in range(args.steps):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        res, hncl = ctx.batch_host(hc, hw, offsets, params, kernel, metric, stream=sp, out=hout, ncl=hncl_buf)
-        e2e_ms.append(1e3 * (time.perf_counter() - t0))
+    # ---- end to end through the C ABI with pinned host buffers -------------------------------
+    e2e_ms, h2d, d2h = e2e_host(torch, run, args.steps)
     e2e_total = float(sum(e2e_ms))
     if world > 1:
         t = torch.tensor([e2e_total], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_total = float(t.item())
+    run.close()
 
-    # ---- roofline of the dominant kernel (local density) ------------------------
+    # ---- roofline of the dominant kernel (local density) -------------------------------------
     peak, peak_kind = load_peaks()
-    B = bytes_model.algorithmic_bytes(wl.coords, wl.dc, wl.dm, offsets)
+    B = bytes_model.algorithmic_bytes(wl.coords, wl.dc, wl.dm, run.offsets)
     dens_ms = float(stage_avg[1])
     achieved = B["density_kernel"] / (dens_ms / 1e3) / 1e9
-    traffic = None
-    issue = None  # the sweeps' real bound: instruction issue and the MUFU (XU) pipe, from ncu
+    traffic, issue = None, None
     tfile = os.path.join(ROOT, "profiles", f"traffic_{wl.name}.json")
     if os.path.exists(tfile):
         with open(tfile) as f:
@@ -327,65 +527,40 @@ def main():
                      "nearest_higher_issue_active_frac": tj.get("nearest_higher_issue_active"),
                      "source": tj.get("source")}
 
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cores = os.cpu_count() or 1
-        dt, pts, ref = cpu_baseline_run(wl, cores)
-        cpu = {"value": pts / dt, "unit": "points/s", "cores": cores, "kind": "port",
-               "sample": sample_text(wl) + ", OpenMP over points"}
-        if not batched:
-            cpu["labels_equal_to_gpu"] = bool(np.array_equal(ref.cluster_index, res.cluster_index))
-
-    # ---- serving: Poisson stream of 4-D events through the continuous-batching server ----
-    serving = None
-    if rank == 0 and world == 1 and not args.no_serving:
-        from cluestering_alpaka3_b200 import serve_bench
-        pc, pw, po, _ = serve_bench.make_pool(512)
-        srv = serve_bench.make_server(slots=3, budget_gb=6.0)
-        try:
-            serve_bench.run_rate(srv, pc, pw, po, 2000.0, 0.3, seed=99)  # warm-up
-            serving = [serve_bench.run_rate(srv, pc, pw, po, r, 2.0, seed=1000 + i)
-                       for i, r in enumerate((5000.0, 20000.0, 50000.0))]
-        finally:
-            srv.close()
+    solo = rank == 0 and world == 1
+    cpu = cpu_baseline(wl, os.cpu_count() or 1) if solo and not args.no_cpu_baseline else None
+    plain = plain_block(capi, torch, local, dev, flush, peak, args.steps, max(3, args.warmup)) \
+        if solo and batched and not args.no_plain else None
+    serving = serving_block() if solo and not args.no_serving else None
 
     if rank == 0:
         step_ms = total_ms / args.steps
-        config = {"workload": wl.name, "n_points": n, "ndim": ndim, "dc": wl.dc, "rhoc": wl.rhoc, "dm": wl.dm,
-                  "kernel": [kname, list(kpar)], "metric": "euclidean", "points_per_tile": 128,
-                  "l2": "flushed between steps (256 MiB write)",
-                  "parallelism": "replicas" if world > 1 else "single", "n_clusters": n_clusters,
-                  "step": "one CUDA-graph replay of the whole pipeline"}
-        if batched:
-            config.update({"n_events": E, "batched_points_per_s": value / world,
-                           "plain_loop": plain, "batched_vs_plain": (value / world) / plain["points_per_s"],
-                           "batched_event_latency_ms": {"p50": step_ms, "p99": step_ms}})
         line = {
             "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config,
-            "e2e": {"value": world * n * args.steps / (e2e_total / 1e3), "unit": "points/s",
-                    "h2d_bytes_per_step": int(n * (ndim + 1) * 4 + 12 * E + 264 * E),
-                    "d2h_bytes_per_step": int(n * 2 * 4 + 4 * E)},
-            "roofline": {"bound": "hbm", "kernel": "k_density" if kname == "flat" else "k_density_sym",
-                         "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                         "traffic": traffic, "algorithmic_bytes": B["density_kernel"], "launch_ms": dens_ms},
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": workload_config(wl_all, world),
+            "e2e": {"value": job_points * args.steps / (e2e_total / 1e3), "unit": "points/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "roofline": {"bound": "hbm", "kernel": "k_density" if wl.kernel[0] == "flat" else "k_density_sym",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_kind": peak_kind, "traffic": traffic, "algorithmic_bytes": B["density_kernel"],
+                         "launch_ms": dens_ms},
             "secondary_bound": issue,
-            "stage_ms": {"tiles": stage_avg[0], "density": stage_avg[1], "nearest_higher": stage_avg[2],
-                         "seeds_labels": stage_avg[3]},
-            "b_alg_total": B["total"],
-            "pipeline_hbm_frac": B["total"] / (step_ms / 1e3) / 1e9 / peak,
+            "stage_ms": dict(zip(("tiles", "density", "nearest_higher", "seeds_labels"), map(float, stage_avg))),
+            "b_alg_total": B["total"], "pipeline_hbm_frac": B["total"] / (step_ms / 1e3) / 1e9 / peak,
             "cpu_baseline": cpu, "clocks": clk, "gpu_launches": int(launches),
-            "serving": None if serving is None else {
-                "workload": "Poisson stream of 4-D events (lognormal sizes, median 2000, clipped [100, 200000]), "
-                            "dc=2.5 rhoc=6 dm=2.5 FlatKernel(0.5), 3 slots, 6 GiB device budget",
-                "rates": [{k: r[k] for k in ("offered_events_per_s", "p50_ms", "p99_ms", "points_per_s",
-                                             "achieved_events_per_s", "events_per_batch", "refused")}
-                          for r in serving]},
+            "n_clusters": int(sum(merged.values())) if (batched and rank == 0) else int(ev_ncl.sum()),
+            "near_threshold": near,
         }
+        if batched:
+            line["batched"] = {"n_events_rank0": E, "points_per_s_per_gpu": value / world,
+                               "plain_loop": plain_loop, "batched_vs_plain": (value / world) / plain_loop["points_per_s"],
+                               "batch_latency_ms": {"p50": float(np.percentile(ms, 50)), "p99": float(np.percentile(ms, 99))},
+                               "events_checksum": checksum}
+        line["plain"] = plain
+        line["serving"] = serving
         print(json.dumps(line), flush=True)
-    graph.close()
     ctx.close()
     if world > 1:
         dist.destroy_process_group()

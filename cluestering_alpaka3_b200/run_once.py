@@ -1,6 +1,6 @@
 """Run the clustering pipeline a few times on a synthetic workload (for profilers).
 
-    python -m cluestering_alpaka3_b200.run_once --workload calo4096 --passes 2
+    python -m cluestering_alpaka3_b200.run_once --workload calo4096 --passes 2 [--events 1024]
 
 Each pass enqueues the whole pipeline once (batched entry point; one event for the plain
 workloads) on one stream and waits for it; the wall time of each pass is printed.  Useful as
@@ -14,10 +14,11 @@ import time
 import numpy as np
 
 
-def build(name: str):
+def build(name: str, events: int = 4096):
     from . import synthetic
     if name == "calo4096":
         evs, p = synthetic.calo_events(4096)
+        evs = evs[:events]
         off = np.concatenate([[0], np.cumsum([e[0].shape[1] for e in evs])]).astype(np.int32)
         coords = np.ascontiguousarray(np.concatenate([e[0] for e in evs], axis=1))
         weight = np.ascontiguousarray(np.concatenate([e[1] for e in evs]))
@@ -32,6 +33,8 @@ def main():
     ap.add_argument("--workload", default="calo4096",
                     choices=["calo4096", "blobs2d_16k", "blobs2d_1m", "blobs3d_4m"])
     ap.add_argument("--passes", type=int, default=2)
+    ap.add_argument("--events", type=int, default=4096,
+                    help="calo4096: cluster only the first EVENTS events (small cases for profilers)")
     ap.add_argument("--stages", action="store_true",
                     help="time the four stages with CUDA events and print their medians")
     args = ap.parse_args()
@@ -39,7 +42,7 @@ def main():
     import torch
 
     from . import capi
-    coords, weight, off, dc, rhoc, dm, (kname, kpar) = build(args.workload)
+    coords, weight, off, dc, rhoc, dm, (kname, kpar) = build(args.workload, args.events)
     ndim, n = coords.shape
     kernel = {"flat": capi.FlatKernel, "exp": capi.ExponentialKernel, "gaus": capi.GaussianKernel}[kname](*kpar)
     params = capi.Params(dc=dc, rhoc=rhoc, dm=dm)
