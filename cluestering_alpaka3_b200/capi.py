@@ -115,7 +115,8 @@ class _ServerStats(ctypes.Structure):
 
 class _Tuning(ctypes.Structure):
     _fields_ = [("symmetric_density", ctypes.c_int32), ("nh_split_lanes", ctypes.c_int32),
-                ("overlap_chunk_points", ctypes.c_int64)]
+                ("overlap_chunk_points", ctypes.c_int64), ("density_gate", ctypes.c_int32),
+                ("density_exp2", ctypes.c_int32)]
 
 
 def _load() -> ctypes.CDLL:
@@ -410,10 +411,15 @@ class Context:
         return None
 
     def set_tuning(self, symmetric_density: int | None = None, nh_split_lanes: int | None = None,
-                   overlap_chunk_points: int | None = None):
+                   overlap_chunk_points: int | None = None, density_gate: int | None = None,
+                   density_exp2: int | None = None):
         """Set the runtime choices (clue_context_set_tuning); None keeps the current value."""
         t = _Tuning()
         check(lib.clue_context_get_tuning(self.handle, ctypes.byref(t)))
+        if density_gate is not None:
+            t.density_gate = density_gate
+        if density_exp2 is not None:
+            t.density_exp2 = density_exp2
         if symmetric_density is not None:
             t.symmetric_density = symmetric_density
         if nh_split_lanes is not None:

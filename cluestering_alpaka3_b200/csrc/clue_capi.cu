@@ -1410,6 +1410,8 @@ void clue_tuning_defaults(clue_tuning* t) {
   t->symmetric_density = d.tune_symmetric;
   t->nh_split_lanes = d.tune_nh_split;
   t->overlap_chunk_points = d.tune_overlap_chunk_points;
+  t->density_gate = d.tune_density_gate;
+  t->density_exp2 = d.tune_density_exp2;
 }
 
 clue_status clue_context_set_tuning(clue_context ctx, const clue_tuning* t) {
@@ -1432,9 +1434,15 @@ clue_status clue_context_set_tuning(clue_context ctx, const clue_tuning* t) {
     set_error("overlap_chunk_points must be >= 0");
     return CLUE_ERR_INVALID_ARG;
   }
+  if ((t->density_gate != 0 && t->density_gate != 1) || (t->density_exp2 != 0 && t->density_exp2 != 1)) {
+    set_error("density_gate and density_exp2 must be 0 or 1");
+    return CLUE_ERR_INVALID_ARG;
+  }
   ctx->ws.tune_symmetric = t->symmetric_density;
   ctx->ws.tune_nh_split = t->nh_split_lanes;
   ctx->ws.tune_overlap_chunk_points = t->overlap_chunk_points;
+  ctx->ws.tune_density_gate = t->density_gate;
+  ctx->ws.tune_density_exp2 = t->density_exp2;
   return CLUE_OK;
 }
 
@@ -1446,6 +1454,8 @@ clue_status clue_context_get_tuning(clue_context ctx, clue_tuning* t) {
   t->symmetric_density = ctx->ws.tune_symmetric;
   t->nh_split_lanes = ctx->ws.tune_nh_split;
   t->overlap_chunk_points = ctx->ws.tune_overlap_chunk_points;
+  t->density_gate = ctx->ws.tune_density_gate;
+  t->density_exp2 = ctx->ws.tune_density_exp2;
   return CLUE_OK;
 }
 
@@ -1469,11 +1479,13 @@ clue_status clue_autotune_batch(clue_context ctx, const clue_params* params, con
     return b;
   };
   char key[160];
-  std::snprintf(key, sizeof(key), "clue-tune-v1 ndim=%d nbucket=%d ebucket=%d kernel=%d metric=%d flags=%d", ndim,
+  std::snprintf(key, sizeof(key), "clue-tune-v2 ndim=%d nbucket=%d ebucket=%d kernel=%d metric=%d flags=%d", ndim,
                 ceil_log2(n), ceil_log2(n_events), kernel->type, metric->type, params->flags);
-  auto apply = [&](int sym, int split) {
+  auto apply = [&](int sym, int split, int gate, int exp2) {
     ws.tune_symmetric = sym;
     ws.tune_nh_split = split;
+    ws.tune_density_gate = gate;
+    ws.tune_density_exp2 = exp2;
   };
   auto report = [&]() {
     if (chosen) clue_context_get_tuning(ctx, chosen);
@@ -1481,14 +1493,16 @@ clue_status clue_autotune_batch(clue_context ctx, const clue_params* params, con
   if (cache_path) {
     if (FILE* f = std::fopen(cache_path, "r")) {
       char line[256];
-      int sym = -1, split = -1;
+      int sym = -1, split = -1, gate = -1, exp2 = -1;
       const size_t kl = std::strlen(key);
       while (std::fgets(line, sizeof(line), f))
         if (std::strncmp(line, key, kl) == 0 && line[kl] == ' ')
-          std::sscanf(line + kl, " | symmetric_density=%d nh_split_lanes=%d", &sym, &split);
+          std::sscanf(line + kl, " | symmetric_density=%d nh_split_lanes=%d density_gate=%d density_exp2=%d", &sym,
+                      &split, &gate, &exp2);
       std::fclose(f);
-      if ((sym == 0 || sym == 1) && split >= 0 && split <= 16) {  // the last entry of the key wins
-        apply(sym, split);
+      if ((sym == 0 || sym == 1) && split >= 0 && split <= 16 && (gate == 0 || gate == 1) &&
+          (exp2 == 0 || exp2 == 1)) {  // the last entry of the key wins
+        apply(sym, split, gate, exp2);
         report();
         return CLUE_OK;
       }
@@ -1513,8 +1527,8 @@ clue_status clue_autotune_batch(clue_context ctx, const clue_params* params, con
   if (st != CLUE_OK) set_error(std::string("autotune: ") + cudaGetErrorString(ce));
   clue_outputs out{};
   out.cluster_index = labels;
-  auto measure = [&](int sym, int split) -> float {
-    apply(sym, split);
+  auto measure = [&](int sym, int split, int gate, int exp2) -> float {
+    apply(sym, split, gate, exp2);
     float t[3] = {0, 0, 0};
     for (int r = 0; r < 4 && st == CLUE_OK; ++r) {  // one warm-up, then three timed runs
       if (cudaEventRecord(e0, s) != cudaSuccess) st = CLUE_ERR_CUDA;
@@ -1529,22 +1543,37 @@ clue_status clue_autotune_batch(clue_context ctx, const clue_params* params, con
     return t[1];
   };
   const int sym0 = sym_ok ? 1 : ws.tune_symmetric;
-  int best_sym = sym0, best_split = 8;
+  int best_sym = sym0, best_split = 8, best_gate = 0, best_exp2 = 0;
   float best = 0.0f;
   const int splits[] = {8, 0, 4, 16};  // the default first: it wins ties
   for (int split : splits) {
-    const float ms = measure(sym0, split);
+    const float ms = measure(sym0, split, 0, 0);
     if (st != CLUE_OK) break;
     if (split == 8 || ms < best) {
       best = ms;
       best_split = split;
     }
   }
+  // the symmetric sweep's pair-step alternatives (they apply to its Euclidean unit-amplitude
+  // forms; elsewhere they time the same kernel and lose ties)
+  if (st == CLUE_OK && sym_ok && metric->type == CLUE_METRIC_EUCLIDEAN && ndim <= 4) {
+    const int alts[3][2] = {{1, 0}, {0, 1}, {1, 1}};
+    for (const auto& a : alts) {
+      const float ms = measure(1, best_split, a[0], a[1]);
+      if (st != CLUE_OK) break;
+      if (ms < best) {
+        best = ms;
+        best_gate = a[0];
+        best_exp2 = a[1];
+      }
+    }
+  }
   if (st == CLUE_OK && sym_ok) {
-    const float ms = measure(0, best_split);
+    const float ms = measure(0, best_split, 0, 0);
     if (st == CLUE_OK && ms < best) {
       best = ms;
       best_sym = 0;
+      best_gate = best_exp2 = 0;
     }
   }
   if (labels) cudaFree(labels);
@@ -1552,14 +1581,15 @@ clue_status clue_autotune_batch(clue_context ctx, const clue_params* params, con
   if (e1) cudaEventDestroy(e1);
   cudaSetDevice(prev);
   if (st != CLUE_OK) return st;
-  apply(best_sym, best_split);
+  apply(best_sym, best_split, best_gate, best_exp2);
   if (cache_path) {
     FILE* f = std::fopen(cache_path, "a");
     if (!f) {
       set_error(std::string("autotune: cannot write the cache ") + cache_path);
       return CLUE_ERR_INVALID_ARG;
     }
-    std::fprintf(f, "%s | symmetric_density=%d nh_split_lanes=%d | %.4f ms\n", key, best_sym, best_split, best);
+    std::fprintf(f, "%s | symmetric_density=%d nh_split_lanes=%d density_gate=%d density_exp2=%d | %.4f ms\n", key,
+                 best_sym, best_split, best_gate, best_exp2, best);
     std::fclose(f);
   }
   report();

@@ -399,6 +399,33 @@ __device__ __forceinline__ float ex2_approx(float x) {
   asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
   return y;
 }
+// 2^e of two values on the FMA pipe instead of the MUFU (XU) pipe, for e <= 0: e is split as
+// n + f with n the nearest integer (adding and subtracting 1.5 * 2^23 rounds to an integer) and
+// |f| <= 1/2; 2^f = exp(f ln 2) is the Taylor series of exp truncated after degree 6 (Horner
+// form, paired fused multiply-adds), and 2^n is added to the exponent field.  Truncation error
+// (ln2 / 2)^7 / 7! * exp(ln2 / 2) < 1.7e-7 relative to 2^f >= 0.7, plus a few ulp of rounding:
+// below 5e-7 relative.  e below -126 is clamped (the result stays a normal number); e = 0 gives
+// exactly 1.
+__device__ __forceinline__ float2 exp2_poly2(float2 e) {
+  constexpr double kLn2 = 0.69314718055994530942;
+  constexpr float c1 = (float)kLn2, c2 = (float)(kLn2 * kLn2 / 2.0), c3 = (float)(kLn2 * kLn2 * kLn2 / 6.0),
+                  c4 = (float)(kLn2 * kLn2 * kLn2 * kLn2 / 24.0),
+                  c5 = (float)(kLn2 * kLn2 * kLn2 * kLn2 * kLn2 / 120.0),
+                  c6 = (float)(kLn2 * kLn2 * kLn2 * kLn2 * kLn2 * kLn2 / 720.0);
+  const float2 magic = make_float2(12582912.0f, 12582912.0f);
+  e = make_float2(fmaxf(e.x, -126.0f), fmaxf(e.y, -126.0f));
+  const float2 t = add2(e, magic);
+  const float2 f = sub2(e, sub2(t, magic));
+  float2 p = fma2(make_float2(c6, c6), f, make_float2(c5, c5));
+  p = fma2(p, f, make_float2(c4, c4));
+  p = fma2(p, f, make_float2(c3, c3));
+  p = fma2(p, f, make_float2(c2, c2));
+  p = fma2(p, f, make_float2(c1, c1));
+  p = fma2(p, f, make_float2(1.0f, 1.0f));
+  const int nx = __float_as_int(t.x) - 0x4B400000, ny = __float_as_int(t.y) - 0x4B400000;
+  return make_float2(__int_as_float(__float_as_int(p.x) + (nx << 23)),
+                     __int_as_float(__float_as_int(p.y) + (ny << 23)));
+}
 __device__ __forceinline__ float exp_approx(float x) {
   float y;
   asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x * 1.4426950408889634f));

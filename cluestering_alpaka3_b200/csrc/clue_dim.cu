@@ -1531,7 +1531,12 @@ __device__ __forceinline__ int fix_exponent(const EvGrid* g, float kmax) {
   return max(-126, min(126, 61 - e));
 }
 
-template <int N, int MT, int FORM>
+// VAR selects measured alternatives of the pair step (clue_tuning.density_gate / density_exp2):
+// bit 0: a warp vote per pair of steps skips the kernel evaluation and the mirrored shuffles when
+// no lane of the warp has a candidate within dc (the same bits: the skipped terms are zeros);
+// bit 1: the unit-amplitude forms evaluate 2^x with exp2_poly2 on the FMA pipe instead of
+// ex2.approx on the MUFU pipe (within 5e-7 relative per term).
+template <int N, int MT, int FORM, int VAR>
 __global__ void __launch_bounds__(kTileThreads, (N <= 4 ? 8 : 4) * 128 / kTileThreads) k_density_sym(
     const KParams kp, Events ev, const int32_t* __restrict__ off, const int32_t* __restrict__ chunk_tile,
     const uint32_t* __restrict__ chunk_off, const uint32_t* __restrict__ chunk_total,
@@ -1576,10 +1581,12 @@ __global__ void __launch_bounds__(kTileThreads, (N <= 4 ? 8 : 4) * 128 / kTileTh
     if (FORM == kDensExpUnit) {
       const float2 d = M::kRoot ? make_float2(sqrt_approx(s.x), sqrt_approx(s.y)) : s;
       const float2 e = mul2(kexp2, d);
+      if (VAR & 2) return exp2_poly2(e);
       return make_float2(ex2_approx(e.x), ex2_approx(e.y));
     }
     if (FORM == kDensGauss0Unit) {
       const float2 e = mul2(kexp2, M::kRoot ? s : mul2(s, s));
+      if (VAR & 2) return exp2_poly2(e);
       return make_float2(ex2_approx(e.x), ex2_approx(e.y));
     }
     return make_float2(kval(s.x, false), kval(s.y, false));
@@ -1661,13 +1668,16 @@ __global__ void __launch_bounds__(kTileThreads, (N <= 4 ? 8 : 4) * 128 / kTileTh
           }
           const float2 cw = make_float2(__shfl_xor_sync(0xffffffffu, ow, k), __shfl_xor_sync(0xffffffffu, ow, k + 1));
           const float2 sd = partial_pair<N, MT>(x, ca, cb, kp.mpar);
-          float2 kv = kval2(sd);
-          kv.x = hv && sd.x <= tdc ? kv.x : 0.0f;
-          kv.y = hv && sd.y <= tdc ? kv.y : 0.0f;
-          acc2 = fma2(kv, cw, acc2);
-          const float2 tc = mul2(kv, wi2);
-          cacc2 = add2(cacc2, make_float2(__shfl_xor_sync(0xffffffffu, tc.x, k),
-                                          __shfl_xor_sync(0xffffffffu, tc.y, k + 1)));
+          const bool ix = hv && sd.x <= tdc, iy = hv && sd.y <= tdc;
+          if ((VAR & 1) == 0 || __any_sync(0xffffffffu, ix || iy)) {
+            float2 kv = kval2(sd);
+            kv.x = ix ? kv.x : 0.0f;
+            kv.y = iy ? kv.y : 0.0f;
+            acc2 = fma2(kv, cw, acc2);
+            const float2 tc = mul2(kv, wi2);
+            cacc2 = add2(cacc2, make_float2(__shfl_xor_sync(0xffffffffu, tc.x, k),
+                                            __shfl_xor_sync(0xffffffffu, tc.y, k + 1)));
+          }
         }
         acc = fadd(acc, fadd(acc2.x, acc2.y));
         const float cacc = fadd(cacc2.x, cacc2.y);
@@ -1992,11 +2002,26 @@ void launch_density_spatial(const KParams& kp, Workspace& ws, cudaStream_t s) {
     launch_density_spatial_form<N, MT, kDensGeneric>(kp, ws, s, 0.0f);
 }
 // Symmetric density: kernel form and largest kernel value (the self term is 1).
-template <int N, int MT, int FORM>
-void launch_density_sym_form(const KParams& kp, Workspace& ws, cudaStream_t s, float kexp, float kmax) {
-  k_density_sym<N, MT, FORM><<<chunk_grid(kp), kTileThreads, 0, s>>>(
+template <int N, int MT, int FORM, int VAR>
+void launch_density_sym_var(const KParams& kp, Workspace& ws, cudaStream_t s, float kexp, float kmax) {
+  k_density_sym<N, MT, FORM, VAR><<<chunk_grid(kp), kTileThreads, 0, s>>>(
       kp, events_of(ws), ws.offsets, ws.chunk_tile, ws.chunk_count, ws.chunk_total, ws.rec_m_cur, ws.mq, ws.tblk_off,
       ws.tblk, ws.rec_r, ws.rho_fix, kexp, kmax);
+}
+template <int N, int MT, int FORM>
+void launch_density_sym_form(const KParams& kp, Workspace& ws, cudaStream_t s, float kexp, float kmax) {
+  // the pair-step alternatives are built for the Euclidean metric and the unit-amplitude forms
+  // in up to four dimensions (the benchmark configurations); elsewhere the plain step runs
+  if constexpr (MT == CLUE_METRIC_EUCLIDEAN && FORM != kDensGeneric && N <= 4) {
+    const int var = (ws.tune_density_gate ? 1 : 0) | (ws.tune_density_exp2 ? 2 : 0);
+    switch (var) {
+      case 1: launch_density_sym_var<N, MT, FORM, 1>(kp, ws, s, kexp, kmax); return;
+      case 2: launch_density_sym_var<N, MT, FORM, 2>(kp, ws, s, kexp, kmax); return;
+      case 3: launch_density_sym_var<N, MT, FORM, 3>(kp, ws, s, kexp, kmax); return;
+      default: break;
+    }
+  }
+  launch_density_sym_var<N, MT, FORM, 0>(kp, ws, s, kexp, kmax);
 }
 template <int N, int MT>
 void launch_density_sym(const KParams& kp, Workspace& ws, cudaStream_t s, bool fuse_combine) {

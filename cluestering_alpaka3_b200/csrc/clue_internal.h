@@ -141,6 +141,8 @@ struct Workspace {
   int32_t tune_symmetric = 1;                  // symmetric density sweep where it applies
   int32_t tune_nh_split = 8;                   // nearest higher: split a block needed by <= this many lanes
   int64_t tune_overlap_chunk_points = 4400000;  // host-memory batches; 0: no overlap
+  int32_t tune_density_gate = 0;               // symmetric density: vote-gated pair steps
+  int32_t tune_density_exp2 = 0;               // symmetric density: 2^x on the FMA pipe
 
   // overlapped host-memory batches (clue_batch_make_clusters): copy streams, per-chunk events
   // and a pinned copy of every chunk's status and seed total

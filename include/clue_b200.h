@@ -39,7 +39,7 @@ extern "C" {
 #endif
 
 #define CLUE_MAX_DIM 10
-#define CLUE_ABI_VERSION 1
+#define CLUE_ABI_VERSION 2
 
 typedef enum clue_status {
   CLUE_OK = 0,
@@ -308,6 +308,10 @@ typedef struct clue_tuning {
   int32_t symmetric_density;
   int32_t nh_split_lanes;
   int64_t overlap_chunk_points;
+  /* symmetric density sweep, unit-amplitude exponential / zero-mean Gaussian kernels, Euclidean
+   * metric, up to four dimensions: */
+  int32_t density_gate;  /* 1: skip the kernel evaluation of candidate pairs no lane holds within dc */
+  int32_t density_exp2;  /* 1: evaluate 2^x on the FMA pipe (Taylor polynomial) instead of the MUFU */
 } clue_tuning;
 void clue_tuning_defaults(clue_tuning* t);
 clue_status clue_context_set_tuning(clue_context ctx, const clue_tuning* t);

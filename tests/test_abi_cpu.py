@@ -34,7 +34,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version():
     from cluestering_alpaka3_b200 import capi
-    assert capi.lib.clue_abi_version() == 1
+    assert capi.lib.clue_abi_version() == 2
 
 
 @pytest.mark.parametrize("dc,rhoc,dm,seed,ppbin", [(0.0, 1, 1, 1, 128), (-1, 1, 1, 1, 128), (1, -1, 1, 1, 128),

@@ -188,14 +188,29 @@ def test_autotune_batch_cache_and_equivalence(tmp_path):
             np.testing.assert_array_equal(getattr(got, name).view(np.uint32), getattr(ref, name).view(np.uint32),
                                           err_msg=f"split {split}: {name}")
         np.testing.assert_array_equal(ncl, ref_ncl)
-    base.set_tuning(nh_split_lanes=8, symmetric_density=0)
+    base.set_tuning(nh_split_lanes=8, density_gate=1)  # the vote-gated pair steps skip only zero terms
+    gated, _ = base.batch_host(coords, weight, off, p, k, m)
+    for name in ("cluster_index", "is_seed", "rho", "nearest_higher", "delta"):
+        np.testing.assert_array_equal(getattr(gated, name).view(np.uint32), getattr(ref, name).view(np.uint32),
+                                      err_msg=f"gated: {name}")
+    import os
+    from parity_util import check_tolerant
+    cfg = O.Config(dc=2.0, rhoc=4.0, dm=3.0, kernel="exp", kernel_par=(1.0, 1.0), nthreads=os.cpu_count() or 1)
+    for gate in (0, 1):  # 2^x on the FMA pipe: the tolerance rule
+        base.set_tuning(density_gate=gate, density_exp2=1)
+        poly, _ = base.batch_host(coords, weight, off, p, k, m)
+        check_tolerant(coords, weight, cfg, poly, offsets=off, tag=f"exp2 on the FMA pipe, gate {gate}")
+    base.set_tuning(nh_split_lanes=8, symmetric_density=0, density_gate=0, density_exp2=0)
     one_sided, _ = base.batch_host(coords, weight, off, p, k, m)
     np.testing.assert_allclose(one_sided.rho, ref.rho, rtol=2e-5)
     with pytest.raises(capi.ClueError):
         base.set_tuning(nh_split_lanes=17)
     with pytest.raises(capi.ClueError):
         base.set_tuning(symmetric_density=2)
+    with pytest.raises(capi.ClueError):
+        base.set_tuning(density_exp2=3)
     base.reset_tuning()
-    assert base.tuning() == {"symmetric_density": 1, "nh_split_lanes": 8, "overlap_chunk_points": 4400000}
+    assert base.tuning() == {"symmetric_density": 1, "nh_split_lanes": 8, "overlap_chunk_points": 4400000,
+                             "density_gate": 0, "density_exp2": 0}
     for c in (tuned, other, base):
         c.close()
