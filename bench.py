@@ -273,9 +273,11 @@ class DeviceRun:
         self.metric = capi.Metric()
         self.dcoords = torch.from_numpy(wl.coords).to(dev)
         self.dweight = torch.from_numpy(wl.weight).to(dev)
+        # the outputs the reference's make_clusters leaves in PointsDevice (labels, seed flags,
+        # densities, nearest highers; the reference stores no delta)
         self.outs = {k: torch.empty(self.n, dtype=dt, device=dev) for k, dt in
                      (("cluster_index", torch.int32), ("is_seed", torch.int32), ("rho", torch.float32),
-                      ("nearest_higher", torch.int32), ("delta", torch.float32))}
+                      ("nearest_higher", torch.int32))}
         self.optr = {k: v.data_ptr() for k, v in self.outs.items()}
         self.ncl = torch.zeros(self.E, dtype=torch.int32, device=dev)
         self.graph = ctx.capture_batch(self.dcoords.data_ptr(), self.dweight.data_ptr(), self.ndim, self.offsets,

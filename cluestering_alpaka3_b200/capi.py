@@ -116,7 +116,7 @@ class _ServerStats(ctypes.Structure):
 class _Tuning(ctypes.Structure):
     _fields_ = [("symmetric_density", ctypes.c_int32), ("nh_split_lanes", ctypes.c_int32),
                 ("overlap_chunk_points", ctypes.c_int64), ("density_gate", ctypes.c_int32),
-                ("density_exp2", ctypes.c_int32)]
+                ("density_exp2", ctypes.c_int32), ("labels_bfs", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 def _load() -> ctypes.CDLL:
@@ -412,10 +412,12 @@ class Context:
 
     def set_tuning(self, symmetric_density: int | None = None, nh_split_lanes: int | None = None,
                    overlap_chunk_points: int | None = None, density_gate: int | None = None,
-                   density_exp2: int | None = None):
+                   density_exp2: int | None = None, labels_bfs: int | None = None):
         """Set the runtime choices (clue_context_set_tuning); None keeps the current value."""
         t = _Tuning()
         check(lib.clue_context_get_tuning(self.handle, ctypes.byref(t)))
+        if labels_bfs is not None:
+            t.labels_bfs = labels_bfs
         if density_gate is not None:
             t.density_gate = density_gate
         if density_exp2 is not None:

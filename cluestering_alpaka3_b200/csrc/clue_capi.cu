@@ -148,6 +148,7 @@ std::vector<ArenaItem> arena_items(Workspace& nw, void** evtab, size_t n, size_t
       {(void**)&nw.tblk, std::min(n, n / 32 + ntiles + 1) * 2 * w * 16},
       {(void**)&nw.tblk_off, (ntiles + 1) * 4},
       {(void**)&nw.rho_fix, n * 8},
+      {(void**)&nw.ev_chunk, ((n >> 10) + 1) * 4},
   };
 }
 
@@ -1412,6 +1413,8 @@ void clue_tuning_defaults(clue_tuning* t) {
   t->overlap_chunk_points = d.tune_overlap_chunk_points;
   t->density_gate = d.tune_density_gate;
   t->density_exp2 = d.tune_density_exp2;
+  t->labels_bfs = d.tune_labels_bfs;
+  t->reserved = 0;
 }
 
 clue_status clue_context_set_tuning(clue_context ctx, const clue_tuning* t) {
@@ -1434,8 +1437,9 @@ clue_status clue_context_set_tuning(clue_context ctx, const clue_tuning* t) {
     set_error("overlap_chunk_points must be >= 0");
     return CLUE_ERR_INVALID_ARG;
   }
-  if ((t->density_gate != 0 && t->density_gate != 1) || (t->density_exp2 != 0 && t->density_exp2 != 1)) {
-    set_error("density_gate and density_exp2 must be 0 or 1");
+  if ((t->density_gate != 0 && t->density_gate != 1) || (t->density_exp2 != 0 && t->density_exp2 != 1) ||
+      (t->labels_bfs != 0 && t->labels_bfs != 1)) {
+    set_error("density_gate, density_exp2 and labels_bfs must be 0 or 1");
     return CLUE_ERR_INVALID_ARG;
   }
   ctx->ws.tune_symmetric = t->symmetric_density;
@@ -1443,6 +1447,7 @@ clue_status clue_context_set_tuning(clue_context ctx, const clue_tuning* t) {
   ctx->ws.tune_overlap_chunk_points = t->overlap_chunk_points;
   ctx->ws.tune_density_gate = t->density_gate;
   ctx->ws.tune_density_exp2 = t->density_exp2;
+  ctx->ws.tune_labels_bfs = t->labels_bfs;
   return CLUE_OK;
 }
 
@@ -1456,6 +1461,8 @@ clue_status clue_context_get_tuning(clue_context ctx, clue_tuning* t) {
   t->overlap_chunk_points = ctx->ws.tune_overlap_chunk_points;
   t->density_gate = ctx->ws.tune_density_gate;
   t->density_exp2 = ctx->ws.tune_density_exp2;
+  t->labels_bfs = ctx->ws.tune_labels_bfs;
+  t->reserved = 0;
   return CLUE_OK;
 }
 
@@ -1481,11 +1488,13 @@ clue_status clue_autotune_batch(clue_context ctx, const clue_params* params, con
   char key[160];
   std::snprintf(key, sizeof(key), "clue-tune-v2 ndim=%d nbucket=%d ebucket=%d kernel=%d metric=%d flags=%d", ndim,
                 ceil_log2(n), ceil_log2(n_events), kernel->type, metric->type, params->flags);
+  int bfs_now = 0;
   auto apply = [&](int sym, int split, int gate, int exp2) {
     ws.tune_symmetric = sym;
     ws.tune_nh_split = split;
     ws.tune_density_gate = gate;
     ws.tune_density_exp2 = exp2;
+    ws.tune_labels_bfs = bfs_now;
   };
   auto report = [&]() {
     if (chosen) clue_context_get_tuning(ctx, chosen);
@@ -1493,15 +1502,17 @@ clue_status clue_autotune_batch(clue_context ctx, const clue_params* params, con
   if (cache_path) {
     if (FILE* f = std::fopen(cache_path, "r")) {
       char line[256];
-      int sym = -1, split = -1, gate = -1, exp2 = -1;
+      int sym = -1, split = -1, gate = -1, exp2 = -1, bfs = -1;
       const size_t kl = std::strlen(key);
       while (std::fgets(line, sizeof(line), f))
         if (std::strncmp(line, key, kl) == 0 && line[kl] == ' ')
-          std::sscanf(line + kl, " | symmetric_density=%d nh_split_lanes=%d density_gate=%d density_exp2=%d", &sym,
-                      &split, &gate, &exp2);
+          std::sscanf(line + kl,
+                      " | symmetric_density=%d nh_split_lanes=%d density_gate=%d density_exp2=%d labels_bfs=%d", &sym,
+                      &split, &gate, &exp2, &bfs);
       std::fclose(f);
       if ((sym == 0 || sym == 1) && split >= 0 && split <= 16 && (gate == 0 || gate == 1) &&
-          (exp2 == 0 || exp2 == 1)) {  // the last entry of the key wins
+          (exp2 == 0 || exp2 == 1) && (bfs == 0 || bfs == 1)) {  // the last entry of the key wins
+        bfs_now = bfs;
         apply(sym, split, gate, exp2);
         report();
         return CLUE_OK;
@@ -1576,6 +1587,17 @@ clue_status clue_autotune_batch(clue_context ctx, const clue_params* params, con
       best_gate = best_exp2 = 0;
     }
   }
+  int best_bfs = 0;
+  if (st == CLUE_OK) {  // the breadth-first label form on the best of the rest (the same labels)
+    bfs_now = 1;
+    const float ms = measure(best_sym, best_split, best_gate, best_exp2);
+    bfs_now = 0;
+    if (st == CLUE_OK && ms < best) {
+      best = ms;
+      best_bfs = 1;
+    }
+  }
+  bfs_now = best_bfs;
   if (labels) cudaFree(labels);
   if (e0) cudaEventDestroy(e0);
   if (e1) cudaEventDestroy(e1);
@@ -1588,8 +1610,9 @@ clue_status clue_autotune_batch(clue_context ctx, const clue_params* params, con
       set_error(std::string("autotune: cannot write the cache ") + cache_path);
       return CLUE_ERR_INVALID_ARG;
     }
-    std::fprintf(f, "%s | symmetric_density=%d nh_split_lanes=%d density_gate=%d density_exp2=%d | %.4f ms\n", key,
-                 best_sym, best_split, best_gate, best_exp2, best);
+    std::fprintf(f,
+                 "%s | symmetric_density=%d nh_split_lanes=%d density_gate=%d density_exp2=%d labels_bfs=%d | %.4f ms\n",
+                 key, best_sym, best_split, best_gate, best_exp2, best_bfs, best);
     std::fclose(f);
   }
   report();

@@ -78,6 +78,10 @@ struct EvGrid {
   uint32_t wmax_bits;       // largest |weight| of the event (float bits; non-negative floats order as integers)
 };
 
+// Levels of the breadth-first label form (clue_tuning.labels_bfs) enqueued without host
+// synchronisation; deeper forests continue by pointer jumping from the host.
+constexpr int kBfsLevels = 64;
+
 // Device-side status block (counters and flags), read back once per call.
 struct DevStatus {
   uint32_t nonfinite;
@@ -92,6 +96,7 @@ struct DevStatus {
   uint32_t near_seed_dc;   // nearest higher found and |delta - seed_dc| <= tol * seed_dc
   uint32_t near_dm;        // nearest higher found and |delta - dm| <= tol * dm
   uint32_t nh_near_ties;   // nearest-higher choice compares densities within tol (CLUE_FLAG_NEAR_TIES)
+  uint32_t bfs_count[kBfsLevels + 1];  // frontier sizes of the breadth-first label form
 };
 
 // Relative tolerance of the near-threshold counts: the tolerance rho is held to against FP64.

@@ -51,10 +51,12 @@ struct InPtrs {
 
 // Event tables of one call.
 struct Events {
-  EvGrid* eg;            // [E]
-  const int32_t* pt;     // [E + 1] point offsets
-  const int32_t* tile;   // [E + 1] global tile offsets
+  EvGrid* eg;               // [E]
+  const int32_t* pt;        // [E + 1] point offsets
+  const int32_t* tile;      // [E + 1] global tile offsets
+  const int32_t* chunk_ev;  // [n / 1024 + 1] event of the first point of every 1024-point chunk
 };
+constexpr int kEvChunkShift = 10;
 
 __device__ __forceinline__ int warp_min_i(int v) {
 #pragma unroll
@@ -548,16 +550,42 @@ __global__ void __launch_bounds__(256) k_bbox_single(InPtrs in, int n, EvGrid* g
   if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&st->nonfinite, 1u);
 }
 
+// Event of point i.  Events are contiguous, ascending point ranges: chunk_ev holds the event of
+// the first point of i's 1024-point chunk, and the events that start later inside the chunk are
+// stepped over (a few steps at most for events of 100 points and more), which replaces a binary
+// search of about log2(E) dependent loads.  Without the table (one event, or a workspace
+// without it) the binary search.
+__device__ __forceinline__ int event_of(const int32_t* __restrict__ ev_pt, const int32_t* __restrict__ chunk_ev,
+                                        int E, int i) {
+  if (E == 1) return 0;
+  if (!chunk_ev) return find_event(ev_pt, E, i);
+  int e = __ldg(chunk_ev + (i >> kEvChunkShift));
+  while (__ldg(ev_pt + e + 1) <= i) ++e;
+  return e;
+}
+
 // Event of point i, looked up once per warp when the warp's points share one event (the usual
 // case: events are contiguous ranges of points) and per lane otherwise.
-__device__ __forceinline__ int warp_event(const int32_t* __restrict__ ev_pt, int E, int i, bool active,
-                                          bool& uniform) {
+__device__ __forceinline__ int warp_event(const int32_t* __restrict__ ev_pt, const int32_t* __restrict__ chunk_ev,
+                                          int E, int i, bool active, bool& uniform) {
   const unsigned am = __activemask();
   const int first = __shfl_sync(am, i, __ffs(am) - 1);
   const int last = __shfl_sync(am, i, 31 - __clz(am));
-  const int e0 = find_event(ev_pt, E, first);
+  const int e0 = event_of(ev_pt, chunk_ev, E, first);
   uniform = last < ev_pt[e0 + 1];
-  return uniform ? e0 : (active ? find_event(ev_pt, E, i) : e0);
+  return uniform ? e0 : (active ? event_of(ev_pt, chunk_ev, E, i) : e0);
+}
+
+// The chunk table of event_of: chunk c (points [1024 c, 1024 c + 1024)) gets the event that
+// holds its first point; every non-empty event writes the chunks whose first point it holds.
+__global__ void __launch_bounds__(256) k_event_chunks(int E, const int32_t* __restrict__ ev_pt,
+                                                      int32_t* __restrict__ chunk_ev) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += stride) {
+    const int a = ev_pt[e], b = ev_pt[e + 1];
+    if (a >= b) continue;
+    for (int c = (a + (1 << kEvChunkShift) - 1) >> kEvChunkShift; c <= (b - 1) >> kEvChunkShift; ++c) chunk_ev[c] = e;
+  }
 }
 
 // Bounding box and largest |weight| of many events.  Every warp takes spans of `span`
@@ -566,7 +594,8 @@ __device__ __forceinline__ int warp_event(const int32_t* __restrict__ ev_pt, int
 // group that straddles events falls back to per-lane atomics.
 template <int N>
 __global__ void __launch_bounds__(256) k_bbox_events(InPtrs in, int n, int E, const int32_t* __restrict__ ev_pt,
-                                                     EvGrid* eg, DevStatus* st, int span) {
+                                                     const int32_t* __restrict__ chunk_ev, EvGrid* eg, DevStatus* st,
+                                                     int span) {
   const int lane = threadIdx.x & 31;
   const int nwarps = (gridDim.x * blockDim.x) >> 5;
   bool bad = false;
@@ -595,7 +624,7 @@ __global__ void __launch_bounds__(256) k_bbox_events(InPtrs in, int n, int E, co
     for (int i0 = base; i0 < end; i0 += 32) {
       const int i = min(i0 + lane, end - 1);  // lanes past the end repeat the last point
       bool uniform;
-      const int e = warp_event(ev_pt, E, i, true, uniform);
+      const int e = warp_event(ev_pt, chunk_ev, E, i, true, uniform);
       uint32_t emn[N];
 #pragma unroll
       for (int d = 0; d < N; ++d) {
@@ -660,7 +689,7 @@ __global__ void __launch_bounds__(256) k_bin(const KParams kp, InPtrs in, Events
   const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kp.n; i += stride) {
     bool uniform;
-    const EvGrid* g = ev.eg + warp_event(ev.pt, kp.n_events, i, true, uniform);
+    const EvGrid* g = ev.eg + warp_event(ev.pt, ev.chunk_ev, kp.n_events, i, true, uniform);
     int gb = g->tile_base;
 #pragma unroll
     for (int d = 0; d < N; ++d)
@@ -727,7 +756,7 @@ __global__ void __launch_bounds__(256) k_morton_keys(const KParams kp, Events ev
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < kp.n; q += stride) {
     const uint32_t t = tile_keys[q];
     bool uniform;  // tile-sorted positions are event-major: event e holds [ev.pt[e], ev.pt[e + 1])
-    const EvGrid* g = ev.eg + warp_event(ev.pt, kp.n_events, q, true, uniform);
+    const EvGrid* g = ev.eg + warp_event(ev.pt, ev.chunk_ev, kp.n_events, q, true, uniform);
     int hb[N];
     home_bins<N>(g, (int)t, hb);
     float x[N], pl;
@@ -763,7 +792,7 @@ __global__ void __launch_bounds__(256) k_bin_composite(const KParams kp, InPtrs 
   const int stride = gridDim.x * blockDim.x;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kp.n; i += stride) {
     bool uniform;
-    const EvGrid* g = ev.eg + warp_event(ev.pt, kp.n_events, i, true, uniform);
+    const EvGrid* g = ev.eg + warp_event(ev.pt, ev.chunk_ev, kp.n_events, i, true, uniform);
     int gb = g->tile_base;
     uint32_t m = 0;
 #pragma unroll
@@ -1707,7 +1736,7 @@ __global__ void __launch_bounds__(256) k_density_combine(const KParams kp, Event
   const int stride = gridDim.x * blockDim.x;
   for (int q = blockIdx.x * blockDim.x + threadIdx.x; q < n; q += stride) {
     bool uniform;
-    const EvGrid* g = ev.eg + warp_event(ev.pt, kp.n_events, q, true, uniform);
+    const EvGrid* g = ev.eg + warp_event(ev.pt, ev.chunk_ev, kp.n_events, q, true, uniform);
     float x[N], acc;
     load_rec<N>(rec_r, q, x, acc);
     const float recv = (float)((double)rho_fix[q] * ldexp(1.0, -fix_exponent(g, kmax)));
@@ -1731,7 +1760,7 @@ __global__ void __launch_bounds__(256) k_combine_block_bbox(const KParams kp, Ev
     const bool valid = q < n;
     const int qq = valid ? q : b << 5;
     bool uniform;
-    const EvGrid* g = ev.eg + warp_event(ev.pt, kp.n_events, qq, true, uniform);
+    const EvGrid* g = ev.eg + warp_event(ev.pt, ev.chunk_ev, kp.n_events, qq, true, uniform);
     float x[N], acc;
     load_rec<N>(rec_r, qq, x, acc);
     const float rho = fadd(acc, (float)((double)rho_fix[qq] * ldexp(1.0, -fix_exponent(g, kmax))));
@@ -1890,6 +1919,74 @@ __global__ void __launch_bounds__(256) k_jump(int32_t* par, int n, int iters, De
   if (blockIdx.x == 0 && threadIdx.x == 0) atomicMax(&st->label_rounds, (uint32_t)round + 1);
 }
 
+// ---- stage 5, breadth-first form (clue_tuning.labels_bfs) ----------------------
+// The reference's follower association map (Followers::fill, AssociationMap.hpp:193-251: counts
+// per nearest higher, a scan, a scatter) and its assignment from the seeds
+// (KernelAssignClusters, ClusteringKernels.hpp:246-281, a depth-first walk per seed), here with
+// the walk done level by level over all seeds at once: the frontier of level l holds the points
+// l steps below a seed, and each of their followers takes the seed as its parent.  Points no
+// seed reaches keep their nearest higher as parent, whose chain ends at a point that is not a
+// seed, so k_finalize labels them -1 as pointer jumping does.
+
+// counts[p] = followers of p (par[i] = p >= 0).
+__global__ void __launch_bounds__(256) k_follower_count(const int32_t* __restrict__ par, int n,
+                                                        uint32_t* __restrict__ counts) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const int p = par[i];
+    if (p >= 0) atomicAdd(counts + p, 1u);
+  }
+}
+
+// Scatter of every follower into its parent's run (order inside a run is the atomic order; the
+// labels do not depend on it).  cursor starts as the exclusive scan of the counts.
+__global__ void __launch_bounds__(256) k_follower_fill(const int32_t* __restrict__ par, int n,
+                                                       uint32_t* __restrict__ cursor, int32_t* __restrict__ followers) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const int p = par[i];
+    if (p >= 0) followers[atomicAdd(cursor + p, 1u)] = i;
+  }
+}
+
+// Level 0: the seeds (parent -1 and the seed flag).
+__global__ void __launch_bounds__(256) k_bfs_seeds(const int32_t* __restrict__ par,
+                                                   const int32_t* __restrict__ is_seed_s, int n,
+                                                   int32_t* __restrict__ frontier, DevStatus* st) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+    if (par[i] < 0 && is_seed_s[i]) frontier[atomicAdd(&st->bfs_count[0], 1u)] = i;
+}
+
+// One level: every frontier point hands its seed to its followers, which form the next frontier.
+// off[p] .. off[p] + counts[p] is p's run (off = the scanned counts before the fill advanced
+// them, i.e. the cursor minus the count).
+__global__ void __launch_bounds__(256) k_bfs_level(const uint32_t* __restrict__ end, const uint32_t* __restrict__ counts,
+                                                   const int32_t* __restrict__ followers, int32_t* __restrict__ par,
+                                                   const int32_t* __restrict__ fin, int32_t* __restrict__ fout,
+                                                   DevStatus* st, int level) {
+  const uint32_t nin = st->bfs_count[level];
+  if (nin == 0) return;
+  const int stride = gridDim.x * blockDim.x;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < (int)nin; t += stride) {
+    const int u = fin[t];
+    const int seed = level == 0 ? u : par[u];
+    const uint32_t e = end[u], b = e - counts[u];
+    for (uint32_t q = b; q < e; ++q) {
+      const int c = followers[q];
+      par[c] = seed;
+      if (counts[c]) fout[atomicAdd(&st->bfs_count[level + 1], 1u)] = c;  // leaves end the walk
+    }
+  }
+}
+
+// After the last enqueued level: a frontier left over marks the run unresolved in the slot the
+// host checks after the enqueued label rounds (unresolved[3]), and the host continues by
+// pointer jumping (finish_labels), which completes any mix of seed and nearest-higher parents.
+__global__ void k_bfs_done(DevStatus* st) {
+  if (st->bfs_count[kBfsLevels] != 0) st->unresolved[3] = 1u;
+}
+
 // Seed list capacity of an event: every seed, or the reference's SeedArray capacity
 // max(seed_capacity, points without nearest higher) (SetupSeeds.hpp:10-20).
 __device__ __forceinline__ int64_t seed_cap(const KParams& kp, const EvGrid* g) {
@@ -1910,7 +2007,7 @@ __global__ void __launch_bounds__(256) k_finalize(const KParams kp, Events ev, c
   const int stride = gridDim.x * blockDim.x;
   for (int pos = blockIdx.x * blockDim.x + threadIdx.x; pos < kp.n; pos += stride) {
     bool uniform;
-    const int e = warp_event(ev.pt, kp.n_events, pos, true, uniform);
+    const int e = warp_event(ev.pt, ev.chunk_ev, kp.n_events, pos, true, uniform);
     const int p = par[pos];
     const int root = p >= 0 ? p : pos;
     int lab = -1;
@@ -1961,7 +2058,7 @@ int grid_for(int n, int threads) {
 
 inline int chunk_grid(const KParams& kp) { return kp.n / kChunk + kp.ntiles + 1; }
 
-inline Events events_of(Workspace& ws) { return Events{ws.ev, ws.ev_pt, ws.ev_tile}; }
+inline Events events_of(Workspace& ws) { return Events{ws.ev, ws.ev_pt, ws.ev_tile, ws.ev_chunk}; }
 
 template <int N, int MT>
 void launch_density(const KParams& kp, Workspace& ws, cudaStream_t s) {
@@ -2105,6 +2202,7 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
 
   stage_mark(ws, 0, s);
   k_init<N><<<grid_for(kp.n_events, 256), 256, 0, s>>>(kp, ev, ws.ev_pt, ws.ev_tile, ws.status);
+  int launches_pre = 0;
   if (kp.n_events == 1)
     k_bbox_single<N><<<grid_for(n, 256), 256, 0, s>>>(in, n, ws.ev, ws.status);
   else
@@ -2113,10 +2211,14 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
     // are enough points, so the loads of many spans are in flight
     const int span = std::max(32, std::min(1024, (n / (148 * 64 * 4)) & ~31));
     const int blocks = std::max(1, std::min(grid_for(n, 256), ((n + span - 1) / span + 7) / 8));
-    k_bbox_events<N><<<blocks, 256, 0, s>>>(in, n, kp.n_events, ws.ev_pt, ws.ev, ws.status, span);
+    if (ws.ev_chunk) {
+      k_event_chunks<<<grid_for(kp.n_events, 256), 256, 0, s>>>(kp.n_events, ws.ev_pt, ws.ev_chunk);
+      ++launches_pre;
+    }
+    k_bbox_events<N><<<blocks, 256, 0, s>>>(in, n, kp.n_events, ws.ev_pt, ws.ev_chunk, ws.ev, ws.status, span);
   }
   k_grid<N><<<grid_for(kp.n_events, 256), 256, 0, s>>>(kp.n_events, ws.ev);
-  int launches = 4;  // init, bbox, grid, bin
+  int launches = 4 + launches_pre;  // init, (chunk table,) bbox, grid, bin
   // density order: the reference's candidate order for the flat kernel (bit-exact sums), spatial
   // order for the exponential and Gaussian kernels (whose device expf already differs from the
   // host's by an ulp) unless the caller asks for the reference order
@@ -2235,15 +2337,35 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
   stage_mark(ws, 3, s);
   CLUE_METRIC_SWITCH(a.metric, launch_seeds, kp, ws, s);
   exclusive_scan(ws.seed_flag, ws.seed_flag, (size_t)n, ws.scan_scratch, ws.seed_total, s);
-  for (int r = 0; r < kJumpLaunches; ++r)
-    k_jump<<<grid_for(n, 256), 256, 0, s>>>(ws.par, n, kJumpIters, ws.status, r);
+  int label_launches = kJumpLaunches;
+  if (ws.tune_labels_bfs) {
+    // follower CSR in buffers that are dead by now: the sort keys and the weight records
+    uint32_t* counts = ws.keys[0];
+    uint32_t* run_end = ws.keys[1];
+    int32_t* followers = reinterpret_cast<int32_t*>(ws.rec_w);
+    int32_t* front[2] = {followers + n, followers + 2 * (size_t)n};
+    cudaMemsetAsync(counts, 0, (size_t)n * sizeof(uint32_t), s);
+    k_follower_count<<<grid_for(n, 256), 256, 0, s>>>(ws.par, n, counts);
+    exclusive_scan(counts, run_end, (size_t)n, ws.scan_scratch, nullptr, s);
+    k_follower_fill<<<grid_for(n, 256), 256, 0, s>>>(ws.par, n, run_end, followers);
+    k_bfs_seeds<<<grid_for(n, 256), 256, 0, s>>>(ws.par, ws.is_seed_s, n, front[0], ws.status);
+    const int lg = std::min(grid_for(n, 256), 148 * 8);
+    for (int l = 0; l < kBfsLevels; ++l)
+      k_bfs_level<<<lg, 256, 0, s>>>(run_end, counts, followers, ws.par, front[l & 1], front[(l + 1) & 1], ws.status,
+                                     l);
+    k_bfs_done<<<1, 1, 0, s>>>(ws.status);
+    label_launches = kScanLaunches + kBfsLevels + 4;  // count, scan, fill, seeds, levels, done
+  } else {
+    for (int r = 0; r < kJumpLaunches; ++r)
+      k_jump<<<grid_for(n, 256), 256, 0, s>>>(ws.par, n, kJumpIters, ws.status, r);
+  }
   k_finalize<N><<<grid_for(n, 256), 256, 0, s>>>(kp, ev, ws.par, ws.is_seed_s, ws.seed_flag, ws.perm, ws.nh_s,
                                                  ws.rec_r, ws.delta_s, a.out);
   k_event_info<<<grid_for(kp.n_events, 256), 256, 0, s>>>(kp, ws.ev, ws.ev_pt, ws.seed_flag, ws.seed_total,
                                                          a.ev_n_seeds, a.ev_n_clusters, ws.status);
   stage_mark(ws, 4, s);
   // Morton boxes, nh, seeds, scan, jumps, finalize, event info
-  ws.launches += launches + 3 + 1 + kScanLaunches + kJumpLaunches + 1 + 1;
+  ws.launches += launches + 3 + 1 + kScanLaunches + label_launches + 1 + 1;
   CLUE_CUDA_TRY(cudaGetLastError());
   return CLUE_OK;
 }

@@ -97,6 +97,7 @@ struct Workspace {
   EvGrid* ev = nullptr;
   int32_t* ev_pt = nullptr;
   int32_t* ev_tile = nullptr;
+  int32_t* ev_chunk = nullptr;  // [n / 1024 + 1] event of the first point of every 1024-point chunk
   DevStatus* status = nullptr;
   uint32_t* keys[2] = {nullptr, nullptr};
   int32_t* vals[2] = {nullptr, nullptr};
@@ -143,6 +144,7 @@ struct Workspace {
   int64_t tune_overlap_chunk_points = 4400000;  // host-memory batches; 0: no overlap
   int32_t tune_density_gate = 0;               // symmetric density: vote-gated pair steps
   int32_t tune_density_exp2 = 0;               // symmetric density: 2^x on the FMA pipe
+  int32_t tune_labels_bfs = 0;                 // labels by follower CSR + frontier BFS, not pointer jumping
 
   // overlapped host-memory batches (clue_batch_make_clusters): copy streams, per-chunk events
   // and a pinned copy of every chunk's status and seed total

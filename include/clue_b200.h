@@ -312,6 +312,10 @@ typedef struct clue_tuning {
    * metric, up to four dimensions: */
   int32_t density_gate;  /* 1: skip the kernel evaluation of candidate pairs no lane holds within dc */
   int32_t density_exp2;  /* 1: evaluate 2^x on the FMA pipe (Taylor polynomial) instead of the MUFU */
+  /* 1: labels from a follower CSR (counts, scan, scatter: the reference's Followers::fill) and a
+   * frontier-parallel breadth-first walk from the seeds; 0: pointer jumping.  Same labels. */
+  int32_t labels_bfs;
+  int32_t reserved;      /* 0 */
 } clue_tuning;
 void clue_tuning_defaults(clue_tuning* t);
 clue_status clue_context_set_tuning(clue_context ctx, const clue_tuning* t);

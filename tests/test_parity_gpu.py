@@ -359,3 +359,34 @@ def test_symmetric_event_bits_independent_of_batch_size(gpu_context, n_pad):
                                       err_msg=name)
     nh = res.nearest_higher[n_pad:]
     np.testing.assert_array_equal(np.where(nh >= 0, nh - n_pad, -1), alone.nearest_higher)
+
+
+# ---- labels by follower CSR + breadth-first walk (clue_tuning.labels_bfs) -----------------------
+@pytest.mark.parametrize("case", ["blobs", "deep_chains", "seed_capacity"])
+def test_labels_bfs_equal_pointer_jumping(case):
+    # The breadth-first form (the reference's follower association map and a walk from the seeds,
+    # level by level) gives the same labels as pointer jumping: bit for bit against the oracle,
+    # also past the enqueued levels (a 1-D ramp whose chains are tens of thousands deep) and with
+    # seeds dropped by the reference's seed-list capacity.
+    from cluestering_alpaka3_b200 import capi
+    from parity_util import gpu_args, oracle_cfg
+    rng = np.random.default_rng(300)
+    if case == "blobs":
+        c, w = random_blobs(rng, 20000, 2, nblobs=12, extent=60.0)
+        kw = dict(dc=1.2, rhoc=4.0, dm=1.8)
+    elif case == "deep_chains":
+        n = 30000
+        c = (np.sqrt(np.linspace(0.0, 1.0, n)) * 800.0).astype(np.float32)[None, :].copy()
+        w = np.ones(n, np.float32)
+        kw = dict(dc=0.2, rhoc=1.0, dm=0.5)
+    else:
+        c, w = random_blobs(rng, 5000, 2, nblobs=20, extent=50.0, sigma=0.8)
+        kw = dict(dc=0.6, rhoc=2.0, dm=3.0, seed_dc=0.6, seed_capacity=0)
+    ctx = capi.Context(0)
+    try:
+        ctx.set_tuning(labels_bfs=1)
+        got = ctx.make_clusters_host(c, w, *gpu_args(**kw))
+    finally:
+        ctx.close()
+    ref = O.run(c, w, oracle_cfg(**kw))
+    assert_exact(ref, got)
