@@ -44,6 +44,7 @@ EXPORTED = [
     "clue_server_create", "clue_server_destroy", "clue_server_submit", "clue_server_wait",
     "clue_server_stats_read", "clue_server_replay", "clue_tuning_defaults", "clue_context_set_tuning",
     "clue_context_get_tuning", "clue_autotune_batch", "clue_silhouette", "clue_context_read_near_counts",
+    "clue_cluster_centroids",
 ]
 
 
@@ -185,6 +186,7 @@ def _load() -> ctypes.CDLL:
     sig["clue_server_replay"] = ([vp, i32, vp, vp, vp, vp, vp, ctypes.POINTER(_Outputs), vp, ctypes.POINTER(i32)],
                                  ctypes.c_int)
     sig["clue_silhouette"] = ([vp, i32, i32, vp, vp, vp, ctypes.POINTER(f32), vp], ctypes.c_int)
+    sig["clue_cluster_centroids"] = ([vp, i32, i32, vp, vp, i32, vp, vp, ctypes.POINTER(i32), vp], ctypes.c_int)
     sig["clue_tuning_defaults"] = ([ctypes.POINTER(_Tuning)], None)
     sig["clue_context_set_tuning"] = ([vp, ctypes.POINTER(_Tuning)], ctypes.c_int)
     sig["clue_context_get_tuning"] = ([vp, ctypes.POINTER(_Tuning)], ctypes.c_int)
@@ -460,6 +462,46 @@ class Context:
                                   ctypes.c_void_p(per_point_ptr or None), ctypes.byref(mean),
                                   ctypes.c_void_p(stream)))
         return float(mean.value)
+
+    def cluster_centroids_device(self, coords_ptr: int, labels_ptr: int, ndim: int, n: int, capacity: int,
+                                 centroids_ptr: int, sizes_ptr: int = 0, stream: int = 0) -> int:
+        """Cluster centroids on the GPU (clue_cluster_centroids) into a device buffer of
+        capacity x ndim floats (and optionally the sizes); returns the number of clusters."""
+        ncl = ctypes.c_int32(0)
+        check(lib.clue_cluster_centroids(self.handle, ndim, n, ctypes.c_void_p(coords_ptr), ctypes.c_void_p(labels_ptr),
+                                         capacity, ctypes.c_void_p(centroids_ptr), ctypes.c_void_p(sizes_ptr or None),
+                                         ctypes.byref(ncl), ctypes.c_void_p(stream)))
+        return int(ncl.value)
+
+    def cluster_centroids(self, coords: np.ndarray, labels: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+        """Host arrays in, (centroids (n_clusters, ndim) float32, sizes) out, computed on the GPU."""
+        c = np.ascontiguousarray(coords, dtype=np.float32)
+        if c.ndim == 1:
+            c = c[None, :]
+        ndim, n = c.shape
+        lab = np.ascontiguousarray(labels, dtype=np.int32)
+        cap = int(lab.max(initial=-1)) + 1
+        bufs = []
+        try:
+            def dev(nbytes):
+                p = ctypes.c_void_p()
+                check(lib.clue_device_alloc(self.device, max(nbytes, 4), ctypes.byref(p)))
+                bufs.append(p)
+                return p
+            dc, dl = dev(c.nbytes), dev(lab.nbytes)
+            dcen, dsz = dev(cap * ndim * 4), dev(cap * 4)
+            check(lib.clue_memcpy_htod(dc, c.ctypes.data, c.nbytes, None))
+            check(lib.clue_memcpy_htod(dl, lab.ctypes.data, lab.nbytes, None))
+            ncl = self.cluster_centroids_device(dc.value, dl.value, ndim, n, cap, dcen.value, dsz.value)
+            cen = np.empty((ncl, ndim), np.float32)
+            sz = np.empty(ncl, np.int32)
+            if ncl:
+                check(lib.clue_memcpy_dtoh(cen.ctypes.data, dcen, cen.nbytes, None))
+                check(lib.clue_memcpy_dtoh(sz.ctypes.data, dsz, sz.nbytes, None))
+            return cen, sz
+        finally:
+            for p in bufs:
+                lib.clue_device_free(p)
 
     def set_timing(self, enable: bool = True):
         check(lib.clue_context_set_timing(self.handle, 1 if enable else 0))

@@ -1,4 +1,5 @@
-// clue_scores.cu -- silhouette score of clustered points on the GPU (clue_silhouette).
+// clue_scores.cu -- post-processing of clustered points on the GPU: silhouette score
+// (clue_silhouette) and cluster centroids (clue_cluster_centroids).
 //
 // The reference computes it on the host (include/CLUEstering/utils/detail/scores.hpp:17-99):
 // for a point i of a cluster with at least two points, a = mean distance to the other points of
@@ -118,9 +119,77 @@ void launch_silhouette(int n, int n_clustered, const float* coords, const int32_
 }  // namespace
 }  // namespace clue_b200
 
+namespace clue_b200 {
+namespace {
+
+// Centroid of cluster c, dimension d (reference utils/detail/cluster_centroid.hpp:39-65): the
+// cluster's coordinates summed from 0 in ascending point order (the CSR of clue_get_clusters
+// lists a cluster's points that way) with separately rounded FP32 adds, divided by the size as
+// a float.  One thread per (cluster, dimension); the sums are sequential so the bits match
+// the reference's host loop.
+__global__ void __launch_bounds__(256) k_centroids(int ndim, int n, int n_clusters, const float* __restrict__ coords,
+                                                   const int32_t* __restrict__ offsets,
+                                                   const int32_t* __restrict__ points, float* __restrict__ centroids,
+                                                   int32_t* __restrict__ sizes) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n_clusters * ndim; t += stride) {
+    const int c = t / ndim, d = t - c * ndim;
+    const int b = offsets[c], e = offsets[c + 1];
+    const float* x = coords + (size_t)d * n;
+    float acc = 0.0f;
+    for (int q = b; q < e; ++q) acc = fadd(acc, __ldg(x + points[q]));
+    centroids[(size_t)c * ndim + d] = fdiv(acc, (float)(e - b));
+    if (sizes && d == 0) sizes[c] = e - b;
+  }
+}
+
+}  // namespace
+}  // namespace clue_b200
+
 using namespace clue_b200;
 
 extern "C" {
+
+clue_status clue_cluster_centroids(clue_context ctx, int32_t ndim, int32_t n, const float* coords,
+                                   const int32_t* cluster_index, int32_t capacity, float* centroids,
+                                   int32_t* sizes, int32_t* n_clusters_out, void* stream) {
+  if (!ctx || !coords || !cluster_index || (!centroids && capacity > 0) || n <= 0 || capacity < 0 || ndim < 1 ||
+      ndim > kMaxDim) {
+    set_error("clue_cluster_centroids: null argument, n <= 0, capacity < 0 or ndim outside [1, 10]");
+    return CLUE_ERR_INVALID_ARG;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  int32_t *offsets = nullptr, *points = nullptr;
+  cudaError_t e = cudaMalloc(&offsets, ((size_t)n + 1) * sizeof(int32_t));
+  if (e == cudaSuccess) e = cudaMalloc(&points, (size_t)n * sizeof(int32_t));
+  if (e != cudaSuccess) {
+    if (offsets) cudaFree(offsets);
+    set_error(std::string("clue_cluster_centroids: ") + cudaGetErrorString(e));
+    return CLUE_ERR_OUT_OF_MEMORY;
+  }
+  int32_t n_clusters = 0, n_clustered = 0;
+  clue_status st = clue_get_clusters(ctx, n, cluster_index, offsets, points, &n_clusters, &n_clustered, stream);
+  if (st == CLUE_OK && n_clusters_out) *n_clusters_out = n_clusters;
+  if (st == CLUE_OK && n_clusters > capacity) {
+    set_error("clue_cluster_centroids: more clusters (" + std::to_string(n_clusters) + ") than the capacity (" +
+              std::to_string(capacity) + ")");
+    st = CLUE_ERR_CAPACITY;
+  }
+  if (st == CLUE_OK && n_clusters > 0) {
+    const int work = n_clusters * ndim;
+    k_centroids<<<std::max(1, std::min((work + 255) / 256, 148 * 16)), 256, 0, s>>>(
+        ndim, n, n_clusters, coords, offsets, points, centroids, sizes);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // the temporaries are freed below
+    if (e != cudaSuccess) {
+      set_error(std::string("clue_cluster_centroids: ") + cudaGetErrorString(e));
+      st = CLUE_ERR_CUDA;
+    }
+  }
+  cudaFree(offsets);
+  cudaFree(points);
+  return st;
+}
 
 clue_status clue_silhouette(clue_context ctx, int32_t ndim, int32_t n, const float* coords,
                             const int32_t* cluster_index, float* per_point, float* mean, void* stream) {

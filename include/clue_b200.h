@@ -26,6 +26,8 @@
  *                          include/CLUEstering/data_structures/PointsDevice.hpp:19-107,129-194
  *   clue_get_clusters   <- clue::get_clusters (cluster -> points association map)
  *                          include/CLUEstering/utils/detail/get_clusters.hpp:21-46
+ *   clue_cluster_centroids <- clue::cluster_centroids, ClusterProperties sizes
+ *                          include/CLUEstering/utils/detail/cluster_centroid.hpp:39-65
  *   clue_batch_*        <- no reference counterpart: many independent events in one launch
  */
 #ifndef CLUE_B200_H
@@ -371,6 +373,23 @@ clue_status clue_get_clusters(clue_context ctx, int32_t n, const int32_t* cluste
  */
 clue_status clue_silhouette(clue_context ctx, int32_t ndim, int32_t n, const float* coords,
                             const int32_t* cluster_index, float* per_point, float* mean, void* stream);
+
+/*
+ * Cluster centroids on the GPU (reference include/CLUEstering/utils/detail/cluster_centroid.hpp:
+ * 39-65, computed there on the host): for every cluster c, the unweighted mean of its points'
+ * coordinates, summed in ascending point order in FP32 and divided by the cluster size as a
+ * float (bit for bit the reference's loop).  coords (SoA) and cluster_index are device arrays
+ * of n points (-1 = not clustered).  centroids (device, capacity x ndim floats) receives
+ * centroid c at [c * ndim, c * ndim + ndim); sizes (device, capacity, optional) every cluster's
+ * point count (the reference's ClusterProperties::cluster sizes,
+ * data_structures/ClusterProperties.hpp:19-51).  *n_clusters_out (host, optional) = max label
+ * + 1; more clusters than `capacity` gives CLUE_ERR_CAPACITY with *n_clusters_out set
+ * (capacity 0 with centroids NULL asks for the count alone).  Allocates its temporaries and
+ * synchronises `stream`.
+ */
+clue_status clue_cluster_centroids(clue_context ctx, int32_t ndim, int32_t n, const float* coords,
+                                   const int32_t* cluster_index, int32_t capacity, float* centroids,
+                                   int32_t* sizes, int32_t* n_clusters_out, void* stream);
 
 /* ---- serving (no reference counterpart) -------------------------------------------------
  * A request loop with continuous batching on one GPU.  Callers submit single events (host

@@ -328,6 +328,12 @@ static int run_gpu(const std::string& in, float dc, float rhoc, float dm, const 
   const float sil = clue::silhouette(h_points);
   const float sil_dev = clue::silhouette(queue, d_points);
   CHECK(bits(sil) == bits(sil_dev));
+  // centroids on the GPU equal the host evaluation bit for bit
+  const auto cen_host = clue::cluster_centroids(h_points);
+  const auto cen_dev = clue::cluster_centroids(queue, d_points);
+  CHECK(cen_host.size() == cen_dev.size() && cen_dev.size() == (std::size_t)info.n_clusters);
+  for (std::size_t c = 0; c < cen_host.size() && c < cen_dev.size(); ++c)
+    for (std::size_t d = 0; d < 2; ++d) CHECK(bits(cen_host[c][d]) == bits(cen_dev[c][d]));
   CHECK(clue::validate_results(back, h_points));
   std::printf("silhouette=%.6f n_clusters=%lld dropped=%lld\n", sil, (long long)info.n_clusters,
               (long long)info.dropped_seeds);

@@ -1,10 +1,14 @@
 """Device association map (clue_get_clusters): the CSR the reference's host fill builds
 (data_structures/AssociationMap.hpp:53-74 -- keys 0..max label, point indexes ascending inside a
-key, label -1 left out), computed on the GPU."""
+key, label -1 left out), computed on the GPU, and the centroids computed from it."""
+import os
+
 import numpy as np
 import pytest
 
 from parity_util import gpu_args, random_blobs
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
 def host_csr(labels):
@@ -111,3 +115,30 @@ def test_silhouette_gpu_reference_known_answer(gpu_context):
     dc = torch.from_numpy(np.ascontiguousarray(coords, dtype=np.float32)).cuda()
     dl = torch.from_numpy(res.cluster_index.astype(np.int32)).cuda()
     assert gpu_context.silhouette_device(dc.data_ptr(), dl.data_ptr(), 2, n) >= 0.9
+
+
+@pytest.mark.gpu
+def test_cluster_centroids_gpu_bits(gpu_context):
+    # Centroids on the GPU (clue_cluster_centroids) against the reference's host loop
+    # (utils/detail/cluster_centroid.hpp:39-65): FP32 sums from 0 in ascending point order,
+    # divided by the cluster size as a float; bit for bit.  Sizes are the clusters' point counts.
+    import numpy as np
+    from oracle import oracle as O
+    for name, ndim in (("data_4096", 2), ("blob", 3)):
+        g = np.load(os.path.join(GOLDEN, name + ".npz"))
+        c, w = g["coords"], g["weight"]
+        dc, rhoc, dm = (float(v) for v in g["params"])
+        labels = O.run(c, w, O.Config(dc=dc, rhoc=rhoc, dm=dm)).cluster_index
+        cen, sizes = gpu_context.cluster_centroids(c, labels)
+        k = int(labels.max()) + 1
+        assert cen.shape == (k, c.shape[0])
+        for cl in range(k):
+            members = np.nonzero(labels == cl)[0]
+            assert sizes[cl] == members.size
+            for d in range(c.shape[0]):
+                s = np.cumsum(c[d, members].astype(np.float32), dtype=np.float32)[-1]  # sequential FP32
+                exp = np.float32(s) / np.float32(members.size)
+                assert cen[cl, d].view(np.uint32) == np.float32(exp).view(np.uint32), (name, cl, d)
+    # no clustered point: zero clusters, nothing written
+    cen, sizes = gpu_context.cluster_centroids(np.zeros((2, 10), np.float32), np.full(10, -1, np.int32))
+    assert cen.shape == (0, 2)
