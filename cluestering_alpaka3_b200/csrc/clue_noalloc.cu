@@ -8,7 +8,9 @@
 // keeps all intermediate buffers (tile CSR, sorted point records, seed and label arrays) in
 // one file-scope __device__ array of fixed size, so no allocation of any kind happens.
 //
-// Limits: at most kNoAllocMaxPoints points and kNoAllocMaxTiles tiles of the reference grid.
+// Limits: at most kNoAllocMaxPoints points and kNoAllocMaxTiles tiles of the reference grid, and
+// buffers that fit the array: 32768 points in 1 to 7 dimensions at the default 128 points per
+// tile, about 29,900 to 30,300 in 8 to 10 (the capacity error names the exact limit).
 // Every GPU that loads the library holds the array (kNoAllocBytes) until the process exits.
 // All calls on a device share the array and it keeps the last call's contents; the pipeline
 // writes every entry it later reads, so no clearing between calls is needed.  Calls whose
@@ -19,6 +21,7 @@
 #include <algorithm>
 #include <cstring>
 #include <mutex>
+#include <string>
 
 #include "clue_internal.h"
 
@@ -63,7 +66,9 @@ clue_status noalloc_scratch_address(int device, void** addr) {
 
 size_t up256(size_t x) { return (x + 255) / 256 * 256; }
 
-// Carves the scratch array into the pipeline's buffers; false if it does not fit.
+// Carves the scratch array into the pipeline's buffers, those of the symmetric density sweep
+// included (so a call takes the same sweeps, and gives the same bits, as clue_make_clusters);
+// false if they do not fit.  With base null nothing is carved: the call only checks the fit.
 bool carve(Workspace& ws, void* base, int ndim, size_t n, size_t ntiles) {
   void* evtab = nullptr;
   const size_t w = (size_t)((ndim + 1 + 3) / 4);
@@ -100,10 +105,14 @@ bool carve(Workspace& ws, void* base, int ndim, size_t n, size_t ntiles) {
       {(void**)&ws.chunk_count, (ntiles + 1) * 4},
       {(void**)&ws.chunk_tile, (n / kChunkPoints + ntiles + 1) * 4},
       {(void**)&ws.chunk_total, 16},
+      {(void**)&ws.tblk, std::min(n, n / 32 + ntiles + 1) * 2 * w * 16},
+      {(void**)&ws.tblk_off, (ntiles + 1) * 4},
+      {(void**)&ws.rho_fix, n * 8},
   };
   size_t total = 0;
   for (auto& it : items) total += up256(it.bytes);
   if (total > kNoAllocBytes) return false;
+  if (!base) return true;
   size_t o = 0;
   for (auto& it : items) {
     *it.ptr = static_cast<unsigned char*>(base) + o;
@@ -117,6 +126,28 @@ bool carve(Workspace& ws, void* base, int ndim, size_t n, size_t ntiles) {
   ws.cap_tiles = ntiles;
   ws.cap_words = w;
   return true;
+}
+
+// Largest point count whose grid (points_per_tile ppbin) and buffers fit the scratch in ndim
+// dimensions: 32768 for up to 7 dimensions at 128 points per tile, a little less for 8 to 10
+// (three float4 words per record).
+int max_points(int ndim, int32_t ppbin) {
+  auto fits = [&](int n) {
+    int32_t npd = 0, nt = 0;
+    grid_shape(n, ppbin, ndim, &npd, &nt);
+    Workspace probe;
+    return nt > 0 && nt <= kNoAllocMaxTiles && carve(probe, nullptr, ndim, (size_t)n, (size_t)nt);
+  };
+  if (!fits(1)) return 0;
+  int lo = 1, hi = kNoAllocMaxPoints;
+  while (lo < hi) {
+    const int mid = lo + (hi - lo + 1) / 2;
+    if (fits(mid))
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
 }
 
 clue_status finish_dispatch(Workspace& ws, const RunArgs& a, cudaStream_t s, int first) {
@@ -154,7 +185,9 @@ extern "C" clue_status clue_make_clusters_noalloc(const clue_params* params, con
     return CLUE_ERR_INVALID_ARG;
   }
   if (n > kNoAllocMaxPoints) {
-    set_error("clue_make_clusters_noalloc: at most 32768 points (fixed scratch of 6 MiB)");
+    set_error("clue_make_clusters_noalloc: " + std::to_string(n) + " points requested, at most " +
+              std::to_string(max_points(ndim, params->points_per_tile)) + " in " + std::to_string(ndim) +
+              " dimensions (fixed scratch of 6 MiB)");
     return CLUE_ERR_CAPACITY;
   }
   if (!coords || !weight || !out || !out->cluster_index) {
@@ -164,7 +197,7 @@ extern "C" clue_status clue_make_clusters_noalloc(const clue_params* params, con
   int32_t npd = 0, nt = 0;
   grid_shape(n, params->points_per_tile, ndim, &npd, &nt);
   if (nt <= 0 || nt > kNoAllocMaxTiles) {
-    set_error("clue_make_clusters_noalloc: at most 65536 tiles (raise points_per_tile)");
+    set_error("clue_make_clusters_noalloc: " + std::to_string(nt) + " tiles, at most 65536 (raise points_per_tile)");
     return CLUE_ERR_CAPACITY;
   }
   int device = 0;
@@ -175,7 +208,10 @@ extern "C" clue_status clue_make_clusters_noalloc(const clue_params* params, con
   Workspace ws;
   ws.device = device;
   if (!carve(ws, base, ndim, (size_t)n, (size_t)nt)) {
-    set_error("clue_make_clusters_noalloc: request does not fit the fixed scratch");
+    set_error("clue_make_clusters_noalloc: " + std::to_string(n) + " points requested, at most " +
+              std::to_string(max_points(ndim, params->points_per_tile)) + " in " + std::to_string(ndim) +
+              " dimensions with points_per_tile " + std::to_string(params->points_per_tile) +
+              " (fixed scratch of 6 MiB)");
     return CLUE_ERR_CAPACITY;
   }
 

@@ -334,12 +334,16 @@ clue_status clue_autotune_batch(clue_context ctx, const clue_params* params, con
  * latency-critical path that cannot afford cudaMalloc's implicit synchronisation).  Inputs
  * and outputs are the caller's device buffers; every intermediate buffer lives in one
  * fixed 6 MiB file-scope device array, so the call allocates nothing.
- * Limits: n <= 32768 points and at most 65536 tiles; larger requests return
- * CLUE_ERR_CAPACITY.  The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress) with that device current: make that first call before any stream
- * capture.  All calls on a device share the array (it keeps the last call's contents);
- * calls that overlap on the GPU race and must be serialised by the caller.  Blocks until
- * the results are in `out`; `info` may be NULL.
+ * The same density sweeps as clue_make_clusters, so the outputs are bit for bit those of
+ * clue_make_clusters on the same input.
+ * Limits: at most 65536 tiles, and n <= 32768 points in 1 to 7 dimensions (about 29,900 to
+ * 30,300 in 8 to 10 at the default 128 points per tile); larger requests return
+ * CLUE_ERR_CAPACITY with the exact limit for the request's dimensionality in the message.
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress) with
+ * that device current: make that first call before any stream capture.  All calls on a device
+ * share the array (it keeps the last call's contents); calls that overlap on the GPU race and
+ * must be serialised by the caller.  Every call waits for `stream` to finish its work before
+ * it returns; the results are then in `out`.  `info` may be NULL.
  */
 clue_status clue_make_clusters_noalloc(const clue_params* params, const clue_kernel* kernel,
                                        const clue_metric* metric, int32_t ndim, int32_t n,

@@ -5,8 +5,10 @@ latency-critical path that cannot take cudaMalloc's implicit synchronisation) pa
 device inputs and outputs; the entry point keeps its intermediate buffers in a fixed 6 MiB
 file-scope device array.  These tests call it through the C ABI and compare every output with
 the allocating entry point clue_make_clusters, bit for bit (the tolerance of the flat-kernel
-parity tests), on two different calls in a row so that contents left in the shared array by
-the first call cannot leak into the second.  This file sorts last so that a stop-at-first-
+parity tests; the exponential kernel takes the same density sweep in both, so it matches bit
+for bit too), on two different calls in a row so that contents left in the shared array by
+the first call cannot leak into the second, and at the largest request that fits in 8
+dimensions.  This file sorts last so that a stop-at-first-
 failure run has executed every other test before it.
 """
 import ctypes
@@ -67,6 +69,42 @@ def test_noalloc_matches_allocating_entry_point(gpu_context):
             np.testing.assert_array_equal(got[k].view(np.uint32), ref[k].view(np.uint32), err_msg=f"call {call}: {k}")
         assert info_a.n_clusters == info_b.n_clusters > 0
         assert info_a.n_seeds == info_b.n_seeds
+
+
+def test_noalloc_exponential_kernel_and_8d_limit(gpu_context):
+    # The exponential kernel takes the symmetric density sweep in both entry points (the fixed
+    # scratch holds its buffers), so the outputs agree bit for bit here too; in 8 dimensions
+    # (three float4 words per record) the largest request that fits is a little below 32768
+    # points: it runs and agrees, one point more is refused with the limit in the message.
+    import re
+    from cluestering_alpaka3_b200 import capi
+    from parity_util import random_blobs
+    rng = np.random.default_rng(77)
+    c2, w2 = random_blobs(rng, 12000, 2, nblobs=8, extent=60.0)
+    p2 = capi.Params(dc=2.0, rhoc=4.0, dm=3.0)
+    got, ia = _device_run(True, None, c2, w2, p2, capi.ExponentialKernel(1.0, 1.0), capi.Metric())
+    ref, ib = _device_run(False, gpu_context, c2, w2, p2, capi.ExponentialKernel(1.0, 1.0), capi.Metric())
+    for k in ("cluster_index", "is_seed", "nearest_higher", "rho", "delta"):
+        np.testing.assert_array_equal(got[k].view(np.uint32), ref[k].view(np.uint32), err_msg=f"exp: {k}")
+    assert ia.n_clusters == ib.n_clusters > 0
+
+    p8 = capi.Params(dc=3.0, rhoc=3.0, dm=4.0)
+    ps, ks, ms = p8.struct(), capi.FlatKernel(0.5).struct(), capi.Metric().struct(8)
+    o = capi._Outputs()
+    o.cluster_index = 16  # never dereferenced: the request is refused before any work
+    st = capi.lib.clue_make_clusters_noalloc(ctypes.byref(ps), ctypes.byref(ks), ctypes.byref(ms), 8, 32768,
+                                             ctypes.c_void_p(16), ctypes.c_void_p(16), ctypes.byref(o), None, None)
+    assert st == capi.ERR_CAPACITY
+    limit = int(re.search(r"at most (\d+) in 8 dimensions", capi.last_error()).group(1))
+    assert 29000 < limit < 32768
+    c8, w8 = random_blobs(rng, limit, 8, nblobs=6, extent=40.0)
+    got, ia = _device_run(True, None, c8, w8, p8, capi.FlatKernel(0.5), capi.Metric())
+    ref, ib = _device_run(False, gpu_context, c8, w8, p8, capi.FlatKernel(0.5), capi.Metric())
+    for k in ("cluster_index", "is_seed", "nearest_higher", "rho", "delta"):
+        np.testing.assert_array_equal(got[k].view(np.uint32), ref[k].view(np.uint32), err_msg=f"8-D: {k}")
+    st = capi.lib.clue_make_clusters_noalloc(ctypes.byref(ps), ctypes.byref(ks), ctypes.byref(ms), 8, limit + 1,
+                                             ctypes.c_void_p(16), ctypes.c_void_p(16), ctypes.byref(o), None, None)
+    assert st == capi.ERR_CAPACITY and f"at most {limit}" in capi.last_error()
 
 
 def test_noalloc_rejects_oversized_requests():
