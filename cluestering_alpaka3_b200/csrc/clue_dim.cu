@@ -1508,8 +1508,8 @@ __global__ void __launch_bounds__(kTileThreads, (N <= 4 ? 8 : 4) * 128 / kTileTh
 // order of arrival does not matter) to the candidate's accumulator.
 
 // Block boxes in compact order: block b of tile u is entry bo[u] + b (bo = exclusive scan of
-// the tiles' block counts).  One warp per (chunk, warp) slot, one record per lane (coalesced
-// loads, shuffle reductions); slots past a tile's end write nothing.
+// the tiles' block counts).  One thread per (chunk, warp) slot; slots past a tile's end write
+// nothing.
 template <int N>
 __global__ void __launch_bounds__(256) k_tblock_bbox(int max_slots, const uint32_t* __restrict__ chunk_total,
                                                     const int32_t* __restrict__ off,
@@ -1518,39 +1518,36 @@ __global__ void __launch_bounds__(256) k_tblock_bbox(int max_slots, const uint32
                                                     const uint32_t* __restrict__ bo,
                                                     const float4* __restrict__ rec_m, float4* __restrict__ tblk) {
   constexpr int BW = Blk<N>::kWords;
-  const int lane = threadIdx.x & 31;
   const int nslots = min(max_slots, kChunkWarps * (int)*chunk_total);
-  const int wstride = (gridDim.x * blockDim.x) >> 5;
-  for (int sl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; sl < nslots; sl += wstride) {
+  const int stride = gridDim.x * blockDim.x;
+  for (int sl = blockIdx.x * blockDim.x + threadIdx.x; sl < nslots; sl += stride) {
     const int c = sl / kChunkWarps;
     const int t = chunk_tile[c];
     const int b = (c - (int)chunk_off[t]) * kChunkWarps + sl % kChunkWarps;
     const int first = off[t] + (b << 5);
     const int cnt = min(32, off[t + 1] - first);
-    if (cnt <= 0) continue;  // warp-uniform
-    float x[N], pl;
-    load_rec<N>(rec_m, first + (lane < cnt ? lane : 0), x, pl);  // lanes past the end repeat record 0
-    float out[4 * BW];
-#pragma unroll
-    for (int k = 0; k < 4 * BW; ++k) out[k] = 0.0f;
+    if (cnt <= 0) continue;
+    float bb[4 * BW];
 #pragma unroll
     for (int d = 0; d < N; ++d) {
-      float lo = x[d], hi = x[d];
+      bb[d] = INFINITY;
+      bb[N + d] = -INFINITY;
+    }
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        lo = fminf(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-        hi = fmaxf(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    for (int k = 2 * N; k < 4 * BW; ++k) bb[k] = 0.0f;
+    for (int r = 0; r < cnt; ++r) {
+      float x[N], pl;
+      load_rec<N>(rec_m, first + r, x, pl);
+#pragma unroll
+      for (int d = 0; d < N; ++d) {
+        bb[d] = fminf(bb[d], x[d]);
+        bb[N + d] = fmaxf(bb[N + d], x[d]);
       }
-      out[d] = lo;
-      out[N + d] = hi;
     }
-    if (lane < BW) {
-      float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const size_t id = (size_t)bo[t] + b;
 #pragma unroll
-      for (int k = 0; k < BW; ++k)
-        if (k == lane) v = make_float4(out[4 * k], out[4 * k + 1], out[4 * k + 2], out[4 * k + 3]);
-      tblk[((size_t)bo[t] + b) * BW + lane] = v;
-    }
+    for (int k = 0; k < BW; ++k)
+      tblk[id * BW + k] = make_float4(bb[4 * k], bb[4 * k + 1], bb[4 * k + 2], bb[4 * k + 3]);
   }
 }
 
@@ -2293,7 +2290,7 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
       k_gather_morton<N><<<grid_for(n, 256), 256, 0, s>>>(ws.rec_w, n, ws.mq, ws.rec_m);
       ++launches;
     }
-    k_tblock_bbox<N><<<grid_for(max_slots * 32, 256), 256, 0, s>>>(max_slots, ws.chunk_total, ws.offsets, ws.chunk_tile,
+    k_tblock_bbox<N><<<grid_for(max_slots, 256), 256, 0, s>>>(max_slots, ws.chunk_total, ws.offsets, ws.chunk_tile,
                                                                ws.chunk_count, ws.tblk_off, ws.rec_m_cur, ws.tblk);
     ++launches;
   } else if (spatial_density) {
