@@ -1774,24 +1774,21 @@ __global__ void __launch_bounds__(256) k_combine_block_bbox(const KParams kp, Ev
 // nearest-higher distances within kNearTol of seed_dc or dm.
 template <int N, int MT>
 __global__ void __launch_bounds__(256) k_seeds(const KParams kp, int n, const float4* __restrict__ rec_r,
-                                               const int32_t* __restrict__ nh_s,
+                                               const int32_t* __restrict__ nh_s, const float* __restrict__ delta_s,
                                                const int32_t* __restrict__ perm, int32_t* __restrict__ is_seed_s,
                                                int32_t* __restrict__ par, uint32_t* __restrict__ seed_flag,
                                                DevStatus* st) {
-  using M = Metric<N, MT>;
   const int stride = gridDim.x * blockDim.x;
   uint32_t c_rhoc = 0, c_seed_dc = 0, c_dm = 0;
   for (int pos = blockIdx.x * blockDim.x + threadIdx.x; pos < n; pos += stride) {
-    float x[N], rho, c[N], pl;
+    float x[N], rho;
     load_rec<N>(rec_r, pos, x, rho);
     const int nh = nh_s[pos];
-    if (nh >= 0) {
-      load_rec<N>(rec_r, nh, c, pl);
-    } else {
-#pragma unroll
-      for (int d = 0; d < N; ++d) c[d] = FLT_MAX;  // PointsView::operator[](-1), PointsCommon.hpp:75-81
-    }
-    const float dist = M::finish(M::partial(x, c, kp.mpar));
+    // d(i, nh) is the nearest-higher stage's delta, the same metric value bit for bit; without a
+    // nearest higher the reference measures the distance to PointsView::operator[](-1), whose
+    // coordinates are FLT_MAX (PointsCommon.hpp:75-81): an infinite or FLT_MAX distance, above
+    // any finite seed_dc, which +inf decides the same way
+    const float dist = nh >= 0 ? delta_s[pos] : INFINITY;
     const bool seed = (dist > kp.seed_dc) && (rho >= kp.rhoc);
     is_seed_s[pos] = seed ? 1 : 0;
     par[pos] = seed ? -1 : nh;
@@ -2160,7 +2157,7 @@ void launch_density_sym_metric(int metric, const KParams& kp, Workspace& ws, cud
 }
 template <int N, int MT>
 void launch_seeds(const KParams& kp, Workspace& ws, cudaStream_t s) {
-  k_seeds<N, MT><<<grid_for(kp.n, 256), 256, 0, s>>>(kp, kp.n, ws.rec_r, ws.nh_s, ws.perm, ws.is_seed_s, ws.par,
+  k_seeds<N, MT><<<grid_for(kp.n, 256), 256, 0, s>>>(kp, kp.n, ws.rec_r, ws.nh_s, ws.delta_s, ws.perm, ws.is_seed_s, ws.par,
                                                      ws.seed_flag, ws.status);
 }
 template <int N, int MT>
