@@ -512,20 +512,29 @@ def main():
         e2e_total = float(t.item())
     run.close()
 
-    # ---- roofline of the dominant kernel (local density) -------------------------------------
+    # ---- roofline of the dominant kernel (the longer of the two sweeps) -----------------------
     peak, peak_kind = load_peaks()
     B = bytes_model.algorithmic_bytes(wl.coords, wl.dc, wl.dm, run.offsets)
-    dens_ms = float(stage_avg[1])
-    achieved = B["density_kernel"] / (dens_ms / 1e3) / 1e9
+    nh_dominant = float(stage_avg[2]) > float(stage_avg[1])
+    dom_ms = float(stage_avg[2] if nh_dominant else stage_avg[1])
+    dom_bytes = B["nearest_higher_kernel" if nh_dominant else "density_kernel"]
+    if nh_dominant:
+        dom_kernel = "k_nearest_higher"
+    else:
+        dom_kernel = "k_density" if wl.kernel[0] == "flat" else "k_density_sym"
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9
     traffic, issue = None, None
     tfile = os.path.join(ROOT, "profiles", f"traffic_{wl.name}.json")
     if os.path.exists(tfile):
         with open(tfile) as f:
             tj = json.load(f)
-        traffic = tj.get("density_bytes_per_launch")
+        traffic = tj.get("nearest_higher_bytes_per_launch" if nh_dominant else "density_bytes_per_launch")
         if "density_issue_active" in tj:
-            issue = {"bound": "issue", "kernel": tj.get("density_kernel"),
-                     "issue_active_frac": tj["density_issue_active"], "xu_pipe_frac": tj.get("density_xu_pipe"),
+            issue = {"bound": "issue", "kernel": dom_kernel,
+                     "issue_active_frac": tj.get("nearest_higher_issue_active") if nh_dominant
+                     else tj["density_issue_active"],
+                     "density_issue_active_frac": tj["density_issue_active"],
+                     "density_xu_pipe_frac": tj.get("density_xu_pipe"),
                      "nearest_higher_issue_active_frac": tj.get("nearest_higher_issue_active"),
                      "source": tj.get("source")}
 
@@ -544,10 +553,12 @@ def main():
             "config": workload_config(wl_all, world),
             "e2e": {"value": job_points * args.steps / (e2e_total / 1e3), "unit": "points/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "roofline": {"bound": "hbm", "kernel": "k_density" if wl.kernel[0] == "flat" else "k_density_sym",
+            "roofline": {"bound": "hbm", "kernel": dom_kernel,
                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "peak_kind": peak_kind, "traffic": traffic, "algorithmic_bytes": B["density_kernel"],
-                         "launch_ms": dens_ms},
+                         "peak_kind": peak_kind, "traffic": traffic, "algorithmic_bytes": dom_bytes,
+                         "launch_ms": dom_ms,
+                         "density_frac": B["density_kernel"] / (float(stage_avg[1]) / 1e3) / 1e9 / peak,
+                         "nearest_higher_frac": B["nearest_higher_kernel"] / (float(stage_avg[2]) / 1e3) / 1e9 / peak},
             "secondary_bound": issue,
             "stage_ms": dict(zip(("tiles", "density", "nearest_higher", "seeds_labels"), map(float, stage_avg))),
             "b_alg_total": B["total"], "pipeline_hbm_frac": B["total"] / (step_ms / 1e3) / 1e9 / peak,
