@@ -14,7 +14,9 @@ from dataclasses import dataclass, field
 import numpy as np
 
 _PKG = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_PKG, "libclue_b200.so")
+# CLUE_B200_LIB names another build of the library to load, e.g. libclue_b200_checked.so (the
+# build with device bounds checks); by default the in-tree libclue_b200.so.
+LIB_PATH = os.environ.get("CLUE_B200_LIB") or os.path.join(_PKG, "libclue_b200.so")
 MAX_DIM = 10
 
 OK, ERR_INVALID_ARG, ERR_OOM, ERR_CAPACITY, ERR_TIMEOUT, ERR_CUDA, ERR_NOT_SUPPORTED, \

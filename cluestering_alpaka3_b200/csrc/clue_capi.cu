@@ -683,6 +683,11 @@ static clue_status read_info(Workspace& ws, const KParams& kp, cudaStream_t s, c
   CLUE_CUDA_TRY(cudaMemcpyAsync(total, ws.seed_total, 4, cudaMemcpyDeviceToHost, s));
   CLUE_CUDA_TRY(cudaStreamSynchronize(s));
   unresolved = h->unresolved[3] != 0;
+  if (h->check_site) {
+    set_error(std::string("device bounds check failed in ") + check_site_name(h->check_site) + ": index " +
+              std::to_string(h->check_index));
+    return CLUE_ERR_CUDA;
+  }
   if (h->stage_timeout) {
     set_error("a bulk-copy wait in the density / nearest-higher sweep timed out");
     return CLUE_ERR_TIMEOUT;
@@ -1336,6 +1341,11 @@ static clue_status batch_host_overlapped(clue_context ctx, const clue_params* pa
   const DevStatus* hs = ws.pipe_status_host;
   const uint32_t* ht = reinterpret_cast<const uint32_t*>(hs + KM);
   for (int c = 0; c < K; ++c) {
+    if (hs[c].check_site) {
+      set_error(std::string("device bounds check failed in ") + check_site_name(hs[c].check_site) + ": index " +
+                std::to_string(hs[c].check_index));
+      return CLUE_ERR_CUDA;
+    }
     if (hs[c].stage_timeout) {
       set_error("a bulk-copy wait in the density / nearest-higher sweep timed out");
       return CLUE_ERR_TIMEOUT;

@@ -97,10 +97,55 @@ struct DevStatus {
   uint32_t near_dm;        // nearest higher found and |delta - dm| <= tol * dm
   uint32_t nh_near_ties;   // nearest-higher choice compares densities within tol (CLUE_FLAG_NEAR_TIES)
   uint32_t bfs_count[kBfsLevels + 1];  // frontier sizes of the breadth-first label form
+  uint32_t check_site;   // device bounds checks (CLUE_DEVICE_CHECKS builds): first failing site
+  int32_t check_index;   // and the index it rejected
 };
 
 // Relative tolerance of the near-threshold counts: the tolerance rho is held to against FP64.
 constexpr float kNearTol = 1e-5f;
+
+// ---- device bounds checks -----------------------------------------------------
+// A build with -DCLUE_DEVICE_CHECKS=1 tests every index that the pipeline reads from its own
+// data (permutations, parents, nearest highers, tile numbers) before it addresses memory with
+// it.  A bad index records the first failing site and the index in the status block, and the
+// access is skipped: the kernel neither traps nor reads or writes out of bounds, and the host
+// turns the record into an error after the run.  Without the flag the test compiles away.
+#ifndef CLUE_DEVICE_CHECKS
+#define CLUE_DEVICE_CHECKS 0
+#endif
+enum : uint32_t {
+  kChkGatherPerm = 1,    // k_gather: the tile sort's permutation
+  kChkSeedsPerm = 2,     // k_seeds: the permutation
+  kChkJumpParent = 3,    // k_jump: a parent pointer
+  kChkFinalizeRoot = 4,  // k_finalize: a label root and its original index
+  kChkFinalizeNh = 5,    // k_finalize: a nearest higher
+  kChkDensityTile = 6,   // k_density_sym: a tile of the search box
+  kChkDensityMirror = 7, // k_density_sym: the mirrored term's point
+};
+inline const char* check_site_name(uint32_t site) {
+  switch (site) {
+    case kChkGatherPerm: return "record gather (tile-sort permutation)";
+    case kChkSeedsPerm: return "seed flags (permutation)";
+    case kChkJumpParent: return "pointer jumping (parent)";
+    case kChkFinalizeRoot: return "labels (root)";
+    case kChkFinalizeNh: return "outputs (nearest higher)";
+    case kChkDensityTile: return "symmetric density (search-box tile)";
+    case kChkDensityMirror: return "symmetric density (mirrored point)";
+  }
+  return "unknown";
+}
+#if defined(__CUDACC__)
+__device__ __forceinline__ bool dcheck_bad(DevStatus* st, long long idx, long long n, uint32_t site) {
+#if CLUE_DEVICE_CHECKS
+  if (idx >= 0 && idx < n) return false;
+  if (atomicCAS(&st->check_site, 0u, site) == 0u) st->check_index = (int32_t)idx;
+  return true;
+#else
+  (void)st, (void)idx, (void)n, (void)site;
+  return false;
+#endif
+}
+#endif
 
 // float -> int32 truncation with x86 cvttss2si semantics (NaN and out-of-range give
 // INT32_MIN), which is what the reference's static_cast<int>(float) does on its

@@ -700,10 +700,11 @@ __global__ void __launch_bounds__(256) k_bin(const KParams kp, InPtrs in, Events
 
 template <int N>
 __global__ void __launch_bounds__(256) k_gather(InPtrs in, int n, const int32_t* __restrict__ perm,
-                                                float4* __restrict__ rec_w) {
+                                                float4* __restrict__ rec_w, DevStatus* st) {
   const int stride = gridDim.x * blockDim.x;
   for (int pos = blockIdx.x * blockDim.x + threadIdx.x; pos < n; pos += stride) {
     const int i = perm[pos];
+    if (dcheck_bad(st, i, n, kChkGatherPerm)) continue;
     float x[N];
 #pragma unroll
     for (int d = 0; d < N; ++d) x[d] = in.c[d][i];
@@ -1571,7 +1572,7 @@ __global__ void __launch_bounds__(kTileThreads, (N <= 4 ? 8 : 4) * 128 / kTileTh
     const uint32_t* __restrict__ chunk_off, const uint32_t* __restrict__ chunk_total,
     const float4* __restrict__ rec_m, const int32_t* __restrict__ mq, const uint32_t* __restrict__ bo,
     const float4* __restrict__ tblk, float4* __restrict__ rec_r, int64_t* __restrict__ rho_fix, float kexp,
-    float kmax) {
+    float kmax, DevStatus* st) {
   using M = Metric<N, MT>;
   constexpr int BW = Blk<N>::kWords;
   __shared__ float4 s_rec[kTileThreads / 32][32 * Rec<N>::kWords];
@@ -1662,7 +1663,7 @@ __global__ void __launch_bounds__(kTileThreads, (N <= 4 ? 8 : 4) * 128 / kTileTh
     int u = g->tile_base;
 #pragma unroll
     for (int d = 0; d < N; ++d) u += g->stride[d] * v[d];
-    if (u >= t) {
+    if (u >= t && !dcheck_bad(st, u, kp.ntiles, kChkDensityTile)) {
       const int pb = off[u], pe = off[u + 1];
       const int nb = (pe - pb + 31) >> 5;
       for (int b = (u == t ? a_loc + 1 : 0); b < nb; ++b) {
@@ -1710,9 +1711,11 @@ __global__ void __launch_bounds__(kTileThreads, (N <= 4 ? 8 : 4) * 128 / kTileTh
         }
         acc = fadd(acc, fadd(acc2.x, acc2.y));
         const float cacc = fadd(cacc2.x, cacc2.y);
-        if (cv && cacc != 0.0f)
-          atomicAdd(reinterpret_cast<unsigned long long*>(rho_fix + mq[first + lane]),
-                    (unsigned long long)__float2ll_rn(cacc * scale));
+        if (cv && cacc != 0.0f) {
+          const int mi = mq[first + lane];
+          if (!dcheck_bad(st, mi, kp.n, kChkDensityMirror))
+            atomicAdd(reinterpret_cast<unsigned long long*>(rho_fix + mi), (unsigned long long)__float2ll_rn(cacc * scale));
+        }
       }
     }
     int d = N - 1;
@@ -1792,7 +1795,8 @@ __global__ void __launch_bounds__(256) k_seeds(const KParams kp, int n, const fl
     const bool seed = (dist > kp.seed_dc) && (rho >= kp.rhoc);
     is_seed_s[pos] = seed ? 1 : 0;
     par[pos] = seed ? -1 : nh;
-    seed_flag[perm[pos]] = seed ? 1u : 0u;
+    const int orig = perm[pos];
+    if (!dcheck_bad(st, orig, n, kChkSeedsPerm)) seed_flag[orig] = seed ? 1u : 0u;
     c_rhoc += fabsf(rho - kp.rhoc) <= kNearTol * kp.rhoc ? 1u : 0u;
     c_seed_dc += nh >= 0 && fabsf(dist - kp.seed_dc) <= kNearTol * kp.seed_dc ? 1u : 0u;
     c_dm += nh >= 0 && fabsf(dist - kp.dm) <= kNearTol * kp.dm ? 1u : 0u;
@@ -1895,6 +1899,7 @@ __global__ void __launch_bounds__(256) k_jump(int32_t* par, int n, int iters, De
       bool any = false;
 #pragma unroll
       for (int k = 0; k < K; ++k) {
+        if (act[k] && dcheck_bad(st, p[k], n, kChkJumpParent)) act[k] = false;
         if (act[k]) {
           const int pp = __ldcg(par + p[k]);
           if (pp < 0) {
@@ -2000,13 +2005,15 @@ __global__ void __launch_bounds__(256) k_finalize(const KParams kp, Events ev, c
                                                   const int32_t* __restrict__ perm,
                                                   const int32_t* __restrict__ nh_s,
                                                   const float4* __restrict__ rec_r,
-                                                  const float* __restrict__ delta_s, clue_outputs out) {
+                                                  const float* __restrict__ delta_s, clue_outputs out,
+                                                  DevStatus* st) {
   const int stride = gridDim.x * blockDim.x;
   for (int pos = blockIdx.x * blockDim.x + threadIdx.x; pos < kp.n; pos += stride) {
     bool uniform;
     const int e = warp_event(ev.pt, ev.chunk_ev, kp.n_events, pos, true, uniform);
     const int p = par[pos];
     const int root = p >= 0 ? p : pos;
+    if (dcheck_bad(st, root, kp.n, kChkFinalizeRoot) || dcheck_bad(st, perm[root], kp.n, kChkFinalizeRoot)) continue;
     int lab = -1;
     if (is_seed_s[root]) {
       const uint32_t rk = seed_rank[perm[root]] - seed_rank[ev.pt[e]];
@@ -2023,7 +2030,7 @@ __global__ void __launch_bounds__(256) k_finalize(const KParams kp, Events ev, c
     }
     if (out.nearest_higher) {
       const int nh = seed ? -1 : nh_s[pos];
-      out.nearest_higher[i] = nh >= 0 ? perm[nh] : -1;
+      out.nearest_higher[i] = nh >= 0 && !dcheck_bad(st, nh, kp.n, kChkFinalizeNh) ? perm[nh] : -1;
     }
     if (out.delta) out.delta[i] = delta_s[pos];
   }
@@ -2100,7 +2107,7 @@ template <int N, int MT, int FORM, int VAR>
 void launch_density_sym_var(const KParams& kp, Workspace& ws, cudaStream_t s, float kexp, float kmax) {
   k_density_sym<N, MT, FORM, VAR><<<chunk_grid(kp), kTileThreads, 0, s>>>(
       kp, events_of(ws), ws.offsets, ws.chunk_tile, ws.chunk_count, ws.chunk_total, ws.rec_m_cur, ws.mq, ws.tblk_off,
-      ws.tblk, ws.rec_r, ws.rho_fix, kexp, kmax);
+      ws.tblk, ws.rec_r, ws.rho_fix, kexp, kmax, ws.status);
 }
 template <int N, int MT, int FORM>
 void launch_density_sym_form(const KParams& kp, Workspace& ws, cudaStream_t s, float kexp, float kmax) {
@@ -2238,7 +2245,7 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
     ws.perm = ws.vals[cur];
     ws.sorted_keys = ws.keys[cur];
     offsets_from_sorted(ws.sorted_keys, n, kp.ntiles, ws.offsets, s, mbits);
-    k_gather<N><<<grid_for(n, 256), 256, 0, s>>>(in, n, ws.perm, ws.rec_w);
+    k_gather<N><<<grid_for(n, 256), 256, 0, s>>>(in, n, ws.perm, ws.rec_w, ws.status);
     ws.mq = ws.vals[cur ^ 1];
     ws.minv = ws.mq_alt;
     k_iota2<<<grid_for(n, 256), 256, 0, s>>>(ws.mq, ws.minv, n);
@@ -2250,7 +2257,7 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
     ws.perm = ws.vals[cur];
     ws.sorted_keys = ws.keys[cur];
     offsets_from_sorted(ws.sorted_keys, n, kp.ntiles, ws.offsets, s);
-    k_gather<N><<<grid_for(n, 256), 256, 0, s>>>(in, n, ws.perm, ws.rec_w);
+    k_gather<N><<<grid_for(n, 256), 256, 0, s>>>(in, n, ws.perm, ws.rec_w, ws.status);
     // fine Morton order inside every tile: a stable sort by Morton key, then a stable sort by
     // tile; mq[p] = tile-sorted position of the p-th record in (tile, Morton) order
     uint32_t* mkeys[2] = {ws.keys[cur ^ 1], ws.mkeys_alt};
@@ -2357,7 +2364,7 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
       k_jump<<<grid_for(n, 256), 256, 0, s>>>(ws.par, n, kJumpIters, ws.status, r);
   }
   k_finalize<N><<<grid_for(n, 256), 256, 0, s>>>(kp, ev, ws.par, ws.is_seed_s, ws.seed_flag, ws.perm, ws.nh_s,
-                                                 ws.rec_r, ws.delta_s, a.out);
+                                                 ws.rec_r, ws.delta_s, a.out, ws.status);
   k_event_info<<<grid_for(kp.n_events, 256), 256, 0, s>>>(kp, ws.ev, ws.ev_pt, ws.seed_flag, ws.seed_total,
                                                          a.ev_n_seeds, a.ev_n_clusters, ws.status);
   stage_mark(ws, 4, s);
@@ -2381,7 +2388,7 @@ clue_status finish_labels(Workspace& ws, const RunArgs& a, cudaStream_t s, int f
     if (unres == 0) break;
   }
   k_finalize<N><<<grid_for(n, 256), 256, 0, s>>>(a.kp, events_of(ws), ws.par, ws.is_seed_s, ws.seed_flag, ws.perm,
-                                                 ws.nh_s, ws.rec_r, ws.delta_s, a.out);
+                                                 ws.nh_s, ws.rec_r, ws.delta_s, a.out, ws.status);
   ++ws.launches;
   CLUE_CUDA_TRY(cudaGetLastError());
   return CLUE_OK;

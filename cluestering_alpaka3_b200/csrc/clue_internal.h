@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cstddef>
 #include <cstdint>
@@ -171,7 +172,14 @@ struct Workspace {
 };
 
 // Records stage boundary k on s when timing is enabled.
+// Also closes the previous stage's NVTX range and opens the next one, so that a profiler's
+// timeline (nsys) shows the host enqueue of every stage by name; NVTX calls cost a pointer test
+// when no tool is attached.
 inline void stage_mark(Workspace& ws, int k, cudaStream_t s) {
+  static const char* const kNames[CLUE_N_STAGES] = {"clue: tiles", "clue: local density", "clue: nearest higher",
+                                                    "clue: seeds and labels"};
+  if (k > 0) nvtxRangePop();
+  if (k < CLUE_N_STAGES) nvtxRangePushA(kNames[k]);
   if (ws.timing && ws.tev[k]) cudaEventRecord(ws.tev[k], s);
 }
 

@@ -260,6 +260,11 @@ extern "C" clue_status clue_make_clusters_noalloc(const clue_params* params, con
     CLUE_CUDA_TRY(cudaMemcpyAsync(&h, ws.status, sizeof(DevStatus), cudaMemcpyDeviceToHost, s));
     CLUE_CUDA_TRY(cudaMemcpyAsync(&total, ws.seed_total, 4, cudaMemcpyDeviceToHost, s));
     CLUE_CUDA_TRY(cudaStreamSynchronize(s));
+    if (h.check_site) {
+      set_error(std::string("device bounds check failed in ") + check_site_name(h.check_site) + ": index " +
+                std::to_string(h.check_index));
+      return CLUE_ERR_CUDA;
+    }
     if (h.stage_timeout) {
       set_error("a bulk-copy wait in the density / nearest-higher sweep timed out");
       return CLUE_ERR_TIMEOUT;
