@@ -1224,7 +1224,7 @@ __global__ void __launch_bounds__(kTileThreads) k_density(const KParams kp, Even
 // distances by higher rho, then lower index.
 
 template <int N, int MT, int TIE>
-__global__ void __launch_bounds__(kTileThreads, (N <= 2 ? 8 : (N <= 4 ? 6 : 4)) * 128 / kTileThreads) k_nearest_higher(
+__global__ void __launch_bounds__(kTileThreads, (N <= 4 ? 8 : 4) * 128 / kTileThreads) k_nearest_higher(
     const KParams kp, Events ev, const int32_t* __restrict__ off, const int32_t* __restrict__ ord,
     const int32_t* __restrict__ chunk_tile, const uint32_t* __restrict__ chunk_off,
     const uint32_t* __restrict__ chunk_total, const float4* __restrict__ rec_r, const float4* __restrict__ rec_m,
