@@ -354,6 +354,10 @@ using namespace clue_b200;
 
 struct clue_context_s {
   Workspace ws;
+  // A second workspace and stream for the odd chunks of an overlapped host-memory batch, so that
+  // consecutive chunks' pipelines run concurrently (created on the first such batch).
+  Workspace* alt = nullptr;
+  cudaStream_t alt_stream = nullptr;
 };
 
 extern "C" {
@@ -579,6 +583,11 @@ clue_status clue_context_destroy(clue_context ctx) {
   cudaGetDevice(&prev);
   cudaSetDevice(ctx->ws.device);
   workspace_release(ctx->ws);
+  if (ctx->alt) {
+    workspace_release(*ctx->alt);
+    delete ctx->alt;
+  }
+  if (ctx->alt_stream) cudaStreamDestroy(ctx->alt_stream);
   cudaSetDevice(prev);
   delete ctx;
   return CLUE_OK;
@@ -1188,6 +1197,22 @@ static clue_status batch_host_overlapped(clue_context ctx, const clue_params* pa
   int prev = 0;
   CLUE_CUDA_TRY(cudaGetDevice(&prev));
   CLUE_CUDA_TRY(cudaSetDevice(ws.device));
+  Workspace* alt = nullptr;  // without room for a second workspace the chunks run one after another
+  if (K >= 2) {
+    if (!ctx->alt) {
+      ctx->alt = new Workspace();
+      ctx->alt->device = ws.device;
+      CLUE_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->alt_stream, cudaStreamNonBlocking));
+    }
+    alt = ctx->alt;
+    alt->tune_symmetric = ws.tune_symmetric;
+    alt->tune_nh_split = ws.tune_nh_split;
+    alt->tune_density_gate = ws.tune_density_gate;
+    alt->tune_density_exp2 = ws.tune_density_exp2;
+    alt->tune_labels_bfs = ws.tune_labels_bfs;
+    if (workspace_reserve(*alt, ndim, max_n, max_tiles, max_ev) != CLUE_OK) alt = nullptr;
+  }
+  cudaStream_t s2 = alt ? ctx->alt_stream : nullptr;
   struct DeviceGuard {
     int prev;
     ~DeviceGuard() { cudaSetDevice(prev); }
@@ -1249,6 +1274,7 @@ static clue_status batch_host_overlapped(clue_context ctx, const clue_params* pa
   CLUE_CUDA_TRY(cudaEventRecord(ev_start, s));
   CLUE_CUDA_TRY(cudaStreamWaitEvent(h2d, ev_start, 0));
   CLUE_CUDA_TRY(cudaStreamWaitEvent(d2h, ev_start, 0));
+  if (s2) CLUE_CUDA_TRY(cudaStreamWaitEvent(s2, ev_start, 0));
   for (int c = 0; c < K; ++c) {
     const int E = cut[c + 1] - cut[c];
     const size_t a0 = (size_t)ev_off[cut[c]], cnt = (size_t)ev_off[cut[c + 1]] - a0;
@@ -1271,14 +1297,14 @@ static clue_status batch_host_overlapped(clue_context ctx, const clue_params* pa
   auto drain = [&]() {
     cudaStreamSynchronize(h2d);
     cudaStreamSynchronize(s);
+    if (s2) cudaStreamSynchronize(s2);
     cudaStreamSynchronize(d2h);
   };
 
-  // 3. chunks on the caller's stream (each with its own device event table), results out on
-  //    the copy-out stream
-  EvGrid* const ev_main = ws.ev;
-  int32_t* const pt_main = ws.ev_pt;
-  int32_t* const tile_main = ws.ev_tile;
+  // 3. chunks on the caller's stream and, the odd ones, on the second workspace's stream (each
+  //    with its own device event table): consecutive chunks run concurrently, so one chunk's
+  //    small-kernel phases and kernel tails overlap the next one's sweeps; results go out on the
+  //    copy-out stream as each chunk finishes
   for (int c = 0; c < K && st == CLUE_OK; ++c) {
     const int e0 = cut[c], E = cut[c + 1] - e0;
     const size_t a0 = (size_t)ev_off[e0], cnt = (size_t)ev_off[cut[c + 1]] - a0;
@@ -1291,22 +1317,28 @@ static clue_status batch_host_overlapped(clue_context ctx, const clue_params* pa
     a.out.nearest_higher = dev_out.nearest_higher ? dev_out.nearest_higher + a0 : nullptr;
     a.out.delta = dev_out.delta ? dev_out.delta + a0 : nullptr;
     a.ev_n_clusters = dev_ncl ? dev_ncl + e0 : nullptr;
-    cudaError_t ce = cudaStreamWaitEvent(s, ev_in(c), 0);
+    const bool on_alt = alt && (c & 1);
+    Workspace& W = on_alt ? *alt : ws;
+    cudaStream_t sc = on_alt ? s2 : s;
+    cudaError_t ce = cudaStreamWaitEvent(sc, ev_in(c), 0);
     if (ce == cudaSuccess) {
-      event_table_carve(dtab + dev_tab[c], (size_t)E, &ws.ev, &ws.ev_pt, &ws.ev_tile);
-      st = run_pipeline_dispatch(ws, a, s);
-      ws.ev = ev_main;
-      ws.ev_pt = pt_main;
-      ws.ev_tile = tile_main;
+      EvGrid* const w_ev = W.ev;
+      int32_t* const w_pt = W.ev_pt;
+      int32_t* const w_tile = W.ev_tile;
+      event_table_carve(dtab + dev_tab[c], (size_t)E, &W.ev, &W.ev_pt, &W.ev_tile);
+      st = run_pipeline_dispatch(W, a, sc);
+      W.ev = w_ev;
+      W.ev_pt = w_pt;
+      W.ev_tile = w_tile;
     }
     if (ce == cudaSuccess && st == CLUE_OK) {
       if (a.out.nearest_higher && a0 > 0)
-        k_shift_indices<<<(int)std::min<size_t>((cnt + 255) / 256, 148 * 8), 256, 0, s>>>(a.out.nearest_higher,
-                                                                                         (int)cnt, (int32_t)a0);
-      k_save_status<<<1, 64, 0, s>>>(ws.status, ws.seed_total, dslot + c, dtotal + c);
+        k_shift_indices<<<(int)std::min<size_t>((cnt + 255) / 256, 148 * 8), 256, 0, sc>>>(a.out.nearest_higher,
+                                                                                          (int)cnt, (int32_t)a0);
+      k_save_status<<<1, 64, 0, sc>>>(W.status, W.seed_total, dslot + c, dtotal + c);
       ce = cudaGetLastError();
     }
-    if (ce == cudaSuccess && st == CLUE_OK) ce = cudaEventRecord(ev_done(c), s);
+    if (ce == cudaSuccess && st == CLUE_OK) ce = cudaEventRecord(ev_done(c), sc);
     if (ce == cudaSuccess && st == CLUE_OK) ce = cudaStreamWaitEvent(d2h, ev_done(c), 0);
     auto back = [&](void* dst, const void* src, size_t bytes) {
       if (ce == cudaSuccess && dst) ce = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, d2h);
@@ -1324,6 +1356,10 @@ static clue_status batch_host_overlapped(clue_context ctx, const clue_params* pa
       set_error(std::string("overlapped batch: ") + cudaGetErrorString(ce));
       st = CLUE_ERR_CUDA;
     }
+  }
+  if (st == CLUE_OK && s2) {  // the caller's stream waits for the second stream's chunks
+    CLUE_CUDA_TRY(cudaEventRecord(ws.pipe_ev[2], s2));
+    CLUE_CUDA_TRY(cudaStreamWaitEvent(s, ws.pipe_ev[2], 0));
   }
   if (st == CLUE_OK) {
     cudaError_t ce = cudaMemcpyAsync(ws.pipe_status_host, dslot, KM * (sizeof(DevStatus) + 4),
