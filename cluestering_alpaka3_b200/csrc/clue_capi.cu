@@ -1213,6 +1213,7 @@ static clue_status batch_host_overlapped(clue_context ctx, const clue_params* pa
     if (workspace_reserve(*alt, ndim, max_n, max_tiles, max_ev) != CLUE_OK) alt = nullptr;
   }
   cudaStream_t s2 = alt ? ctx->alt_stream : nullptr;
+  const uint64_t alt_launches0 = alt ? alt->launches : 0;
   struct DeviceGuard {
     int prev;
     ~DeviceGuard() { cudaSetDevice(prev); }
@@ -1357,6 +1358,7 @@ static clue_status batch_host_overlapped(clue_context ctx, const clue_params* pa
       st = CLUE_ERR_CUDA;
     }
   }
+  if (alt) ws.launches += alt->launches - alt_launches0;  // the context counts both workspaces' kernels
   if (st == CLUE_OK && s2) {  // the caller's stream waits for the second stream's chunks
     CLUE_CUDA_TRY(cudaEventRecord(ws.pipe_ev[2], s2));
     CLUE_CUDA_TRY(cudaStreamWaitEvent(s, ws.pipe_ev[2], 0));
