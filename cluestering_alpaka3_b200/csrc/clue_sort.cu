@@ -125,7 +125,16 @@ __global__ void __launch_bounds__(kSortThreads, 4) k_radix_scatter(
     key[r] = valid ? kin[base + k] : 0u;
     val[r] = valid ? (vin ? vin[base + k] : base + k) : 0;
     const uint32_t d = valid ? (key[r] >> shift) & (kRadix - 1) : (uint32_t)kRadix;
-    const uint32_t peers = __match_any_sync(0xffffffffu, d);
+    // lanes holding the same digit: one ballot per digit bit (and one for validity), measured
+    // faster than __match_any_sync (tile stage of calo4096 1.04 -> 0.92 ms)
+    uint32_t peers = __ballot_sync(0xffffffffu, valid);
+    peers = valid ? peers : ~peers;
+#pragma unroll
+    for (int b = 0; b < kRadixBits; ++b) {
+      const bool bit = (d >> b) & 1u;
+      const uint32_t bb = __ballot_sync(0xffffffffu, bit);
+      peers &= bit ? bb : ~bb;
+    }
     const uint32_t rank = __popc(peers & lt);
     off[r] = valid ? wcnt[warp][d] + rank : 0u;
     __syncwarp();
