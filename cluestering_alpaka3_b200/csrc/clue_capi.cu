@@ -134,7 +134,7 @@ struct ArenaItem {
 // words; `nw` receives the carved pointers once an arena is placed (arena_place).
 std::vector<ArenaItem> arena_items(Workspace& nw, void** evtab, size_t n, size_t ntiles, size_t n_events, size_t w) {
   const size_t nb = (size_t)sort_blocks((int)n);
-  const size_t hist_len = (size_t)kRadix * nb;
+  const size_t hist_len = hist_words(nb);
   const size_t scan_words = scan_scratch_words(std::max(std::max(hist_len, n), ntiles)) + 1;
   return {
       {evtab, event_table_bytes(n_events)},

@@ -700,9 +700,11 @@ __global__ void __launch_bounds__(256) k_bin(const KParams kp, InPtrs in, Events
 
 template <int N>
 __global__ void __launch_bounds__(256) k_gather(InPtrs in, int n, const int32_t* __restrict__ perm,
-                                                float4* __restrict__ rec_w, DevStatus* st) {
+                                                float4* __restrict__ rec_w, DevStatus* st,
+                                                int32_t* __restrict__ ida, int32_t* __restrict__ idb) {
   const int stride = gridDim.x * blockDim.x;
   for (int pos = blockIdx.x * blockDim.x + threadIdx.x; pos < n; pos += stride) {
+    if (ida) ida[pos] = idb[pos] = pos;  // identity orders, when asked for
     const int i = perm[pos];
     if (dcheck_bad(st, i, n, kChkGatherPerm)) continue;
     float x[N];
@@ -812,11 +814,6 @@ __global__ void __launch_bounds__(256) k_bin_composite(const KParams kp, InPtrs 
     }
     keys[i] = ((uint32_t)gb << mbits) | (m >> (MortonBits<N>::kBits - mbits));
   }
-}
-
-__global__ void __launch_bounds__(256) k_iota2(int32_t* __restrict__ a, int32_t* __restrict__ b, int n) {
-  const int stride = gridDim.x * blockDim.x;
-  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) a[p] = b[p] = p;
 }
 
 // Inverse permutation: minv[mq[p]] = p.
@@ -2245,19 +2242,18 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
     ws.perm = ws.vals[cur];
     ws.sorted_keys = ws.keys[cur];
     offsets_from_sorted(ws.sorted_keys, n, kp.ntiles, ws.offsets, s, mbits);
-    k_gather<N><<<grid_for(n, 256), 256, 0, s>>>(in, n, ws.perm, ws.rec_w, ws.status);
     ws.mq = ws.vals[cur ^ 1];
     ws.minv = ws.mq_alt;
-    k_iota2<<<grid_for(n, 256), 256, 0, s>>>(ws.mq, ws.minv, n);
+    k_gather<N><<<grid_for(n, 256), 256, 0, s>>>(in, n, ws.perm, ws.rec_w, ws.status, ws.mq, ws.minv);
     ws.rec_m_cur = ws.rec_w;
-    launches += radix_sort_launches(bits + mbits) + 3;
+    launches += radix_sort_launches(bits + mbits) + 2;
   } else {
     k_bin<N><<<grid_for(n, 256), 256, 0, s>>>(kp, in, ev, ws.keys[0]);
     const int cur = radix_sort_pairs(ws.keys, ws.vals, true, n, bits, ws.hist, ws.scan_scratch, s);
     ws.perm = ws.vals[cur];
     ws.sorted_keys = ws.keys[cur];
     offsets_from_sorted(ws.sorted_keys, n, kp.ntiles, ws.offsets, s);
-    k_gather<N><<<grid_for(n, 256), 256, 0, s>>>(in, n, ws.perm, ws.rec_w, ws.status);
+    k_gather<N><<<grid_for(n, 256), 256, 0, s>>>(in, n, ws.perm, ws.rec_w, ws.status, nullptr, nullptr);
     // fine Morton order inside every tile: a stable sort by Morton key, then a stable sort by
     // tile; mq[p] = tile-sorted position of the p-th record in (tile, Morton) order
     uint32_t* mkeys[2] = {ws.keys[cur ^ 1], ws.mkeys_alt};

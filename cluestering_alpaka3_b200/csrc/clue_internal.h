@@ -36,6 +36,8 @@ constexpr int kScanItems = 8;
 constexpr int kScanTile = kScanThreads * kScanItems;
 
 inline int sort_blocks(int n) { return (n + kSortTile - 1) / kSortTile; }
+// Digit-major per-block digit counts of one radix pass, then the kRadix digit totals.
+inline size_t hist_words(int nblocks) { return (size_t)kRadix * nblocks + kRadix; }
 inline int bits_for(uint32_t maxkey) {
   int b = 0;
   while (b < 32 && (maxkey >> b) != 0) ++b;
@@ -50,7 +52,7 @@ inline size_t scan_scratch_words(size_t len) { return (len + kScanTile - 1) / kS
 int radix_sort_pairs(uint32_t* keys[2], int32_t* vals[2], bool vals_identity, int n, int bits,
                      uint32_t* hist, uint32_t* scan_scratch, cudaStream_t s);
 // Kernel launches made by radix_sort_pairs / exclusive_scan for the given sizes.
-inline int radix_sort_launches(int bits) { return (bits <= 0 ? 1 : (bits + kRadixBits - 1) / kRadixBits) * 5; }
+inline int radix_sort_launches(int bits) { return (bits <= 0 ? 1 : (bits + kRadixBits - 1) / kRadixBits) * 3; }
 constexpr int kScanLaunches = 3;
 
 // Exclusive scan of len uint32 values (in may alias out).  Writes the total to *total

@@ -73,7 +73,7 @@ bool carve(Workspace& ws, void* base, int ndim, size_t n, size_t ntiles) {
   void* evtab = nullptr;
   const size_t w = (size_t)((ndim + 1 + 3) / 4);
   const size_t nb = (size_t)sort_blocks((int)n);
-  const size_t hist_len = (size_t)kRadix * nb;
+  const size_t hist_len = hist_words(nb);
   const size_t scan_words = scan_scratch_words(std::max(std::max(hist_len, n), ntiles)) + 1;
   struct Item {
     void** ptr;

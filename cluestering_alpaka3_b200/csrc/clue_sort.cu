@@ -94,7 +94,8 @@ __device__ __forceinline__ uint32_t block_excl_scan(uint32_t v, uint32_t* tot) {
 // registers (tile stage of calo4096 1.104 -> 1.068 ms).
 __global__ void __launch_bounds__(kSortThreads, 4) k_radix_scatter(
     const uint32_t* __restrict__ kin, const int32_t* __restrict__ vin, uint32_t* __restrict__ kout,
-    int32_t* __restrict__ vout, int n, int shift, const uint32_t* __restrict__ scanned, int nblocks) {
+    int32_t* __restrict__ vout, int n, int shift, const uint32_t* __restrict__ scanned,
+    const uint32_t* __restrict__ tot, int nblocks) {
   static_assert(kSortThreads == kRadix, "one thread per digit");
   constexpr int kWarps = kSortThreads / 32;
   constexpr int kSlice = kSortItems * 32;  // items per warp
@@ -110,10 +111,12 @@ __global__ void __launch_bounds__(kSortThreads, 4) k_radix_scatter(
   {
     const int d = threadIdx.x;
     const size_t idx = (size_t)d * nblocks + blockIdx.x;
-    const uint32_t first = scanned[idx];
-    const uint32_t next = idx + 1 < (size_t)kRadix * nblocks ? scanned[idx + 1] : (uint32_t)n;
-    dstart = block_excl_scan(next - first, nullptr);  // ends with a block barrier
-    gbase[d] = first - dstart;
+    const uint32_t first = scanned[idx];  // digit d's items in earlier blocks
+    const uint32_t total = tot[d];
+    const uint32_t next = (int)blockIdx.x + 1 < nblocks ? scanned[idx + 1] : total;
+    const uint32_t dbase = block_excl_scan(total, nullptr);  // items of smaller digits
+    dstart = block_excl_scan(next - first, nullptr);          // ends with a block barrier
+    gbase[d] = dbase + first - dstart;
   }
   uint32_t key[kSortItems], off[kSortItems];
   int32_t val[kSortItems];
@@ -169,6 +172,25 @@ __global__ void __launch_bounds__(kSortThreads, 4) k_radix_scatter(
     kout[g] = kk;
     vout[g] = s_val[k];
   }
+}
+
+// Exclusive scan of every digit's row of the digit-major histogram, one CTA per digit (rows are
+// contiguous); the row's total goes to tot[d].
+__global__ void __launch_bounds__(1024) k_scan_rows(uint32_t* __restrict__ hist, int nblocks,
+                                                    uint32_t* __restrict__ tot) {
+  uint32_t* row = hist + (size_t)blockIdx.x * nblocks;
+  const int per = (nblocks + 1023) / 1024;
+  const int beg = min(nblocks, (int)threadIdx.x * per), end = min(nblocks, beg + per);
+  uint32_t s = 0;
+  for (int b = beg; b < end; ++b) s += row[b];
+  uint32_t total;
+  uint32_t run = block_excl_scan(s, &total);
+  for (int b = beg; b < end; ++b) {
+    const uint32_t c = row[b];
+    row[b] = run;
+    run += c;
+  }
+  if (threadIdx.x == 0) tot[blockIdx.x] = total;
 }
 
 __global__ void __launch_bounds__(kScanThreads) k_scan_reduce(const uint32_t* __restrict__ in, size_t len,
@@ -247,11 +269,12 @@ int radix_sort_pairs(uint32_t* keys[2], int32_t* vals[2], bool vals_identity, in
   const int passes = bits <= 0 ? 1 : (bits + kRadixBits - 1) / kRadixBits;
   for (int p = 0; p < passes; ++p) {
     const int shift = p * kRadixBits;
+    uint32_t* tot = hist + (size_t)kRadix * nb;
     k_radix_hist<<<nb, kSortThreads, 0, s>>>(keys[cur], n, shift, hist, nb);
-    exclusive_scan(hist, hist, (size_t)kRadix * nb, scan_scratch, nullptr, s);
+    k_scan_rows<<<kRadix, 1024, 0, s>>>(hist, nb, tot);
     const int32_t* vin = (p == 0 && vals_identity) ? nullptr : vals[cur];
     k_radix_scatter<<<nb, kSortThreads, 0, s>>>(keys[cur], vin, keys[cur ^ 1], vals[cur ^ 1], n, shift,
-                                                hist, nb);
+                                                hist, tot, nb);
     cur ^= 1;
   }
   return cur;
