@@ -1255,46 +1255,6 @@ static clue_status batch_host_overlapped(clue_context ctx, const clue_params* pa
   auto ev_in = [&](int c) { return ws.pipe_ev[1 + 3 * c]; };
   auto ev_done = [&](int c) { return ws.pipe_ev[3 + 3 * c]; };
 
-  // 1. every chunk's grids and parameters, each event table in its own pinned slot (the host
-  //    never waits for the GPU before all chunks are enqueued)
-  std::vector<RunArgs> args(K);
-  std::vector<int32_t> rel;
-  void* pinned_main = ws.pinned;
-  for (int c = 0; c < K && st == CLUE_OK; ++c) {
-    const int e0 = cut[c], E = cut[c + 1] - e0;
-    rel.assign(ev_off + e0, ev_off + e0 + E + 1);
-    for (auto& v : rel) v -= ev_off[e0];
-    ws.pinned = static_cast<char*>(ws.pipe_pinned) + (size_t)c * host_tab;
-    st = prepare_batch(ctx, params, kernel, metric, ndim, E, rel.data(), out, args[c]);
-  }
-  ws.pinned = pinned_main;
-  if (st != CLUE_OK) return st;
-
-  // 2. copy-in stream: each chunk's event table, then its inputs, so a chunk can start as soon
-  //    as its own copies are done
-  CLUE_CUDA_TRY(cudaEventRecord(ev_start, s));
-  CLUE_CUDA_TRY(cudaStreamWaitEvent(h2d, ev_start, 0));
-  CLUE_CUDA_TRY(cudaStreamWaitEvent(d2h, ev_start, 0));
-  if (s2) CLUE_CUDA_TRY(cudaStreamWaitEvent(s2, ev_start, 0));
-  for (int c = 0; c < K; ++c) {
-    const int E = cut[c + 1] - cut[c];
-    const size_t a0 = (size_t)ev_off[cut[c]], cnt = (size_t)ev_off[cut[c + 1]] - a0;
-    if (E > 1) {  // a single event's table is written by the pipeline's first kernel
-      EvGrid *heg, *deg;
-      int32_t *hpt, *htile, *dpt, *dtile;
-      event_table_carve(static_cast<char*>(ws.pipe_pinned) + (size_t)c * host_tab, ws.cap_events, &heg, &hpt,
-                        &htile);
-      event_table_carve(dtab + dev_tab[c], (size_t)E, &deg, &dpt, &dtile);
-      CLUE_CUDA_TRY(cudaMemcpyAsync(deg, heg, (size_t)E * sizeof(EvGrid), cudaMemcpyHostToDevice, h2d));
-      CLUE_CUDA_TRY(cudaMemcpyAsync(dpt, hpt, (size_t)(E + 1) * 4, cudaMemcpyHostToDevice, h2d));
-      CLUE_CUDA_TRY(cudaMemcpyAsync(dtile, htile, (size_t)(E + 1) * 4, cudaMemcpyHostToDevice, h2d));
-    }
-    for (int d = 0; d < ndim; ++d)
-      CLUE_CUDA_TRY(cudaMemcpyAsync(dcoords + (size_t)d * nn + a0, coords + (size_t)d * nn + a0, cnt * 4,
-                                    cudaMemcpyHostToDevice, h2d));
-    CLUE_CUDA_TRY(cudaMemcpyAsync(dweight + a0, weight + a0, cnt * 4, cudaMemcpyHostToDevice, h2d));
-    CLUE_CUDA_TRY(cudaEventRecord(ev_in(c), h2d));
-  }
   auto drain = [&]() {
     cudaStreamSynchronize(h2d);
     cudaStreamSynchronize(s);
@@ -1302,7 +1262,58 @@ static clue_status batch_host_overlapped(clue_context ctx, const clue_params* pa
     cudaStreamSynchronize(d2h);
   };
 
-  // 3. chunks on the caller's stream and, the odd ones, on the second workspace's stream (each
+  // 1. copy-in stream, chunk by chunk: the chunk's inputs (they need no preparation, so the copy
+  //    engine starts at once), then the host computes the chunk's grids and parameters into its
+  //    own pinned event table while those inputs are in flight, then the table goes up; a chunk
+  //    can start as soon as its own copies are done, and the host never waits for the GPU before
+  //    all chunks are enqueued
+  CLUE_CUDA_TRY(cudaEventRecord(ev_start, s));
+  CLUE_CUDA_TRY(cudaStreamWaitEvent(h2d, ev_start, 0));
+  CLUE_CUDA_TRY(cudaStreamWaitEvent(d2h, ev_start, 0));
+  if (s2) CLUE_CUDA_TRY(cudaStreamWaitEvent(s2, ev_start, 0));
+  std::vector<RunArgs> args(K);
+  std::vector<int32_t> rel;
+  void* pinned_main = ws.pinned;
+  for (int c = 0; c < K && st == CLUE_OK; ++c) {
+    const int e0 = cut[c], E = cut[c + 1] - e0;
+    const size_t a0 = (size_t)ev_off[e0], cnt = (size_t)ev_off[cut[c + 1]] - a0;
+    cudaError_t ce = cudaSuccess;
+    for (int d = 0; d < ndim && ce == cudaSuccess; ++d)
+      ce = cudaMemcpyAsync(dcoords + (size_t)d * nn + a0, coords + (size_t)d * nn + a0, cnt * 4,
+                           cudaMemcpyHostToDevice, h2d);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(dweight + a0, weight + a0, cnt * 4, cudaMemcpyHostToDevice, h2d);
+    if (ce != cudaSuccess) {
+      set_error(std::string("overlapped batch: ") + cudaGetErrorString(ce));
+      st = CLUE_ERR_CUDA;
+      break;
+    }
+    rel.assign(ev_off + e0, ev_off + e0 + E + 1);
+    for (auto& v : rel) v -= ev_off[e0];
+    ws.pinned = static_cast<char*>(ws.pipe_pinned) + (size_t)c * host_tab;
+    st = prepare_batch(ctx, params, kernel, metric, ndim, E, rel.data(), out, args[c]);
+    ws.pinned = pinned_main;
+    if (st != CLUE_OK) break;
+    if (E > 1) {  // a single event's table is written by the pipeline's first kernel
+      EvGrid *heg, *deg;
+      int32_t *hpt, *htile, *dpt, *dtile;
+      event_table_carve(static_cast<char*>(ws.pipe_pinned) + (size_t)c * host_tab, ws.cap_events, &heg, &hpt,
+                        &htile);
+      event_table_carve(dtab + dev_tab[c], (size_t)E, &deg, &dpt, &dtile);
+      ce = cudaMemcpyAsync(deg, heg, (size_t)E * sizeof(EvGrid), cudaMemcpyHostToDevice, h2d);
+      if (ce == cudaSuccess) ce = cudaMemcpyAsync(dpt, hpt, (size_t)(E + 1) * 4, cudaMemcpyHostToDevice, h2d);
+      if (ce == cudaSuccess) ce = cudaMemcpyAsync(dtile, htile, (size_t)(E + 1) * 4, cudaMemcpyHostToDevice, h2d);
+    }
+    if (ce == cudaSuccess) ce = cudaEventRecord(ev_in(c), h2d);
+    if (ce != cudaSuccess) {
+      set_error(std::string("overlapped batch: ") + cudaGetErrorString(ce));
+      st = CLUE_ERR_CUDA;
+    }
+  }
+  if (st != CLUE_OK) {
+    drain();
+    return st;
+  }
+  // 2. chunks on the caller's stream and, the odd ones, on the second workspace's stream (each
   //    with its own device event table): consecutive chunks run concurrently, so one chunk's
   //    small-kernel phases and kernel tails overlap the next one's sweeps; results go out on the
   //    copy-out stream as each chunk finishes
