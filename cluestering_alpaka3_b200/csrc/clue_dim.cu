@@ -601,6 +601,56 @@ __global__ void __launch_bounds__(256) k_bbox_events(InPtrs in, int n, int E, co
   bool bad = false;
   for (int base = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * span; base < n; base += nwarps * span) {
     const int end = min(n, base + span);
+    {
+      // the usual case, a span inside one event: four 32-point groups per step with their loads
+      // in flight together, one warp reduction and 2N + 1 atomics
+      const int e0 = event_of(ev_pt, chunk_ev, E, base);
+      if (ev_pt[e0 + 1] >= end) {
+        uint32_t bmn[N], bmx[N], bw = 0;
+#pragma unroll
+        for (int d = 0; d < N; ++d) {
+          bmn[d] = 0xffffffffu;
+          bmx[d] = 0;
+        }
+        for (int i0 = base; i0 < end; i0 += 128) {
+          float xs[4][N], wv[4];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            const int i = min(i0 + 32 * k + lane, end - 1);  // lanes past the end repeat the last point
+#pragma unroll
+            for (int d = 0; d < N; ++d) xs[k][d] = in.c[d][i];
+            wv[k] = in.w[i];
+          }
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+#pragma unroll
+            for (int d = 0; d < N; ++d) {
+              bad |= !isfinite(xs[k][d]);
+              const uint32_t u = enc_float(xs[k][d]);
+              bmn[d] = min(bmn[d], u);
+              bmx[d] = max(bmx[d], u);
+            }
+            bad |= !isfinite(wv[k]);
+            bw = max(bw, __float_as_uint(fabsf(wv[k])));
+          }
+        }
+#pragma unroll
+        for (int d = 0; d < N; ++d) {
+          bmn[d] = warp_min_u(bmn[d]);
+          bmx[d] = warp_max_u(bmx[d]);
+        }
+        bw = warp_max_u(bw);
+        if (lane == 0) {
+#pragma unroll
+          for (int d = 0; d < N; ++d) {
+            atomicMin(&eg[e0].enc_min[d], bmn[d]);
+            atomicMax(&eg[e0].enc_max[d], bmx[d]);
+          }
+          atomicMax(&eg[e0].wmax_bits, bw);
+        }
+        continue;
+      }
+    }
     int cur = -1;  // event of the running box (warp-uniform), -1: none
     uint32_t amn[N], amx[N], aw = 0;
 #pragma unroll
@@ -785,34 +835,46 @@ __global__ void __launch_bounds__(256) k_tile_of(const uint32_t* __restrict__ ti
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) out[p] = tile_keys[mq[p]];
 }
 
-// Composite key (tile << mbits | Morton code of the point inside its tile, top mbits bits) of every
-// point, for the single sort that yields the (tile, Morton) order directly.
+// Composite key (tile << mbits | Morton code of the point inside its tile, top mbits bits) of
+// every point, for the single sort that yields the (tile, Morton) order directly.  Every thread
+// takes four points per step, their coordinates loaded together before the keys are computed.
 template <int N>
 __global__ void __launch_bounds__(256) k_bin_composite(const KParams kp, InPtrs in, Events ev, int mbits,
                                                        uint32_t* __restrict__ keys) {
   constexpr int bpd = MortonBits<N>::kPerDim;
+  constexpr int kPer = 4;
   const float scale = (float)(1u << bpd);
-  const int stride = gridDim.x * blockDim.x;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kp.n; i += stride) {
-    bool uniform;
-    const EvGrid* g = ev.eg + warp_event(ev.pt, ev.chunk_ev, kp.n_events, i, true, uniform);
-    int gb = g->tile_base;
-    uint32_t m = 0;
+  for (int base = blockIdx.x * (256 * kPer); base < kp.n; base += gridDim.x * 256 * kPer) {
+    float xs[kPer][N];
 #pragma unroll
-    for (int d = 0; d < N; ++d) {
-      // getBin without wrapped coordinates (the composite sort is only taken without them):
-      // the quotient also places the point inside its tile for the Morton code
-      const float x = in.c[d][i];
-      const float q = fdiv(fsub(x, g->mn[d]), g->size[d]);
-      int b = cvt_i32(q);
-      b = b < g->nperdim - 1 ? b : g->nperdim - 1;
-      b = b > 0 ? b : 0;
-      gb += g->stride[d] * b;
-      int c = g->size[d] > 0.0f ? (int)((q - (float)b) * scale) : 0;
-      c = c < 0 ? 0 : (c > (1 << bpd) - 1 ? (1 << bpd) - 1 : c);
-      m |= spread_bits<N>((uint32_t)c) << d;
+    for (int k = 0; k < kPer; ++k) {
+      const int i = min(base + k * 256 + (int)threadIdx.x, kp.n - 1);
+#pragma unroll
+      for (int d = 0; d < N; ++d) xs[k][d] = in.c[d][i];
     }
-    keys[i] = ((uint32_t)gb << mbits) | (m >> (MortonBits<N>::kBits - mbits));
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) {
+      const int i = base + k * 256 + (int)threadIdx.x;
+      if (i >= kp.n) break;
+      bool uniform;
+      const EvGrid* g = ev.eg + warp_event(ev.pt, ev.chunk_ev, kp.n_events, i, true, uniform);
+      int gb = g->tile_base;
+      uint32_t m = 0;
+#pragma unroll
+      for (int d = 0; d < N; ++d) {
+        // getBin without wrapped coordinates (the composite sort is only taken without them):
+        // the quotient also places the point inside its tile for the Morton code
+        const float q = fdiv(fsub(xs[k][d], g->mn[d]), g->size[d]);
+        int b = cvt_i32(q);
+        b = b < g->nperdim - 1 ? b : g->nperdim - 1;
+        b = b > 0 ? b : 0;
+        gb += g->stride[d] * b;
+        int c = g->size[d] > 0.0f ? (int)((q - (float)b) * scale) : 0;
+        c = c < 0 ? 0 : (c > (1 << bpd) - 1 ? (1 << bpd) - 1 : c);
+        m |= spread_bits<N>((uint32_t)c) << d;
+      }
+      keys[i] = ((uint32_t)gb << mbits) | (m >> (MortonBits<N>::kBits - mbits));
+    }
   }
 }
 
@@ -2237,7 +2299,7 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
   // points' indices.  The other sweeps take the tile order by index and a Morton order beside it.
   const bool composite = symmetric && bits + mbits <= 32;
   if (composite) {
-    k_bin_composite<N><<<grid_for(n, 256), 256, 0, s>>>(kp, in, ev, mbits, ws.keys[0]);
+    k_bin_composite<N><<<grid_for(n, 1024), 256, 0, s>>>(kp, in, ev, mbits, ws.keys[0]);
     const int cur = radix_sort_pairs(ws.keys, ws.vals, true, n, bits + mbits, ws.hist, ws.scan_scratch, s);
     ws.perm = ws.vals[cur];
     ws.sorted_keys = ws.keys[cur];
