@@ -1329,10 +1329,14 @@ __global__ void __launch_bounds__(kTileThreads, (N <= 4 ? 8 : 4) * 128 / kTileTh
     // rule; distances that may round to the best one's: rank rule).  consider_full() is that
     // test; it may run after other candidates' updates, since the best is an exact minimum.
     auto consider_fast = [&](int j, float s, float rho_j, bool in_block) -> bool {
-      const bool c = need && in_block && s <= bnd && rho_j >= rho_i;
-      const bool fast = c && rho_j > rho_i && s * slack < s_best;
       // selects rather than a branch: the candidate's position is a shared-memory broadcast
       const int qj = sq[j];
+      // The home point itself (equal density, never higher) is left out here: the full test
+      // would reject it only after a global load of its original index, and every pair of
+      // candidates holding some lane's own point would take that path (measured: nearest
+      // higher on calo4096 4.04 -> 3.79 ms, on the 4M 3-D points 2.40 -> 2.17 ms).
+      const bool c = need && in_block && s <= bnd && rho_j >= rho_i && qj != pos;
+      const bool fast = c && rho_j > rho_i && s * slack < s_best;
       const float bj = fminf(tdm, s * slack);
       s_best = fast ? s : s_best;
       bnd = fast ? bj : bnd;
@@ -1410,6 +1414,7 @@ __global__ void __launch_bounds__(kTileThreads, (N <= 4 ? 8 : 4) * 128 / kTileTh
       const float rho_h = __shfl_sync(0xffffffffu, rho_i, hl);
       const float bnd_h = __shfl_sync(0xffffffffu, bnd, hl);
       const int orig_h = __shfl_sync(0xffffffffu, orig_i, hl);
+      const int pos_h = __shfl_sync(0xffffffffu, pos, hl);
       // a before b (both higher than the home, same tile)
       auto less = [&](float sa, float ra, int ja, float sb, float rb, int jb) -> bool {
         if (sa * slack < sb) return true;
@@ -1428,7 +1433,10 @@ __global__ void __launch_bounds__(kTileThreads, (N <= 4 ? 8 : 4) * 128 / kTileTh
         const float sj = M::partial(xh, c, kp.mpar);
         if (gv && sj <= bnd_h && rj >= rho_h) {
           bool higher = rj > rho_h;
-          if (!higher && rj > 0.0f) higher = __ldg(perm + sq[j]) > orig_h;
+          if (!higher && rj > 0.0f) {  // (the home point itself needs no load: never higher)
+            const int qj = sq[j];
+            higher = qj != pos_h && __ldg(perm + qj) > orig_h;
+          }
           if (higher && (j_loc < 0 || less(sj, rj, j, s_loc, r_loc, j_loc))) {
             s_loc = sj;
             r_loc = rj;
