@@ -508,7 +508,8 @@ __global__ void k_init(const KParams kp, Events ev, int32_t* ev_pt, int32_t* ev_
   }
 }
 
-// Bounding box of a single event with grid-wide atomics.
+// Bounding box and largest |weight| of a single event: per-thread, warp and block reductions,
+// then one set of atomics per CTA.
 template <int N>
 __global__ void __launch_bounds__(256) k_bbox_single(InPtrs in, int n, EvGrid* g, DevStatus* st) {
   uint32_t emn[N], emx[N];
@@ -519,35 +520,77 @@ __global__ void __launch_bounds__(256) k_bbox_single(InPtrs in, int n, EvGrid* g
   }
   bool bad = false;
   uint32_t wmax = 0u;
-  const int stride = gridDim.x * blockDim.x;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+  auto take = [&](const float* x, float w) {
 #pragma unroll
     for (int d = 0; d < N; ++d) {
-      const float x = in.c[d][i];
-      bad |= !isfinite(x);
-      const uint32_t e = enc_float(x);
+      bad |= !isfinite(x[d]);
+      const uint32_t e = enc_float(x[d]);
       emn[d] = min(emn[d], e);
       emx[d] = max(emx[d], e);
     }
-    const float w = in.w[i];
     bad |= !isfinite(w);
     wmax = max(wmax, __float_as_uint(fabsf(w)));
+  };
+  const int stride = gridDim.x * blockDim.x;
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  // four points per thread and step, their loads in flight together
+  for (; i + 3 * stride < n; i += 4 * stride) {
+    float x[4][N], w[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+#pragma unroll
+      for (int d = 0; d < N; ++d) x[k][d] = in.c[d][i + k * stride];
+      w[k] = in.w[i + k * stride];
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) take(x[k], w[k]);
   }
+  for (; i < n; i += stride) {
+    float x[N];
+#pragma unroll
+    for (int d = 0; d < N; ++d) x[d] = in.c[d][i];
+    take(x, in.w[i]);
+  }
+  // warp, then block reduction: one set of atomics per CTA (same-address atomics from every
+  // warp of a large grid serialise at the L2)
+  __shared__ uint32_t s_red[8][2 * N + 2];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int d = 0; d < N; ++d) {
     emn[d] = warp_min_u(emn[d]);
     emx[d] = warp_max_u(emx[d]);
   }
   wmax = warp_max_u(wmax);
-  if ((threadIdx.x & 31) == 0) {
+  const bool wbad = __any_sync(0xffffffffu, bad);
+  if (lane == 0) {
 #pragma unroll
     for (int d = 0; d < N; ++d) {
-      atomicMin(&g->enc_min[d], emn[d]);
-      atomicMax(&g->enc_max[d], emx[d]);
+      s_red[warp][d] = emn[d];
+      s_red[warp][N + d] = emx[d];
     }
-    atomicMax(&g->wmax_bits, wmax);
+    s_red[warp][2 * N] = wmax;
+    s_red[warp][2 * N + 1] = wbad ? 1u : 0u;
   }
-  if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&st->nonfinite, 1u);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int nw = blockDim.x >> 5;
+    for (int w = 1; w < nw; ++w) {
+#pragma unroll
+      for (int d = 0; d < N; ++d) {
+        s_red[0][d] = min(s_red[0][d], s_red[w][d]);
+        s_red[0][N + d] = max(s_red[0][N + d], s_red[w][N + d]);
+      }
+      s_red[0][2 * N] = max(s_red[0][2 * N], s_red[w][2 * N]);
+      s_red[0][2 * N + 1] |= s_red[w][2 * N + 1];
+    }
+#pragma unroll
+    for (int d = 0; d < N; ++d) {
+      atomicMin(&g->enc_min[d], s_red[0][d]);
+      atomicMax(&g->enc_max[d], s_red[0][N + d]);
+    }
+    atomicMax(&g->wmax_bits, s_red[0][2 * N]);
+    if (s_red[0][2 * N + 1]) atomicOr(&st->nonfinite, 1u);
+  }
 }
 
 // Event of point i.  Events are contiguous, ascending point ranges: chunk_ev holds the event of
@@ -2275,7 +2318,7 @@ clue_status run_pipeline(Workspace& ws, const RunArgs& a, cudaStream_t s) {
   k_init<N><<<grid_for(kp.n_events, 256), 256, 0, s>>>(kp, ev, ws.ev_pt, ws.ev_tile, ws.status);
   int launches_pre = 0;
   if (kp.n_events == 1)
-    k_bbox_single<N><<<grid_for(n, 256), 256, 0, s>>>(in, n, ws.ev, ws.status);
+    k_bbox_single<N><<<std::max(1, std::min(grid_for(n, 1024), 148 * 4)), 256, 0, s>>>(in, n, ws.ev, ws.status);
   else
   {
     // spans of 32..1024 points: about four spans per resident warp (64 per SM) when there
