@@ -214,3 +214,33 @@ def test_autotune_batch_cache_and_equivalence(tmp_path):
                              "density_gate": 0, "density_exp2": 0, "labels_bfs": 0, "reserved": 0}
     for c in (tuned, other, base):
         c.close()
+
+
+@pytest.mark.parametrize("host", [False, True])
+def test_batch_nonfinite_rejected(gpu_context, host):
+    # A non-finite coordinate inside an event's span and a non-finite weight at the batch's
+    # last point are reported, by the device-memory batch and by the overlapped host batch
+    # (4M points or more, in chunks); the context stays usable afterwards.
+    import torch
+    from cluestering_alpaka3_b200 import capi
+    evs, off, coords, weight = make_events(91, 3300 if host else 400, lo=200, hi=20000 if host else 4000)
+    n = coords.shape[1]
+    assert not host or n >= 4_000_000  # the overlapped path
+    p, k, m = gpu_args(kernel=("flat", (0.5,)), dc=2.0, rhoc=4.0, dm=3.0)
+    e = len(off) // 2
+    for bad in ("coord", "weight"):
+        c, w = coords.copy(), weight.copy()
+        if bad == "coord":
+            c[1, (off[e] + off[e + 1]) // 2] = np.nan
+        else:
+            w[n - 1] = np.inf
+        with pytest.raises(capi.ClueInvalidArgument):
+            if host:
+                gpu_context.batch_host(c, w, off, p, k, m)
+            else:
+                dc_, dw_ = torch.from_numpy(c).cuda(), torch.from_numpy(w).cuda()
+                lab = torch.empty(n, dtype=torch.int32, device="cuda")
+                gpu_context.batch_device(dc_.data_ptr(), dw_.data_ptr(), 2, off, {"cluster_index": lab.data_ptr()},
+                                         p, k, m)
+    res, _ = gpu_context.batch_host(coords[:, :off[3]].copy(), weight[:off[3]].copy(), off[:4], p, k, m)
+    assert res.cluster_index.shape == (int(off[3]),)

@@ -228,6 +228,23 @@ def test_nonfinite_rejected(gpu_context):
     assert r.cluster_index.shape == (100,)
 
 
+@pytest.mark.parametrize("dim,where", [(2, 0), (0, 300_001), (3, 599_999)])
+def test_nonfinite_rejected_large_event(gpu_context, dim, where):
+    """Many CTAs reduce one event's box (four points per thread and step, then a remainder):
+    a non-finite coordinate or weight anywhere is reported (dim 3: the weight)."""
+    from cluestering_alpaka3_b200 import capi
+    from parity_util import gpu_args
+    rng = np.random.default_rng(7)
+    c = rng.uniform(0.0, 100.0, (3, 600_000)).astype(np.float32)
+    w = np.ones(600_000, np.float32)
+    if dim == 3:
+        w[where] = np.nan
+    else:
+        c[dim, where] = np.inf
+    with pytest.raises(capi.ClueInvalidArgument):
+        gpu_context.make_clusters_host(c, w, *gpu_args(dc=1.0, rhoc=1.0))
+
+
 def test_blobs2d_medium_exact(gpu_context):
     from cluestering_alpaka3_b200 import synthetic
     wl = synthetic.blobs_2d_1m(n=1 << 17)
