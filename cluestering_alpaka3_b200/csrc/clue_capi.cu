@@ -358,6 +358,11 @@ struct clue_context_s {
   // consecutive chunks' pipelines run concurrently (created on the first such batch).
   Workspace* alt = nullptr;
   cudaStream_t alt_stream = nullptr;
+  // The overlapped host batch's even chunks run on chunk_stream (a stream of the context, so a
+  // caller's legacy default stream never has to be captured), and every chunk's pipeline is
+  // captured into a graph whose executable is kept here and updated in place on the next call.
+  cudaGraphExec_t chunk_exec[Workspace::kPipeMaxChunks] = {};
+  cudaStream_t chunk_stream = nullptr;
 };
 
 extern "C" {
@@ -588,6 +593,9 @@ clue_status clue_context_destroy(clue_context ctx) {
     delete ctx->alt;
   }
   if (ctx->alt_stream) cudaStreamDestroy(ctx->alt_stream);
+  if (ctx->chunk_stream) cudaStreamDestroy(ctx->chunk_stream);
+  for (auto& ge : ctx->chunk_exec)
+    if (ge) cudaGraphExecDestroy(ge);
   cudaSetDevice(prev);
   delete ctx;
   return CLUE_OK;
@@ -1151,9 +1159,9 @@ static bool batch_overlap_ok(clue_context ctx, const clue_params* params, const 
 // A large host-memory batch in K chunks of whole events, so the copies overlap the pipeline:
 // every chunk's event table and inputs go up on a copy stream (all enqueued at once, each chunk
 // with its own pinned and device event table, since a copy engine runs its queue in order and
-// a small copy on the compute stream would wait behind all the inputs), chunk c runs on the
-// caller's stream once its copies are in, and its outputs come down on a second copy stream
-// while chunk c + 1 runs.  Events are independent and a chunk's results do not depend on the
+// a small copy on the compute stream would wait behind all the inputs), chunk c runs as one
+// graph launch on a stream of the context once its copies are in, and its outputs come down on
+// a second copy stream while chunk c + 1 runs; the caller's stream waits for all of it.  Events are independent and a chunk's results do not depend on the
 // other events in it, so the outputs are those of one pass over the whole batch (nearest-higher
 // indices are shifted to the batch).  The rare chunk whose label chains outlast the fixed
 // pointer-jumping rounds is run again alone.
@@ -1212,6 +1220,8 @@ static clue_status batch_host_overlapped(clue_context ctx, const clue_params* pa
     alt->tune_labels_bfs = ws.tune_labels_bfs;
     if (workspace_reserve(*alt, ndim, max_n, max_tiles, max_ev) != CLUE_OK) alt = nullptr;
   }
+  if (!ctx->chunk_stream) CLUE_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->chunk_stream, cudaStreamNonBlocking));
+  cudaStream_t s1 = ctx->chunk_stream;
   cudaStream_t s2 = alt ? ctx->alt_stream : nullptr;
   const uint64_t alt_launches0 = alt ? alt->launches : 0;
   struct DeviceGuard {
@@ -1257,6 +1267,7 @@ static clue_status batch_host_overlapped(clue_context ctx, const clue_params* pa
 
   auto drain = [&]() {
     cudaStreamSynchronize(h2d);
+    cudaStreamSynchronize(s1);
     cudaStreamSynchronize(s);
     if (s2) cudaStreamSynchronize(s2);
     cudaStreamSynchronize(d2h);
@@ -1270,6 +1281,7 @@ static clue_status batch_host_overlapped(clue_context ctx, const clue_params* pa
   CLUE_CUDA_TRY(cudaEventRecord(ev_start, s));
   CLUE_CUDA_TRY(cudaStreamWaitEvent(h2d, ev_start, 0));
   CLUE_CUDA_TRY(cudaStreamWaitEvent(d2h, ev_start, 0));
+  CLUE_CUDA_TRY(cudaStreamWaitEvent(s1, ev_start, 0));
   if (s2) CLUE_CUDA_TRY(cudaStreamWaitEvent(s2, ev_start, 0));
   std::vector<RunArgs> args(K);
   std::vector<int32_t> rel;
@@ -1313,8 +1325,8 @@ static clue_status batch_host_overlapped(clue_context ctx, const clue_params* pa
     drain();
     return st;
   }
-  // 2. chunks on the caller's stream and, the odd ones, on the second workspace's stream (each
-  //    with its own device event table): consecutive chunks run concurrently, so one chunk's
+  // 2. the even chunks on the context's chunk stream and the odd ones on the second workspace's
+  //    stream (each with its own device event table): consecutive chunks run concurrently, so one chunk's
   //    small-kernel phases and kernel tails overlap the next one's sweeps; results go out on the
   //    copy-out stream as each chunk finishes
   for (int c = 0; c < K && st == CLUE_OK; ++c) {
@@ -1331,14 +1343,36 @@ static clue_status batch_host_overlapped(clue_context ctx, const clue_params* pa
     a.ev_n_clusters = dev_ncl ? dev_ncl + e0 : nullptr;
     const bool on_alt = alt && (c & 1);
     Workspace& W = on_alt ? *alt : ws;
-    cudaStream_t sc = on_alt ? s2 : s;
+    cudaStream_t sc = on_alt ? s2 : s1;
     cudaError_t ce = cudaStreamWaitEvent(sc, ev_in(c), 0);
     if (ce == cudaSuccess) {
       EvGrid* const w_ev = W.ev;
       int32_t* const w_pt = W.ev_pt;
       int32_t* const w_tile = W.ev_tile;
       event_table_carve(dtab + dev_tab[c], (size_t)E, &W.ev, &W.ev_pt, &W.ev_tile);
-      st = run_pipeline_dispatch(W, a, sc);
+      // the chunk's pipeline as one graph launch: enqueued kernel by kernel, the launch gaps
+      // of four chunk pipelines cost about 0.7 ms per calo4096 batch
+      const bool timing = W.timing;
+      W.timing = false;
+      cudaGraph_t cg = nullptr;
+      ce = cudaStreamBeginCapture(sc, cudaStreamCaptureModeThreadLocal);
+      if (ce == cudaSuccess) {
+        st = run_pipeline_dispatch(W, a, sc);
+        ce = cudaStreamEndCapture(sc, &cg);
+      }
+      W.timing = timing;
+      if (ce == cudaSuccess && st == CLUE_OK) {
+        cudaGraphExec_t& ge = ctx->chunk_exec[c];
+        cudaGraphExecUpdateResultInfo ui;
+        if (!ge || cudaGraphExecUpdate(ge, cg, &ui) != cudaSuccess) {
+          cudaGetLastError();
+          if (ge) cudaGraphExecDestroy(ge);
+          ge = nullptr;
+          ce = cudaGraphInstantiate(&ge, cg, 0);
+        }
+        if (ce == cudaSuccess) ce = cudaGraphLaunch(ge, sc);
+      }
+      if (cg) cudaGraphDestroy(cg);
       W.ev = w_ev;
       W.ev_pt = w_pt;
       W.ev_tile = w_tile;
@@ -1370,9 +1404,13 @@ static clue_status batch_host_overlapped(clue_context ctx, const clue_params* pa
     }
   }
   if (alt) ws.launches += alt->launches - alt_launches0;  // the context counts both workspaces' kernels
-  if (st == CLUE_OK && s2) {  // the caller's stream waits for the second stream's chunks
-    CLUE_CUDA_TRY(cudaEventRecord(ws.pipe_ev[2], s2));
+  if (st == CLUE_OK) {  // the caller's stream waits for the chunk streams
+    CLUE_CUDA_TRY(cudaEventRecord(ws.pipe_ev[2], s1));
     CLUE_CUDA_TRY(cudaStreamWaitEvent(s, ws.pipe_ev[2], 0));
+    if (s2) {
+      CLUE_CUDA_TRY(cudaEventRecord(ws.pipe_ev[5], s2));
+      CLUE_CUDA_TRY(cudaStreamWaitEvent(s, ws.pipe_ev[5], 0));
+    }
   }
   if (st == CLUE_OK) {
     cudaError_t ce = cudaMemcpyAsync(ws.pipe_status_host, dslot, KM * (sizeof(DevStatus) + 4),
