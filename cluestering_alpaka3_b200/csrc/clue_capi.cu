@@ -363,7 +363,61 @@ struct clue_context_s {
   // captured into a graph whose executable is kept here and updated in place on the next call.
   cudaGraphExec_t chunk_exec[Workspace::kPipeMaxChunks] = {};
   cudaStream_t chunk_stream = nullptr;
+  // the same for the pipeline of a blocking call (run_pipeline_graph)
+  cudaGraphExec_t plain_exec = nullptr;
+  cudaEvent_t plain_ev[2] = {};
 };
+
+// Captures the pipeline enqueued by run_pipeline_dispatch on `g` into a graph and launches it
+// there, keeping the executable in *exec (updated in place when the captured graph has the same
+// shape, else instantiated again).
+static clue_status capture_and_launch(Workspace& w, const RunArgs& a, cudaStream_t g, cudaGraphExec_t* exec) {
+  const bool timing = w.timing;
+  w.timing = false;
+  cudaGraph_t cg = nullptr;
+  clue_status st = CLUE_OK;
+  cudaError_t ce = cudaStreamBeginCapture(g, cudaStreamCaptureModeThreadLocal);
+  if (ce == cudaSuccess) {
+    st = run_pipeline_dispatch(w, a, g);
+    ce = cudaStreamEndCapture(g, &cg);
+  }
+  w.timing = timing;
+  if (ce == cudaSuccess && st == CLUE_OK) {
+    cudaGraphExecUpdateResultInfo ui;
+    if (!*exec || cudaGraphExecUpdate(*exec, cg, &ui) != cudaSuccess) {
+      cudaGetLastError();
+      if (*exec) cudaGraphExecDestroy(*exec);
+      *exec = nullptr;
+      ce = cudaGraphInstantiate(exec, cg, 0);
+    }
+    if (ce == cudaSuccess) ce = cudaGraphLaunch(*exec, g);
+  }
+  if (cg) cudaGraphDestroy(cg);
+  if (st == CLUE_OK && ce != cudaSuccess) {
+    set_error(std::string("pipeline graph: ") + cudaGetErrorString(ce));
+    st = CLUE_ERR_CUDA;
+  }
+  return st;
+}
+
+// One pipeline of a blocking host-memory call as a graph launch on the context's chunk stream,
+// ordered after the work already on the caller's stream s and before its next: enqueued kernel
+// by kernel, the launch gaps cost several microseconds per kernel.  (A stream of the context,
+// since a caller's legacy default stream cannot be captured.)
+static clue_status run_pipeline_graph(clue_context ctx, const RunArgs& a, cudaStream_t s) {
+  Workspace& ws = ctx->ws;
+  if (ws.timing) return run_pipeline_dispatch(ws, a, s);  // stage timing records events per stage
+  if (!ctx->chunk_stream) CLUE_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->chunk_stream, cudaStreamNonBlocking));
+  for (auto& e : ctx->plain_ev)
+    if (!e) CLUE_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  cudaStream_t g = ctx->chunk_stream;
+  CLUE_CUDA_TRY(cudaEventRecord(ctx->plain_ev[0], s));
+  CLUE_CUDA_TRY(cudaStreamWaitEvent(g, ctx->plain_ev[0], 0));
+  const clue_status st = capture_and_launch(ws, a, g, &ctx->plain_exec);
+  CLUE_CUDA_TRY(cudaEventRecord(ctx->plain_ev[1], g));
+  CLUE_CUDA_TRY(cudaStreamWaitEvent(s, ctx->plain_ev[1], 0));
+  return st;
+}
 
 extern "C" {
 
@@ -596,6 +650,9 @@ clue_status clue_context_destroy(clue_context ctx) {
   if (ctx->chunk_stream) cudaStreamDestroy(ctx->chunk_stream);
   for (auto& ge : ctx->chunk_exec)
     if (ge) cudaGraphExecDestroy(ge);
+  if (ctx->plain_exec) cudaGraphExecDestroy(ctx->plain_exec);
+  for (auto& e : ctx->plain_ev)
+    if (e) cudaEventDestroy(e);
   cudaSetDevice(prev);
   delete ctx;
   return CLUE_OK;
@@ -767,7 +824,7 @@ clue_status clue_make_clusters(clue_context ctx, const clue_params* params, cons
     dev_out.delta = out->delta ? reinterpret_cast<float*>(o + 4 * nn) : nullptr;
     a.out = dev_out;
   }
-  st = run_pipeline_dispatch(ws, a, s);
+  st = run_pipeline_graph(ctx, a, s);
   bool unresolved = false;
   if (st == CLUE_OK) st = read_info(ws, a.kp, s, info, unresolved);
   if (st == CLUE_OK && unresolved) {
@@ -1090,7 +1147,7 @@ static clue_status batch_plain(clue_context ctx, const clue_params* params, cons
   a.out = dev_out;
   a.ev_n_clusters = dev_ncl;
   st = upload_events(ws, n_events, s);
-  if (st == CLUE_OK) st = run_pipeline_dispatch(ws, a, s);
+  if (st == CLUE_OK) st = run_pipeline_graph(ctx, a, s);
   bool unresolved = false;
   if (st == CLUE_OK) st = read_info(ws, a.kp, s, info, unresolved);
   if (st == CLUE_OK && unresolved) {
@@ -1352,27 +1409,7 @@ static clue_status batch_host_overlapped(clue_context ctx, const clue_params* pa
       event_table_carve(dtab + dev_tab[c], (size_t)E, &W.ev, &W.ev_pt, &W.ev_tile);
       // the chunk's pipeline as one graph launch: enqueued kernel by kernel, the launch gaps
       // of four chunk pipelines cost about 0.7 ms per calo4096 batch
-      const bool timing = W.timing;
-      W.timing = false;
-      cudaGraph_t cg = nullptr;
-      ce = cudaStreamBeginCapture(sc, cudaStreamCaptureModeThreadLocal);
-      if (ce == cudaSuccess) {
-        st = run_pipeline_dispatch(W, a, sc);
-        ce = cudaStreamEndCapture(sc, &cg);
-      }
-      W.timing = timing;
-      if (ce == cudaSuccess && st == CLUE_OK) {
-        cudaGraphExec_t& ge = ctx->chunk_exec[c];
-        cudaGraphExecUpdateResultInfo ui;
-        if (!ge || cudaGraphExecUpdate(ge, cg, &ui) != cudaSuccess) {
-          cudaGetLastError();
-          if (ge) cudaGraphExecDestroy(ge);
-          ge = nullptr;
-          ce = cudaGraphInstantiate(&ge, cg, 0);
-        }
-        if (ce == cudaSuccess) ce = cudaGraphLaunch(ge, sc);
-      }
-      if (cg) cudaGraphDestroy(cg);
+      st = capture_and_launch(W, a, sc, &ctx->chunk_exec[c]);
       W.ev = w_ev;
       W.ev_pt = w_pt;
       W.ev_tile = w_tile;
