@@ -144,7 +144,7 @@ struct Workspace {
   // runtime choices (clue_context_set_tuning; clue_autotune_batch measures and picks them)
   int32_t tune_symmetric = 1;                  // symmetric density sweep where it applies
   int32_t tune_nh_split = 8;                   // nearest higher: split a block needed by <= this many lanes
-  int64_t tune_overlap_chunk_points = 2700000;  // host-memory batches; 0: no overlap
+  int64_t tune_overlap_chunk_points = 2200000;  // host-memory batches; 0: no overlap
   int32_t tune_density_gate = 0;               // symmetric density: vote-gated pair steps
   int32_t tune_density_exp2 = 0;               // symmetric density: 2^x on the FMA pipe
   int32_t tune_labels_bfs = 0;                 // labels by follower CSR + frontier BFS, not pointer jumping

@@ -299,7 +299,7 @@ clue_status clue_graph_destroy(clue_graph graph);
  *                       many lanes of a warp still need is split among all 32 lanes; 0 never
  *                       splits.  Results are identical for every value.
  *   overlap_chunk_points  host-memory batches of 4M points or more overlap their copies with
- *                       the pipeline in chunks of about this many points (default 2700000);
+ *                       the pipeline in chunks of about this many points (default 2200000);
  *                       0 turns the overlap off.  Results are identical.
  * clue_autotune_batch times the candidate values on a device-resident sample batch (CUDA
  * events on `stream`), keeps the fastest in the context and, with cache_path non-NULL, appends

@@ -128,4 +128,4 @@ def test_tuning_defaults():
     from cluestering_alpaka3_b200 import capi
     t = capi._Tuning()
     capi.lib.clue_tuning_defaults(ctypes.byref(t))
-    assert (t.symmetric_density, t.nh_split_lanes, t.overlap_chunk_points) == (1, 8, 2700000)
+    assert (t.symmetric_density, t.nh_split_lanes, t.overlap_chunk_points) == (1, 8, 2200000)

@@ -210,7 +210,7 @@ def test_autotune_batch_cache_and_equivalence(tmp_path):
     with pytest.raises(capi.ClueError):
         base.set_tuning(density_exp2=3)
     base.reset_tuning()
-    assert base.tuning() == {"symmetric_density": 1, "nh_split_lanes": 8, "overlap_chunk_points": 2700000,
+    assert base.tuning() == {"symmetric_density": 1, "nh_split_lanes": 8, "overlap_chunk_points": 2200000,
                              "density_gate": 0, "density_exp2": 0, "labels_bfs": 0, "reserved": 0}
     for c in (tuned, other, base):
         c.close()
