@@ -203,7 +203,9 @@ size_t clue_context_workspace_bytes(clue_context ctx);
  * coords: SoA, coords[d * n + i];  weight: n floats.  Both in `memory` space, as are
  * the outputs.  With CLUE_MEM_HOST the library copies through pinned staging
  * buffers on `stream`.  Blocks until the results are in `out` (the reference's
- * make_clusters waits as well); `info` may be NULL.
+ * make_clusters waits as well); `info` may be NULL.  The pipeline itself runs as one CUDA
+ * graph launch on a stream of the context, ordered after the work already on `stream` and
+ * before its next (the executable graph is kept in the context and updated on the next call).
  * Non-finite coordinates or weights are rejected with CLUE_ERR_NONFINITE
  * (the reference's behaviour there is undefined: static_cast<int>(NaN)).
  */
@@ -248,9 +250,10 @@ uint64_t clue_context_kernel_launches(clue_context ctx);
  * it had been clustered alone.  ev_n_clusters (optional, n_events entries, same memory space
  * as the outputs) receives every event's cluster count; `info` holds the totals.
  * With CLUE_MEM_HOST, a batch of 4M points or more is run in chunks of whole events whose
- * copies overlap the previous chunk's pipeline (clue_tuning.overlap_chunk_points); the outputs
- * are the same as one pass, and the call returns when they are in `out`.  Pinned host buffers
- * are needed for the copies to overlap.
+ * copies overlap the previous chunk's pipeline (clue_tuning.overlap_chunk_points; consecutive
+ * chunks run concurrently on two workspaces and two streams of the context, each chunk as one
+ * graph launch); the outputs are the same as one pass, and the call returns when they are in
+ * `out`.  Pinned host buffers are needed for the copies to overlap.
  */
 clue_status clue_batch_make_clusters(clue_context ctx, const clue_params* params, const clue_kernel* kernel,
                                      const clue_metric* metric, int32_t ndim, int32_t n_events,
