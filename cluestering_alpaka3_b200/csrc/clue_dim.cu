@@ -42,7 +42,7 @@ constexpr int kChunkWarps = kTileThreads / 32;
 constexpr int kChunk = kChunkPoints;  // home points per CTA in the density / nearest-higher sweeps
 static_assert(kChunkPoints == kTileThreads, "one home point per thread");
 // float4 words per staging buffer (12 KiB).  Two 16 KiB buffers held the reference-order density
-// to six CTAs per SM by shared memory; at 12 KiB registers set it to seven (measured on the 1M
+// to six CTAs per SM by shared memory; at 12 KiB it runs eight (63 registers; measured on the 1M
 // 2-D points: 0.630 -> 0.587 ms, the same bits).
 constexpr int kStageWords = 768;
 constexpr int kMaxSeg = 32;        // tile segments per staged piece
